@@ -1,0 +1,653 @@
+// Oracle: a CPU restatement of syndrome's QC-LDPC path, used ONLY as a checker.
+//
+// This file is test infrastructure.  Only tests/, __graft_entry__.smoke() and
+// bench.py's CPU-baseline leg may load the library built from it; the decoder
+// library (syndrome_b200/) never links or calls it.
+//
+// Every function restates the reference's algorithm with the reference's own
+// operation order so that results are bit-identical:
+//   * layered CSR layout        syndrome src/qc_ldpc.rs:116-140, 281-319, 339-455
+//   * f32 LOMS decode           src/qc_ldpc.rs:962-1221 (scalar branch :1146-1205)
+//   * f32 syndrome check        src/qc_ldpc.rs:1231-1252
+//   * 5G f32 prologue           src/qc_ldpc.rs:711-732
+//   * int8/int16 LOMS decode    src/qc_ldpc.rs:1530-1758 (scalar branch :1670-1745)
+//   * int16 syndrome check      src/qc_ldpc.rs:1766-1787
+//   * 5G int8 prologue          src/qc_ldpc.rs:1486-1523
+//   * quantizer / beta_q        src/quantize.rs:148-155, 298-305, 331-343 (+float_ext.rs round)
+//   * encoder                   src/qc_ldpc.rs:2166-2727 (sparse core solve) and :1996-2125 (dense)
+//   * AWGN channel              src/channel_sim.rs:61-241
+// Built with -ffp-contract=off and without -ffast-math so IEEE f32 operations
+// happen exactly as written.
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+#include "../syndrome_b200/csrc/graph_tables.h"
+#include "../syndrome_b200/csrc/base_graph_tables.inc"
+
+namespace {
+
+struct Params {
+  int bg;  // 0 = BG1, 1 = BG2, -1 = raw edge list
+  int z;
+  int mb;
+  int nb;
+  std::vector<int> layer_off;
+  std::vector<int> cols;
+  std::vector<int> shifts;
+  int maxdeg;
+  // encoder state
+  int enc_kind;  // 0 unbuilt, 1 sparse, 2 dense, -1 singular
+  int sp[9];     // sparse core layout (see derive_core)
+  std::vector<std::vector<uint64_t>> gen;  // dense generator rows (m rows of k bits)
+};
+
+// syndrome src/qc_ldpc.rs:93-122 (Table 5.3.2-1 lifting sets).
+const int kLiftingSets[8][8] = {
+    {2, 4, 8, 16, 32, 64, 128, 256}, {3, 6, 12, 24, 48, 96, 192, 384},
+    {5, 10, 20, 40, 80, 160, 320, 0}, {7, 14, 28, 56, 112, 224, 0, 0},
+    {9, 18, 36, 72, 144, 288, 0, 0},  {11, 22, 44, 88, 176, 352, 0, 0},
+    {13, 26, 52, 104, 208, 0, 0, 0},  {15, 30, 60, 120, 240, 0, 0, 0}};
+
+int ils_for_z(int z) {
+  for (int s = 0; s < 8; ++s)
+    for (int j = 0; j < 8; ++j)
+      if (kLiftingSets[s][j] == z && z != 0) return s;
+  return -1;
+}
+
+// syndrome src/qc_ldpc.rs:281-319: group edges by row, keeping entry order inside a row.
+void build_layout(Params* p, const std::vector<int>& r, const std::vector<int>& c,
+                  const std::vector<int>& s) {
+  std::vector<int> deg(p->mb, 0);
+  for (int x : r) deg[x]++;
+  p->layer_off.assign(p->mb + 1, 0);
+  for (int i = 0; i < p->mb; ++i) p->layer_off[i + 1] = p->layer_off[i] + deg[i];
+  int total = p->layer_off[p->mb];
+  p->cols.assign(total, 0);
+  p->shifts.assign(total, 0);
+  std::vector<int> fill(p->mb, 0);
+  for (size_t i = 0; i < r.size(); ++i) {
+    int pos = p->layer_off[r[i]] + fill[r[i]]++;
+    p->cols[pos] = c[i];
+    p->shifts[pos] = s[i];
+  }
+  p->maxdeg = 0;
+  for (int d : deg) p->maxdeg = std::max(p->maxdeg, d);
+}
+
+inline int rot(int zi, int shift, int z) {
+  int s = zi + shift;
+  return s >= z ? s - z : s;
+}
+
+bool syndrome_ok_f32(const Params* p, const float* llr) {
+  const int z = p->z;
+  for (int l = 0; l < p->mb; ++l) {
+    for (int zi = 0; zi < z; ++zi) {
+      unsigned par = 0;
+      for (int e = p->layer_off[l]; e < p->layer_off[l + 1]; ++e)
+        par ^= (llr[p->cols[e] * z + rot(zi, p->shifts[e], z)] < 0.0f) ? 1u : 0u;
+      if (par) return false;
+    }
+  }
+  return true;
+}
+
+bool syndrome_ok_i16(const Params* p, const int16_t* app) {
+  const int z = p->z;
+  for (int l = 0; l < p->mb; ++l) {
+    for (int zi = 0; zi < z; ++zi) {
+      unsigned par = 0;
+      for (int e = p->layer_off[l]; e < p->layer_off[l + 1]; ++e)
+        par ^= (app[p->cols[e] * z + rot(zi, p->shifts[e], z)] < 0) ? 1u : 0u;
+      if (par) return false;
+    }
+  }
+  return true;
+}
+
+inline uint32_t f2u(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  return u;
+}
+inline float u2f(uint32_t u) {
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
+// ---------------------------------------------------------------- encoder --
+// syndrome src/qc_ldpc.rs:2129-2141 (rotl_xor_into): dst[i] ^= src[(i + shift) mod z].
+void rotl_xor(uint8_t* dst, const uint8_t* src, int shift, int z) {
+  for (int i = 0; i < z; ++i) dst[i] ^= src[rot(i, shift, z)];
+}
+void rotl_set(uint8_t* dst, const uint8_t* src, int shift, int z) {
+  for (int i = 0; i < z; ++i) dst[i] = src[rot(i, shift, z)];
+}
+
+// Core parity entries (offset, shift) of a row: syndrome src/qc_ldpc.rs:2190-2205.
+int core_entries(const Params* p, int row, int kb, int out[4][2]) {
+  int n = 0;
+  for (int e = p->layer_off[row]; e < p->layer_off[row + 1]; ++e) {
+    int c = p->cols[e];
+    if (c >= kb && c < kb + 4 && n < 4) {
+      out[n][0] = c - kb;
+      out[n][1] = p->shifts[e];
+      ++n;
+    }
+  }
+  return n;
+}
+int shift_for(int ent[4][2], int n, int off) {
+  for (int i = 0; i < n; ++i)
+    if (ent[i][0] == off) return ent[i][1];
+  return -1;
+}
+
+// syndrome src/qc_ldpc.rs:2238-2318 (CoreLayout::derive).  sp[] = {p1_edge, p1_x,
+// row_x_is_1, s0p2, s1p2, s1p3, s2p3, s2p4, s3p4}.
+bool derive_core(const Params* p, int kb, int sp[9]) {
+  if (p->mb < 4 || p->nb < kb + 4) return false;
+  int r0[4][2], r1[4][2], r2[4][2], r3[4][2];
+  int n0 = core_entries(p, 0, kb, r0), n1 = core_entries(p, 1, kb, r1);
+  int n2 = core_entries(p, 2, kb, r2), n3 = core_entries(p, 3, kb, r3);
+  if (n0 != 2 || n3 != 2) return false;
+  int s0p1 = shift_for(r0, n0, 0), s0p2 = shift_for(r0, n0, 1);
+  int s3p1 = shift_for(r3, n3, 0), s3p4 = shift_for(r3, n3, 3);
+  if (s0p1 < 0 || s0p2 < 0 || s3p1 < 0 || s3p4 < 0 || s0p1 != s3p1) return false;
+  int r1p1 = shift_for(r1, n1, 0), r2p1 = shift_for(r2, n2, 0);
+  int row_x_is_1, px;
+  if (r1p1 >= 0 && r2p1 < 0) {
+    row_x_is_1 = 1;
+    px = r1p1;
+  } else if (r1p1 < 0 && r2p1 >= 0) {
+    row_x_is_1 = 0;
+    px = r2p1;
+  } else {
+    return false;
+  }
+  int s1p2 = shift_for(r1, n1, 1), s1p3 = shift_for(r1, n1, 2);
+  int s2p3 = shift_for(r2, n2, 2), s2p4 = shift_for(r2, n2, 3);
+  if (s1p2 < 0 || s1p3 < 0 || s2p3 < 0 || s2p4 < 0) return false;
+  if (n1 != (row_x_is_1 ? 3 : 2) || n2 != (row_x_is_1 ? 2 : 3)) return false;
+  for (int row = 4; row < p->mb; ++row) {
+    int hits = 0;
+    for (int e = p->layer_off[row]; e < p->layer_off[row + 1]; ++e) {
+      int c = p->cols[e];
+      if (c >= kb + 4) {
+        ++hits;
+        if (c != kb + row || p->shifts[e] != 0) return false;
+      }
+    }
+    if (hits != 1) return false;
+  }
+  int v[9] = {s0p1, px, row_x_is_1, s0p2, s1p2, s1p3, s2p3, s2p4, s3p4};
+  memcpy(sp, v, sizeof(v));
+  return true;
+}
+
+// syndrome src/qc_ldpc.rs:2006-2085 (ParityGenerator::build): Gauss-Jordan over
+// the augmented [H_p | H_s] system, parity bit i = variable k + i.
+bool build_dense(Params* p) {
+  const int z = p->z, mb = p->mb, nb = p->nb, kb = nb - mb;
+  const int m = mb * z, k = kb * z;
+  const int aug_words = (m + k + 63) / 64;
+  std::vector<std::vector<uint64_t>> aug(m, std::vector<uint64_t>(aug_words, 0));
+  for (int l = 0; l < mb; ++l)
+    for (int e = p->layer_off[l]; e < p->layer_off[l + 1]; ++e)
+      for (int zi = 0; zi < z; ++zi) {
+        int row = l * z + zi;
+        int var = p->cols[e] * z + (zi + p->shifts[e]) % z;
+        int bit = var < k ? m + var : var - k;
+        aug[row][bit >> 6] ^= 1ull << (bit & 63);
+      }
+  for (int col = 0; col < m; ++col) {
+    int piv = -1;
+    for (int r = col; r < m; ++r)
+      if ((aug[r][col >> 6] >> (col & 63)) & 1) {
+        piv = r;
+        break;
+      }
+    if (piv < 0) return false;
+    if (piv != col) std::swap(aug[piv], aug[col]);
+    const std::vector<uint64_t> pr = aug[col];
+    for (int r = 0; r < m; ++r)
+      if (r != col && ((aug[r][col >> 6] >> (col & 63)) & 1))
+        for (int w = 0; w < aug_words; ++w) aug[r][w] ^= pr[w];
+  }
+  const int gw = (k + 63) / 64;
+  p->gen.assign(m, std::vector<uint64_t>(gw, 0));
+  for (int i = 0; i < m; ++i)
+    for (int b = 0; b < k; ++b)
+      if ((aug[i][(m + b) >> 6] >> ((m + b) & 63)) & 1) p->gen[i][b >> 6] |= 1ull << (b & 63);
+  return true;
+}
+
+void ensure_encoder(Params* p) {
+  if (p->enc_kind != 0) return;
+  const int kb = p->nb - p->mb;
+  if (derive_core(p, kb, p->sp))
+    p->enc_kind = 1;
+  else
+    p->enc_kind = build_dense(p) ? 2 : -1;
+}
+
+void lambda_row(const Params* p, int row, int kb, const uint8_t* cw, uint8_t* lam) {
+  const int z = p->z;
+  memset(lam, 0, z);
+  for (int e = p->layer_off[row]; e < p->layer_off[row + 1]; ++e)
+    if (p->cols[e] < kb) rotl_xor(lam, cw + p->cols[e] * z, p->shifts[e], z);
+}
+
+// syndrome src/qc_ldpc.rs:2620-2727 (encode_sparse).
+void encode_sparse(const Params* p, uint8_t* cw) {
+  const int z = p->z, kb = p->nb - p->mb, k = kb * z;
+  const int* sp = p->sp;
+  std::vector<uint8_t> l0(z), l1(z), l2(z), l3(z), p1(z), p2(z), p3(z), p4(z), t(z);
+  lambda_row(p, 0, kb, cw, l0.data());
+  lambda_row(p, 1, kb, cw, l1.data());
+  lambda_row(p, 2, kb, cw, l2.data());
+  lambda_row(p, 3, kb, cw, l3.data());
+  auto inv = [z](int s) { return (z - s) % z; };
+  for (int i = 0; i < z; ++i) t[i] = l0[i] ^ l1[i] ^ l2[i] ^ l3[i];
+  rotl_set(p1.data(), t.data(), inv(sp[1]), z);
+  t = l0;
+  rotl_xor(t.data(), p1.data(), sp[0], z);
+  rotl_set(p2.data(), t.data(), inv(sp[3]), z);
+  t = l1;
+  rotl_xor(t.data(), p2.data(), sp[4], z);
+  if (sp[2]) rotl_xor(t.data(), p1.data(), sp[1], z);
+  rotl_set(p3.data(), t.data(), inv(sp[5]), z);
+  t = l2;
+  rotl_xor(t.data(), p3.data(), sp[6], z);
+  if (!sp[2]) rotl_xor(t.data(), p1.data(), sp[1], z);
+  rotl_set(p4.data(), t.data(), inv(sp[7]), z);
+  memcpy(cw + k, p1.data(), z);
+  memcpy(cw + k + z, p2.data(), z);
+  memcpy(cw + k + 2 * z, p3.data(), z);
+  memcpy(cw + k + 3 * z, p4.data(), z);
+  const uint8_t* core[4] = {p1.data(), p2.data(), p3.data(), p4.data()};
+  for (int row = 4; row < p->mb; ++row) {
+    std::fill(t.begin(), t.end(), 0);
+    for (int e = p->layer_off[row]; e < p->layer_off[row + 1]; ++e) {
+      int c = p->cols[e];
+      if (c < kb)
+        rotl_xor(t.data(), cw + c * z, p->shifts[e], z);
+      else if (c < kb + 4)
+        rotl_xor(t.data(), core[c - kb], p->shifts[e], z);
+    }
+    memcpy(cw + k + row * z, t.data(), z);
+  }
+}
+
+// syndrome src/channel_sim.rs:61-67.
+uint64_t splitmix64(uint64_t seed) {
+  uint64_t z = seed + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return z == 0 ? 1 : z;
+}
+// syndrome src/channel_sim.rs:77-89.
+float next_uniform(uint64_t* st) {
+  uint64_t x = *st;
+  x ^= x << 13;
+  x ^= x >> 7;
+  x ^= x << 17;
+  *st = x;
+  uint32_t mant = (uint32_t)(x >> 41);
+  return u2f(0x3F800000u | mant) - 1.0f;
+}
+// syndrome src/channel_sim.rs:96-103 (Box-Muller, cosine branch).
+float next_gaussian(uint64_t* st) {
+  float u1 = std::max(next_uniform(st), 1e-38f);
+  float u2 = next_uniform(st);
+  const float two_pi = 2.0f * 3.14159265358979323846f;
+  return sqrtf(-2.0f * logf(u1)) * cosf(two_pi * u2);
+}
+
+}  // namespace
+
+extern "C" {
+
+// ------------------------------------------------------------------ layout --
+void* orc_params_5g(int bg, int z) {
+  int ils = ils_for_z(z);
+  if (ils < 0 || (bg != 0 && bg != 1)) return nullptr;
+  const syn_bg_entry_t* ents = bg == 0 ? syn_bg1_entries : syn_bg2_entries;
+  int n = bg == 0 ? SYN_BG1_EDGES : SYN_BG2_EDGES;
+  Params* p = new Params();
+  p->bg = bg;
+  p->z = z;
+  p->mb = bg == 0 ? SYN_BG1_ROWS : SYN_BG2_ROWS;
+  p->nb = bg == 0 ? SYN_BG1_COLS : SYN_BG2_COLS;
+  p->enc_kind = 0;
+  std::vector<int> r(n), c(n), s(n);
+  for (int i = 0; i < n; ++i) {
+    r[i] = ents[i].r;
+    c[i] = ents[i].c;
+    s[i] = (int)((unsigned)ents[i].v[ils] % (unsigned)z);  // syndrome qc_ldpc.rs:135-140
+  }
+  build_layout(p, r, c, s);
+  return p;
+}
+
+void* orc_params_raw(const int* rows, const int* cols, const int* shifts, int n, int mb, int nb,
+                     int z) {
+  if (z <= 0 || z > 384) return nullptr;  // syndrome qc_ldpc.rs:418-423
+  for (int i = 0; i < n; ++i)
+    if (rows[i] < 0 || rows[i] >= mb || cols[i] < 0 || cols[i] >= nb || shifts[i] < 0 ||
+        shifts[i] >= z)
+      return nullptr;
+  Params* p = new Params();
+  p->bg = -1;
+  p->z = z;
+  p->mb = mb;
+  p->nb = nb;
+  p->enc_kind = 0;
+  build_layout(p, std::vector<int>(rows, rows + n), std::vector<int>(cols, cols + n),
+               std::vector<int>(shifts, shifts + n));
+  return p;
+}
+
+void* orc_params_wifi(int z, int rate_num, int rate_den) {
+  for (int i = 0; i < SYN_WIFI_MATRIX_COUNT; ++i) {
+    const syn_wifi_matrix_t& m = syn_wifi_matrices[i];
+    if (m.z == z && m.rate_num == rate_num && m.rate_den == rate_den) {
+      std::vector<int> r(m.edge_count), c(m.edge_count), s(m.edge_count);
+      for (int j = 0; j < m.edge_count; ++j) {
+        r[j] = m.edges[j].r;
+        c[j] = m.edges[j].c;
+        s[j] = m.edges[j].s;
+      }
+      return orc_params_raw(r.data(), c.data(), s.data(), m.edge_count, m.row_blocks,
+                            m.col_blocks, m.z);
+    }
+  }
+  return nullptr;
+}
+
+void orc_params_free(void* h) { delete static_cast<Params*>(h); }
+
+// info[0..7] = {mb, nb, z, edges, maxdeg, N, K, M}
+void orc_params_info(const void* h, int* info) {
+  const Params* p = static_cast<const Params*>(h);
+  info[0] = p->mb;
+  info[1] = p->nb;
+  info[2] = p->z;
+  info[3] = (int)p->cols.size();
+  info[4] = p->maxdeg;
+  info[5] = p->nb * p->z;
+  info[6] = (p->nb - p->mb) * p->z;
+  info[7] = p->mb * p->z;
+}
+
+void orc_params_layout(const void* h, int* layer_off, int* cols, int* shifts) {
+  const Params* p = static_cast<const Params*>(h);
+  std::copy(p->layer_off.begin(), p->layer_off.end(), layer_off);
+  std::copy(p->cols.begin(), p->cols.end(), cols);
+  std::copy(p->shifts.begin(), p->shifts.end(), shifts);
+}
+
+// ------------------------------------------------------------- f32 decode --
+// Returns iterations used.  trace (nullable) receives the N hard bits after every
+// completed iteration, before the syndrome check (qc_ldpc.rs:1208).
+long orc_decode_f32(const void* h, float beta, float* llr, float* edge_r, uint8_t* hard,
+                    long iterations, uint8_t* trace) {
+  const Params* p = static_cast<const Params*>(h);
+  const int z = p->z;
+  const long n = (long)p->nb * z;
+  const long ecount = (long)p->cols.size() * z;
+  for (long i = 0; i < ecount; ++i) edge_r[i] = 0.0f;
+  std::vector<float> q((size_t)std::max(p->maxdeg, 1) * z), m1(z), m2(z);
+  std::vector<uint32_t> sx(z);
+  long used = 0;
+  for (long it = 0; it < iterations; ++it) {
+    ++used;
+    for (int l = 0; l < p->mb; ++l) {
+      const int lb = p->layer_off[l], deg = p->layer_off[l + 1] - lb;
+      for (int e = 0; e < deg; ++e) {
+        const int vb = p->cols[lb + e] * z, sh = p->shifts[lb + e];
+        const float* r = edge_r + (long)(lb + e) * z;
+        for (int zi = 0; zi < z; ++zi) q[e * z + zi] = llr[vb + rot(zi, sh, z)] - r[zi];
+      }
+      for (int zi = 0; zi < z; ++zi) {
+        m1[zi] = FLT_MAX;
+        m2[zi] = FLT_MAX;
+        sx[zi] = 0;
+      }
+      for (int e = 0; e < deg; ++e)
+        for (int zi = 0; zi < z; ++zi) {
+          uint32_t b = f2u(q[e * z + zi]);
+          float a = u2f(b & 0x7FFFFFFFu);
+          sx[zi] ^= b & 0x80000000u;
+          float mm1 = m1[zi];
+          if (a <= mm1) {
+            m2[zi] = mm1;
+            m1[zi] = a;
+          } else if (a < m2[zi]) {
+            m2[zi] = a;
+          }
+        }
+      for (int zi = 0; zi < z; ++zi) {
+        if (m1[zi] == FLT_MAX) m1[zi] = 0.0f;
+        if (m2[zi] == FLT_MAX) m2[zi] = m1[zi];
+      }
+      for (int e = 0; e < deg; ++e) {
+        const int vb = p->cols[lb + e] * z, sh = p->shifts[lb + e];
+        float* r = edge_r + (long)(lb + e) * z;
+        for (int zi = 0; zi < z; ++zi) {
+          uint32_t qb = f2u(q[e * z + zi]);
+          float a = u2f(qb & 0x7FFFFFFFu);
+          uint32_t sgn = sx[zi] ^ (qb & 0x80000000u);
+          float mex = (a == m1[zi]) ? m2[zi] : m1[zi];
+          float mag = mex - beta;
+          if (mag < 0.0f) mag = 0.0f;
+          float nr = u2f(f2u(mag) | sgn);
+          float orr = r[zi];
+          r[zi] = nr;
+          float* dst = &llr[vb + rot(zi, sh, z)];
+          *dst = *dst + (nr - orr);
+        }
+      }
+    }
+    if (trace)
+      for (long i = 0; i < n; ++i) trace[(it)*n + i] = llr[i] < 0.0f ? 1 : 0;
+    if (syndrome_ok_f32(p, llr)) break;
+  }
+  for (long i = 0; i < n; ++i) hard[i] = llr[i] < 0.0f ? 1 : 0;
+  return used;
+}
+
+// syndrome src/qc_ldpc.rs:711-732.
+void orc_init_5g_f32(const void* h, float* llr, long n_filler) {
+  const Params* p = static_cast<const Params*>(h);
+  const long z = p->z, k = (long)(p->nb - p->mb) * z;
+  const long kp = n_filler > k ? 0 : k - n_filler;
+  for (long i = kp; i < k; ++i) llr[i] = 1000000.0f;
+  for (long i = 0; i < 2 * z; ++i) llr[i] = 0.0f;
+}
+
+// ------------------------------------------------------------ int8 decode --
+long orc_decode_i8(const void* h, int beta_q, int app_clamp, int16_t* app, int8_t* edge_r,
+                   uint8_t* hard, long iterations) {
+  const Params* p = static_cast<const Params*>(h);
+  const int z = p->z;
+  const long n = (long)p->nb * z;
+  const long ecount = (long)p->cols.size() * z;
+  const int C = std::max(app_clamp, 0);
+  for (long i = 0; i < ecount; ++i) edge_r[i] = 0;
+  for (long i = 0; i < n; ++i) app[i] = (int16_t)std::min(std::max((int)app[i], -C), C);
+  std::vector<int8_t> q((size_t)std::max(p->maxdeg, 1) * z), m1(z), m2(z);
+  std::vector<uint8_t> sx(z);
+  long used = 0;
+  for (long it = 0; it < iterations; ++it) {
+    ++used;
+    for (int l = 0; l < p->mb; ++l) {
+      const int lb = p->layer_off[l], deg = p->layer_off[l + 1] - lb;
+      for (int e = 0; e < deg; ++e) {
+        const int vb = p->cols[lb + e] * z, sh = p->shifts[lb + e];
+        const int8_t* r = edge_r + (long)(lb + e) * z;
+        for (int zi = 0; zi < z; ++zi) {
+          int d = (int)app[vb + rot(zi, sh, z)] - (int)r[zi];
+          q[e * z + zi] = (int8_t)std::min(std::max(d, -127), 127);
+        }
+      }
+      for (int zi = 0; zi < z; ++zi) {
+        m1[zi] = 127;
+        m2[zi] = 127;
+        sx[zi] = 0;
+      }
+      for (int e = 0; e < deg; ++e)
+        for (int zi = 0; zi < z; ++zi) {
+          int8_t qq = q[e * z + zi];
+          int8_t a = (int8_t)(qq < 0 ? -qq : qq);
+          sx[zi] ^= (uint8_t)qq & 0x80u;
+          int8_t mm1 = m1[zi];
+          m1[zi] = std::min(mm1, a);
+          m2[zi] = std::min(m2[zi], std::max(mm1, a));
+        }
+      if (deg < 2)
+        for (int zi = 0; zi < z; ++zi) {
+          if (deg == 0) m1[zi] = 0;
+          m2[zi] = m1[zi];
+        }
+      for (int e = 0; e < deg; ++e) {
+        const int vb = p->cols[lb + e] * z, sh = p->shifts[lb + e];
+        int8_t* r = edge_r + (long)(lb + e) * z;
+        for (int zi = 0; zi < z; ++zi) {
+          int8_t qq = q[e * z + zi];
+          int8_t a = (int8_t)(qq < 0 ? -qq : qq);
+          uint8_t sgn = sx[zi] ^ ((uint8_t)qq & 0x80u);
+          int8_t mex = (a == m1[zi]) ? m2[zi] : m1[zi];
+          int8_t mag = (int8_t)std::max(mex - beta_q, 0);
+          int8_t neg = (int8_t)((int8_t)sgn >> 7);
+          int8_t nr = (int8_t)((int8_t)(mag ^ neg) - neg);
+          int8_t orr = r[zi];
+          r[zi] = nr;
+          int delta = (int)nr - (int)orr;
+          int16_t* dst = &app[vb + rot(zi, sh, z)];
+          int v = (int)*dst + delta;
+          v = std::min(std::max(v, -32768), 32767);  // i16 saturating add
+          *dst = (int16_t)std::min(std::max(v, -C), C);
+        }
+      }
+    }
+    if (syndrome_ok_i16(p, app)) break;
+  }
+  for (long i = 0; i < n; ++i) hard[i] = app[i] < 0 ? 1 : 0;
+  return used;
+}
+
+// syndrome src/qc_ldpc.rs:1496-1513.
+void orc_prologue_5g_i8(const void* h, int16_t* app, long n_filler, int app_clamp) {
+  const Params* p = static_cast<const Params*>(h);
+  const long z = p->z, k = (long)(p->nb - p->mb) * z;
+  const long kp = n_filler > k ? 0 : k - n_filler;
+  const int16_t fill = (int16_t)std::max(app_clamp, 0);
+  for (long i = kp; i < k; ++i) app[i] = fill;
+  for (long i = 0; i < 2 * z; ++i) app[i] = 0;
+}
+
+// syndrome src/quantize.rs:298-305.
+int orc_beta_q(float beta, float scale) {
+  float s = beta * scale;
+  if (!std::isfinite(s)) return 127;
+  float r = roundf(s);
+  r = std::min(std::max(r, 0.0f), 127.0f);
+  return (int)r;
+}
+
+// syndrome src/quantize.rs:331-343.
+void orc_quantize_i16(const float* llr, int16_t* out, long n, float scale) {
+  for (long i = 0; i < n; ++i) {
+    float v = llr[i] * scale;
+    if (std::isnan(v)) {
+      out[i] = 0;
+      continue;
+    }
+    float r = roundf(v);
+    out[i] = (int16_t)(r >= 127.0f ? 127 : (r <= -127.0f ? -127 : (int)r));
+  }
+}
+
+// ------------------------------------------------------------------ encode --
+// Returns 0 on success, -1 if the parity part is singular.
+int orc_encode(void* h, const uint8_t* info, uint8_t* cw) {
+  Params* p = static_cast<Params*>(h);
+  ensure_encoder(p);
+  const int z = p->z, kb = p->nb - p->mb, k = kb * z, m = p->mb * z;
+  for (int i = 0; i < k; ++i) cw[i] = info[i] & 1;
+  if (p->enc_kind == 1) {
+    encode_sparse(p, cw);
+    return 0;
+  }
+  if (p->enc_kind != 2) return -1;
+  const int gw = (k + 63) / 64;
+  std::vector<uint64_t> sys(gw, 0);
+  for (int j = 0; j < k; ++j)
+    if (cw[j]) sys[j >> 6] |= 1ull << (j & 63);
+  for (int i = 0; i < m; ++i) {
+    uint64_t acc = 0;
+    for (int w = 0; w < gw; ++w) acc ^= (uint64_t)__builtin_popcountll(p->gen[i][w] & sys[w]);
+    cw[k + i] = (uint8_t)(acc & 1);
+  }
+  return 0;
+}
+
+int orc_encoder_is_sparse(void* h) {
+  Params* p = static_cast<Params*>(h);
+  ensure_encoder(p);
+  return p->enc_kind == 1;
+}
+
+// Parity check of a hard-decision vector: 1 if H*c = 0.
+int orc_check_codeword(const void* h, const uint8_t* bits) {
+  const Params* p = static_cast<const Params*>(h);
+  const int z = p->z;
+  for (int l = 0; l < p->mb; ++l)
+    for (int zi = 0; zi < z; ++zi) {
+      unsigned par = 0;
+      for (int e = p->layer_off[l]; e < p->layer_off[l + 1]; ++e)
+        par ^= bits[p->cols[e] * z + rot(zi, p->shifts[e], z)] & 1u;
+      if (par) return 0;
+    }
+  return 1;
+}
+
+// ----------------------------------------------------------------- channel --
+// syndrome src/channel_sim.rs:139-150 and :204-221.
+float orc_awgn_sigma(float ebno_db, float rate) {
+  float lin = powf(10.0f, ebno_db / 10.0f);
+  return sqrtf(1.0f / (2.0f * rate * lin));
+}
+
+void orc_awgn_transmit(float ebno_db, float rate, uint64_t seed, const uint8_t* bits, long n,
+                       float* out) {
+  uint64_t st = splitmix64(seed);
+  float sigma = orc_awgn_sigma(ebno_db, rate);
+  float scale = 2.0f / (sigma * sigma);
+  for (long i = 0; i < n; ++i) {
+    float x = bits[i] == 0 ? 1.0f : -1.0f;
+    float g = next_gaussian(&st);
+    float r = x + g * sigma;
+    out[i] = r * scale;
+  }
+}
+
+// FNV-1a over hard decisions (syndrome src/bin/ldpc_bench_export.rs:44-51).
+uint64_t orc_fnv1a_hard(const uint8_t* hard, long n) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  for (long i = 0; i < n; ++i) {
+    h ^= (uint64_t)(hard[i] & 1);
+    h *= 0x00000100000001b3ull;
+  }
+  return h;
+}
+
+}  // extern "C"

@@ -1,0 +1,181 @@
+"""ctypes binding of the oracle (oracle/liboracle.so): a CPU restatement of the
+reference's decode path used only by the tests as the checker.  Nothing in the
+decoder package imports this module."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+_LIB = None
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(ORACLE_DIR, "liboracle.so")
+        src = os.path.join(ORACLE_DIR, "oracle.cpp")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            subprocess.check_call(["make", "-s", "-C", ORACLE_DIR, "liboracle.so"])
+        L = ctypes.CDLL(path)
+        L.orc_params_5g.restype = ctypes.c_void_p
+        L.orc_params_5g.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.orc_params_wifi.restype = ctypes.c_void_p
+        L.orc_params_wifi.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.orc_params_raw.restype = ctypes.c_void_p
+        L.orc_params_raw.argtypes = [_c_int_p, _c_int_p, _c_int_p] + [ctypes.c_int] * 4
+        L.orc_params_free.argtypes = [ctypes.c_void_p]
+        L.orc_params_info.argtypes = [ctypes.c_void_p, _c_int_p]
+        L.orc_params_layout.argtypes = [ctypes.c_void_p, _c_int_p, _c_int_p, _c_int_p]
+        L.orc_decode_f32.restype = ctypes.c_long
+        L.orc_decode_f32.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p]
+        L.orc_init_5g_f32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long]
+        L.orc_decode_i8.restype = ctypes.c_long
+        L.orc_decode_i8.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long]
+        L.orc_prologue_5g_i8.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_int]
+        L.orc_beta_q.restype = ctypes.c_int
+        L.orc_beta_q.argtypes = [ctypes.c_float, ctypes.c_float]
+        L.orc_quantize_i16.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_float]
+        L.orc_encode.restype = ctypes.c_int
+        L.orc_encode.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_encoder_is_sparse.restype = ctypes.c_int
+        L.orc_encoder_is_sparse.argtypes = [ctypes.c_void_p]
+        L.orc_check_codeword.restype = ctypes.c_int
+        L.orc_check_codeword.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_awgn_sigma.restype = ctypes.c_float
+        L.orc_awgn_sigma.argtypes = [ctypes.c_float, ctypes.c_float]
+        L.orc_awgn_transmit.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_uint64,
+                                        ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p]
+        L.orc_fnv1a_hard.restype = ctypes.c_uint64
+        L.orc_fnv1a_hard.argtypes = [ctypes.c_void_p, ctypes.c_long]
+        _LIB = L
+    return _LIB
+
+
+class Code:
+    """One expanded QC-LDPC code in the oracle (reference QcLdpcParams)."""
+
+    def __init__(self, handle):
+        if not handle:
+            raise ValueError("invalid code parameters")
+        self.h = handle
+        info = np.zeros(8, dtype=np.int32)
+        lib().orc_params_info(self.h, _ptr(info, ctypes.c_int))
+        self.mb, self.nb, self.z, self.edges, self.maxdeg, self.n, self.k, self.m = [int(x) for x in info]
+
+    @classmethod
+    def nr(cls, bg, z):
+        return cls(lib().orc_params_5g(bg, z))
+
+    @classmethod
+    def wifi(cls, z, rn, rd):
+        return cls(lib().orc_params_wifi(z, rn, rd))
+
+    def __del__(self):
+        try:
+            lib().orc_params_free(self.h)
+        except Exception:
+            pass
+
+    def layout(self):
+        lo = np.zeros(self.mb + 1, dtype=np.int32)
+        c = np.zeros(self.edges, dtype=np.int32)
+        s = np.zeros(self.edges, dtype=np.int32)
+        lib().orc_params_layout(self.h, _ptr(lo, ctypes.c_int), _ptr(c, ctypes.c_int), _ptr(s, ctypes.c_int))
+        return lo, c, s
+
+    def encode(self, info):
+        info = np.ascontiguousarray(info, dtype=np.uint8)
+        assert info.size == self.k
+        cw = np.zeros(self.n, dtype=np.uint8)
+        rc = lib().orc_encode(self.h, info.ctypes.data, cw.ctypes.data)
+        assert rc == 0
+        return cw
+
+    def is_sparse_encoder(self):
+        return bool(lib().orc_encoder_is_sparse(self.h))
+
+    def check(self, bits):
+        bits = np.ascontiguousarray(bits, dtype=np.uint8)
+        return bool(lib().orc_check_codeword(self.h, bits.ctypes.data))
+
+    def decode_f32(self, llr, beta, iterations, trace=False):
+        llr = np.array(llr, dtype=np.float32, copy=True)
+        edge_r = np.zeros(self.edges * self.z, dtype=np.float32)
+        hard = np.zeros(self.n, dtype=np.uint8)
+        tr = np.zeros((max(iterations, 1), self.n), dtype=np.uint8) if trace else None
+        used = lib().orc_decode_f32(self.h, beta, llr.ctypes.data, edge_r.ctypes.data, hard.ctypes.data,
+                                    iterations, tr.ctypes.data if trace else None)
+        out = dict(iters=int(used), llr=llr, edge_r=edge_r, hard=hard)
+        if trace:
+            out["trace"] = tr[:used]
+        return out
+
+    def init_5g_f32(self, llr, n_filler):
+        llr = np.array(llr, dtype=np.float32, copy=True)
+        lib().orc_init_5g_f32(self.h, llr.ctypes.data, n_filler)
+        return llr
+
+    def decode_i8(self, app, beta_q, iterations, app_clamp=32767):
+        app = np.array(app, dtype=np.int16, copy=True)
+        edge_r = np.zeros(self.edges * self.z, dtype=np.int8)
+        hard = np.zeros(self.n, dtype=np.uint8)
+        used = lib().orc_decode_i8(self.h, beta_q, app_clamp, app.ctypes.data, edge_r.ctypes.data,
+                                   hard.ctypes.data, iterations)
+        return dict(iters=int(used), app=app, edge_r=edge_r, hard=hard)
+
+    def prologue_5g_i8(self, app, n_filler, app_clamp=32767):
+        app = np.array(app, dtype=np.int16, copy=True)
+        lib().orc_prologue_5g_i8(self.h, app.ctypes.data, n_filler, app_clamp)
+        return app
+
+
+def beta_q(beta, scale=8.0):
+    return int(lib().orc_beta_q(beta, scale))
+
+
+def quantize_i16(llr, scale=8.0):
+    llr = np.ascontiguousarray(llr, dtype=np.float32)
+    out = np.zeros(llr.size, dtype=np.int16)
+    lib().orc_quantize_i16(llr.ctypes.data, out.ctypes.data, llr.size, scale)
+    return out
+
+
+def awgn(bits, ebno_db, rate, seed):
+    bits = np.ascontiguousarray(bits, dtype=np.uint8)
+    out = np.zeros(bits.size, dtype=np.float32)
+    lib().orc_awgn_transmit(ebno_db, rate, seed, bits.ctypes.data, bits.size, out.ctypes.data)
+    return out
+
+
+def awgn_sigma(ebno_db, rate):
+    return float(lib().orc_awgn_sigma(ebno_db, rate))
+
+
+def fnv1a_hard(hard):
+    hard = np.ascontiguousarray(hard, dtype=np.uint8)
+    return int(lib().orc_fnv1a_hard(hard.ctypes.data, hard.size))
+
+
+def random_bits(seed, n):
+    """xorshift64 bit stream of the reference's int8 equivalence test
+    (tests/ldpc_int8_kernel_equivalence.rs:27-37): bit = (s >> 27) & 1."""
+    s = (seed | 1) & 0xFFFFFFFFFFFFFFFF
+    out = np.zeros(n, dtype=np.uint8)
+    M = 0xFFFFFFFFFFFFFFFF
+    for i in range(n):
+        s ^= (s << 13) & M
+        s ^= s >> 7
+        s ^= (s << 17) & M
+        out[i] = (s >> 27) & 1
+    return out

@@ -1,0 +1,18 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "tests")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+REFERENCE_ROOT = os.environ.get("SYNDROME_REFERENCE_ROOT", "/root/reference")
+HAVE_REFERENCE = os.path.isdir(os.path.join(REFERENCE_ROOT, "src"))
+needs_reference = pytest.mark.skipif(not HAVE_REFERENCE, reason="reference source tree not present")
