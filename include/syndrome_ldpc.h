@@ -1,0 +1,203 @@
+/*
+ * syndrome_ldpc.h - C ABI of the B200 QC-LDPC layered offset min-sum decoder.
+ *
+ * Three groups of entry points:
+ *
+ *  1. The drop-in set.  Same symbol names, argument order, argument meaning,
+ *     buffer ownership and status codes as the reference's C ABI crate
+ *     (syndrome capi/src/lib.rs); each declaration cites the function it
+ *     replaces.  Buffers are host memory owned by the caller; the decode runs
+ *     on the current CUDA device and returns when the results are in the
+ *     caller's buffers.
+ *  2. The rest of the reference's Rust decoder API (src/qc_ldpc.rs,
+ *     src/wifi_ldpc_tables.rs, src/quantize.rs, src/channel_sim.rs) as C
+ *     functions, so a Rust shim can keep QcLdpcDecoder's method set.
+ *  3. The batched device API: device pointers, a caller-supplied CUDA stream,
+ *     many codewords per call, packed hard decisions.  This is the GPU-native
+ *     path the drop-in set is built on; it has no counterpart in the reference
+ *     (which decodes one codeword per call on one CPU thread).
+ *
+ * Status codes are the reference's SyndromeStatus (capi/src/lib.rs:73-94) plus
+ * SYNDROME_CUDA_ERROR.  No function allocates on the decode path except the
+ * host-buffer wrappers of group 1/2, which keep per-handle device staging
+ * buffers (allocated on first use, reused, freed by *_destroy).
+ */
+#ifndef SYNDROME_LDPC_H
+#define SYNDROME_LDPC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* SyndromeStatus, capi/src/lib.rs:73-94. */
+#define SYNDROME_OK 0
+#define SYNDROME_INVALID_PARAM (-1)
+#define SYNDROME_CRC_MISMATCH (-2)
+#define SYNDROME_DECODER_NOT_CONVERGED (-3) /* reserved, never returned (as in the reference) */
+#define SYNDROME_BUFFER_TOO_SMALL (-4)
+#define SYNDROME_NULL_POINTER (-5)
+#define SYNDROME_PANIC (-6)                 /* an internal C++ exception was caught */
+#define SYNDROME_CUDA_ERROR (-7)            /* no counterpart in the reference: a CUDA call failed */
+
+/* Precision selector of the batched API. */
+#define SYNDROME_PRECISION_INT8 0
+#define SYNDROME_PRECISION_F32 1
+
+typedef struct SyndromeLdpcDecoder SyndromeLdpcDecoder;
+typedef struct SyndromeLdpcEncoder SyndromeLdpcEncoder;
+
+/* ===================================================== 1. drop-in set ===== */
+
+/* capi/src/lib.rs:148 syndrome_ldpc_decoder_create.  base_graph 0 = BG1, 1 = BG2;
+ * z must be a 3GPP lifting size.  *out_decoder is set to NULL on failure. */
+int32_t syndrome_ldpc_decoder_create(int32_t base_graph, size_t z, float offset_beta,
+                                     SyndromeLdpcDecoder** out_decoder);
+/* capi/src/lib.rs:187.  NULL is a no-op. */
+void syndrome_ldpc_decoder_destroy(SyndromeLdpcDecoder* decoder);
+/* capi/src/lib.rs:202 (N = n_b * Z). */
+size_t syndrome_ldpc_decoder_variable_node_count(const SyndromeLdpcDecoder* decoder);
+/* capi/src/lib.rs:216 (K = k_b * Z, filler bits included). */
+size_t syndrome_ldpc_decoder_info_bit_count(const SyndromeLdpcDecoder* decoder);
+/* capi/src/lib.rs:230 (edges * Z). */
+size_t syndrome_ldpc_decoder_required_edge_buffer(const SyndromeLdpcDecoder* decoder);
+/* capi/src/lib.rs:245 (max layer degree * Z). */
+size_t syndrome_ldpc_decoder_required_layer_buffer(const SyndromeLdpcDecoder* decoder);
+/* capi/src/lib.rs:290 syndrome_ldpc_decode_5g -> QcLdpcDecoder::decode_5g
+ * (src/qc_ldpc.rs:644): 5G prologue on llr (filler = 1e6, [0,2Z) = 0), then f32
+ * LOMS.  llr becomes the posterior, edge_r the final C->V messages, hard the hard
+ * decisions.  llr_len and hard_output_len must equal N (INVALID_PARAM); edge_r and
+ * layer_scratch must hold at least the required sizes (BUFFER_TOO_SMALL).
+ * layer_scratch is validated but not written. */
+int32_t syndrome_ldpc_decode_5g(SyndromeLdpcDecoder* decoder, float* llr, size_t llr_len,
+                                size_t n_filler, float* edge_r, size_t edge_r_len,
+                                float* layer_scratch, size_t layer_scratch_len,
+                                uint8_t* hard_output, size_t hard_output_len, size_t iterations,
+                                size_t* out_iterations_used);
+/* capi/src/lib.rs:369. */
+int32_t syndrome_ldpc_encoder_create(int32_t base_graph, size_t z,
+                                     SyndromeLdpcEncoder** out_encoder);
+/* capi/src/lib.rs:407.  NULL is a no-op. */
+void syndrome_ldpc_encoder_destroy(SyndromeLdpcEncoder* encoder);
+/* capi/src/lib.rs:422. */
+size_t syndrome_ldpc_encoder_info_bit_count(const SyndromeLdpcEncoder* encoder);
+/* capi/src/lib.rs:436. */
+size_t syndrome_ldpc_encoder_codeword_bit_count(const SyndromeLdpcEncoder* encoder);
+/* capi/src/lib.rs:461 -> QcLdpcEncoder::encode_5g (src/qc_ldpc.rs:2547): info_len
+ * must equal K - n_filler, codeword_len must equal N (BUFFER_TOO_SMALL). */
+int32_t syndrome_ldpc_encode_5g(const SyndromeLdpcEncoder* encoder, const uint8_t* info_bits,
+                                size_t info_len, size_t n_filler, uint8_t* codeword,
+                                size_t codeword_len);
+
+/* ====================================== 2. rest of the reference API ===== */
+
+/* src/wifi_ldpc_tables.rs:521 wifi_ldpc_decoder (802.11, Z in {27,54,81}). */
+int32_t syndrome_ldpc_decoder_create_wifi(size_t z, size_t rate_num, size_t rate_den,
+                                          float offset_beta, SyndromeLdpcDecoder** out_decoder);
+/* src/qc_ldpc.rs:566 QcLdpcDecoder::from_raw_edges.  Literal (row, col, shift)
+ * triples, shift < z <= 384.  Additionally rejects a column that appears twice in
+ * one layer (INVALID_PARAM): the GPU kernels update a layer's variables in
+ * parallel. */
+int32_t syndrome_ldpc_decoder_create_raw(const uint8_t* rows, const uint8_t* cols,
+                                         const int16_t* shifts, size_t n_edges,
+                                         size_t num_row_blocks, size_t num_col_blocks, size_t z,
+                                         float offset_beta, SyndromeLdpcDecoder** out_decoder);
+/* src/qc_ldpc.rs:588 (M = m_b * Z). */
+size_t syndrome_ldpc_decoder_check_node_count(const SyndromeLdpcDecoder* decoder);
+/* Lifting size and block dimensions: out[0..4] = {z, m_b, n_b, edges, max layer degree}. */
+int32_t syndrome_ldpc_decoder_dims(const SyndromeLdpcDecoder* decoder, size_t* out5);
+/* src/qc_ldpc.rs:711 init_5g_llr (host buffer, no GPU work). */
+int32_t syndrome_ldpc_init_5g_llr(const SyndromeLdpcDecoder* decoder, float* llr, size_t llr_len,
+                                  size_t n_filler);
+/* src/qc_ldpc.rs:794 decode_layered_offset_min_sum (f32, no prologue).  Same
+ * buffers and errors as syndrome_ldpc_decode_5g. */
+int32_t syndrome_ldpc_decode(SyndromeLdpcDecoder* decoder, float* llr, size_t llr_len,
+                             float* edge_r, size_t edge_r_len, float* layer_scratch,
+                             size_t layer_scratch_len, uint8_t* hard_output,
+                             size_t hard_output_len, size_t iterations,
+                             size_t* out_iterations_used);
+/* src/qc_ldpc.rs:1345 decode_layered_offset_min_sum_i8: int8 messages, int16
+ * posterior.  QuantParams is passed as (scale, app_clamp) (src/quantize.rs:217);
+ * beta_q = round(offset_beta * scale) clamped to [0,127].  app is clamped to
+ * +-max(app_clamp, 0) on entry and becomes the posterior. */
+int32_t syndrome_ldpc_decode_i8(SyndromeLdpcDecoder* decoder, int16_t* app, size_t app_len,
+                                int8_t* edge_r, size_t edge_r_len, int8_t* layer_scratch,
+                                size_t layer_scratch_len, uint8_t* hard_output,
+                                size_t hard_output_len, size_t iterations, float scale,
+                                int16_t app_clamp, size_t* out_iterations_used);
+/* src/qc_ldpc.rs:1486 decode_5g_i8: filler = max(app_clamp, 0), [0,2Z) = 0, then
+ * the int8 decode. */
+int32_t syndrome_ldpc_decode_5g_i8(SyndromeLdpcDecoder* decoder, int16_t* app, size_t app_len,
+                                   size_t n_filler, int8_t* edge_r, size_t edge_r_len,
+                                   int8_t* layer_scratch, size_t layer_scratch_len,
+                                   uint8_t* hard_output, size_t hard_output_len,
+                                   size_t iterations, float scale, int16_t app_clamp,
+                                   size_t* out_iterations_used);
+/* src/wifi_ldpc_tables.rs:490 wifi_ldpc_encoder. */
+int32_t syndrome_ldpc_encoder_create_wifi(size_t z, size_t rate_num, size_t rate_den,
+                                          SyndromeLdpcEncoder** out_encoder);
+/* src/qc_ldpc.rs:2592 QcLdpcEncoder::encode (info_len == K, codeword_len == N). */
+int32_t syndrome_ldpc_encode(const SyndromeLdpcEncoder* encoder, const uint8_t* info_bits,
+                             size_t info_len, uint8_t* codeword, size_t codeword_len);
+/* Many codewords at once on `threads` host threads (0 = all cores); row strides in bytes. */
+int32_t syndrome_ldpc_encode_batch(const SyndromeLdpcEncoder* encoder, const uint8_t* info_bits,
+                                   size_t info_stride, uint8_t* codewords, size_t codeword_stride,
+                                   size_t count, int32_t threads);
+/* src/quantize.rs:331 quantize_llr_i16. */
+void syndrome_quantize_llr_i16(const float* llr, int16_t* out, size_t n, float scale);
+/* src/quantize.rs:298 QuantParams::beta_q. */
+int32_t syndrome_beta_q(float offset_beta, float scale);
+/* src/channel_sim.rs:139 AwgnChannel::new(ebno_db, rate, seed).transmit(bits). */
+void syndrome_awgn_llr(float ebno_db, float code_rate, uint64_t seed, const uint8_t* bits,
+                       size_t n, float* llr_out);
+/* Batch of AwgnChannel::transmit + quantize to int8: codeword b uses seeds[b] and
+ * ebno_db[b]; bits [tx_begin, n) of row b are written to out + b * out_stride. */
+void syndrome_awgn_quantized_batch(const uint8_t* bits, size_t n, size_t bits_stride,
+                                   size_t tx_begin, const float* ebno_db, float code_rate,
+                                   const uint64_t* seeds, float scale, int8_t* out,
+                                   size_t out_stride, size_t count, int32_t threads);
+
+/* ================================================= 3. batched device API == */
+
+/* Device scratch bytes that syndrome_ldpc_decode_batch_* needs for `batch`
+ * codewords when d_edge_r is NULL. */
+size_t syndrome_ldpc_batch_workspace_size(const SyndromeLdpcDecoder* decoder, int32_t precision,
+                                          size_t batch);
+/* Batched int8 decode.  Codeword b's int8 channel LLRs are
+ * d_llr[b * llr_stride + j] for variables llr_offset + j (j < N - llr_offset);
+ * variables [0, llr_offset) start at 0.  nr_prologue != 0 applies decode_5g_i8's
+ * initialisation.  Outputs (all device memory, each optional):
+ *   d_hard_packed[b * hard_words_stride + w]: bit t of word w = hard decision of
+ *     variable 32w + t, for the first hard_bits variables;
+ *   d_iters[b]: iterations used (early stop on a zero syndrome);
+ *   d_app[b * app_stride + i]: final int16 posterior;
+ *   d_edge_r[b * edge_r_stride + e]: final C->V messages (reference layout);
+ *   d_hard[b * hard_stride + i]: hard decisions, one byte per variable.
+ * Enqueued on `stream` (a cudaStream_t; NULL = legacy default stream). */
+int32_t syndrome_ldpc_decode_batch_i8(const SyndromeLdpcDecoder* decoder, const int8_t* d_llr,
+                                      size_t llr_stride, size_t llr_offset, size_t batch,
+                                      int32_t nr_prologue, size_t n_filler, size_t iterations,
+                                      float scale, int16_t app_clamp, uint32_t* d_hard_packed,
+                                      size_t hard_bits, size_t hard_words_stride, int32_t* d_iters,
+                                      int16_t* d_app, size_t app_stride, int8_t* d_edge_r,
+                                      size_t edge_r_stride, uint8_t* d_hard, size_t hard_stride,
+                                      void* d_workspace, size_t workspace_bytes, void* stream);
+/* Batched f32 decode (decode_layered_offset_min_sum / decode_5g semantics). */
+int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const float* d_llr,
+                                       size_t llr_stride, size_t llr_offset, size_t batch,
+                                       int32_t nr_prologue, size_t n_filler, size_t iterations,
+                                       uint32_t* d_hard_packed, size_t hard_bits,
+                                       size_t hard_words_stride, int32_t* d_iters, float* d_app,
+                                       size_t app_stride, float* d_edge_r, size_t edge_r_stride,
+                                       uint8_t* d_hard, size_t hard_stride, void* d_workspace,
+                                       size_t workspace_bytes, void* stream);
+/* Text of the last error on this thread (empty if none). */
+const char* syndrome_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SYNDROME_LDPC_H */

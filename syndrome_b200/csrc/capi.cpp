@@ -1,0 +1,522 @@
+// extern "C" boundary of libsyndrome_b200.so (declarations: include/syndrome_ldpc.h).
+//
+// Group 1 mirrors syndrome capi/src/lib.rs function by function: same null checks
+// first, then the same validation order as the Rust entry points it wraps, the same
+// status codes, and a catch-all guard that reports an internal exception as
+// SYNDROME_PANIC (the reference's catch_unwind guard, capi/src/lib.rs:113-115).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <exception>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/syndrome_ldpc.h"
+#include "channel.h"
+#include "decoder.h"
+#include "encoder.h"
+#include "graph.h"
+
+struct SyndromeLdpcDecoder {
+  syn::Graph graph;
+  syn::Decoder dec;
+  std::mutex mu;  // serialises the host-buffer wrappers that share the staging buffers
+  void* staging = nullptr;
+  size_t staging_bytes = 0;
+  ~SyndromeLdpcDecoder() {
+    if (staging) cudaFree(staging);
+  }
+};
+
+struct SyndromeLdpcEncoder {
+  syn::Encoder enc;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int32_t guard(F&& body) {
+  try {
+    return body();
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return SYNDROME_PANIC;
+  } catch (...) {
+    g_last_error = "unknown exception";
+    return SYNDROME_PANIC;
+  }
+}
+
+int32_t fail(int32_t code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int32_t from_cuda(cudaError_t e, const std::string& msg) {
+  if (e == cudaSuccess) return SYNDROME_OK;
+  if (e == cudaErrorInvalidValue && !msg.empty()) {
+    const bool small = msg.find("workspace") != std::string::npos;
+    return fail(small ? SYNDROME_BUFFER_TOO_SMALL : SYNDROME_INVALID_PARAM, msg);
+  }
+  return fail(SYNDROME_CUDA_ERROR, std::string(cudaGetErrorString(e)) + (msg.empty() ? "" : ": " + msg));
+}
+
+int32_t make_decoder(const syn::Graph& g, float beta, SyndromeLdpcDecoder** out) {
+  auto* d = new SyndromeLdpcDecoder();
+  d->graph = g;
+  std::string err;
+  if (!d->dec.init(g, beta, &err)) {
+    delete d;
+    cudaGetLastError();
+    const bool cuda = err.find("CUDA") != std::string::npos || err.find("cuda") != std::string::npos;
+    return fail(cuda ? SYNDROME_CUDA_ERROR : SYNDROME_INVALID_PARAM, err);
+  }
+  *out = d;
+  return SYNDROME_OK;
+}
+
+// Grows the handle's device staging buffer; caller holds d->mu.
+bool ensure_staging(SyndromeLdpcDecoder* d, size_t bytes) {
+  if (d->staging_bytes >= bytes) return true;
+  if (d->staging) cudaFree(d->staging);
+  d->staging = nullptr;
+  d->staging_bytes = 0;
+  if (cudaMalloc(&d->staging, bytes) != cudaSuccess) return false;
+  d->staging_bytes = bytes;
+  return true;
+}
+
+size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Shared host-buffer path: one codeword, device staging, synchronous.
+// elem: 4 (f32) or 2 (int16 posterior + int8 messages).
+int32_t host_decode(SyndromeLdpcDecoder* d, bool f32, void* app, void* edge_r, uint8_t* hard,
+                    size_t iterations, float scale, int16_t app_clamp, size_t* out_iters) {
+  const syn::Graph& g = d->graph;
+  const size_t n = (size_t)g.n(), ez = (size_t)g.edge_buffer();
+  const size_t app_b = n * (f32 ? 4 : 2), edge_b = ez * (f32 ? 4 : 1);
+  const size_t off_app = 0, off_out = al256(app_b), off_edge = off_out + al256(app_b);
+  const size_t off_hard = off_edge + al256(edge_b), off_it = off_hard + al256(n);
+  const size_t total = off_it + 256;
+  std::lock_guard<std::mutex> lock(d->mu);
+  if (!ensure_staging(d, total)) {
+    cudaGetLastError();
+    return fail(SYNDROME_CUDA_ERROR, "cudaMalloc of the staging buffer failed");
+  }
+  char* base = static_cast<char*>(d->staging);
+  cudaError_t e = cudaMemcpy(base + off_app, app, app_b, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return from_cuda(e, "copy in");
+  syn::BatchRequest r;
+  r.llr = base + off_app;
+  r.llr_i16 = f32 ? 0 : 1;
+  r.llr_stride = (long long)n;
+  r.batch = 1;
+  r.iterations = (int)std::min<size_t>(iterations, INT_MAX);
+  r.beta = d->dec.offset_beta();
+  r.beta_q = syn::beta_q(d->dec.offset_beta(), scale);
+  r.app_clamp = std::max<int>(app_clamp, 0);
+  r.app = base + off_out;
+  r.app_stride = (long long)n;
+  r.edge_r = base + off_edge;
+  r.edge_r_stride = (long long)ez;
+  r.hard = reinterpret_cast<uint8_t*>(base + off_hard);
+  r.hard_stride = (long long)n;
+  r.iters = reinterpret_cast<int32_t*>(base + off_it);
+  std::string msg;
+  e = d->dec.decode(f32 ? syn::Precision::kF32 : syn::Precision::kInt8, r, 0, &msg);
+  if (e != cudaSuccess) return from_cuda(e, msg);
+  int32_t used = 0;
+  if ((e = cudaMemcpy(app, base + off_out, app_b, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(edge_r, base + off_edge, edge_b, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(hard, base + off_hard, n, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(&used, base + off_it, 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return from_cuda(e, "copy out");
+  if (out_iters) *out_iters = (size_t)used;
+  return SYNDROME_OK;
+}
+
+// Validation shared by the f32/int8 host wrappers, in the reference's order
+// (src/qc_ldpc.rs:980-1004 and :1544-1568).
+int32_t validate_buffers(const syn::Graph& g, size_t app_len, size_t hard_len, size_t edge_len,
+                         size_t scratch_len) {
+  if (app_len != (size_t)g.n()) return fail(SYNDROME_INVALID_PARAM, "llr length must equal variable_node_count()");
+  if (hard_len != (size_t)g.n())
+    return fail(SYNDROME_INVALID_PARAM, "hard_output length must equal variable_node_count()");
+  if (edge_len < (size_t)g.edge_buffer()) return fail(SYNDROME_BUFFER_TOO_SMALL, "edge_r too small");
+  if (scratch_len < (size_t)g.layer_buffer())
+    return fail(SYNDROME_BUFFER_TOO_SMALL, "layer_scratch too small");
+  return SYNDROME_OK;
+}
+
+void nr_prologue_f32(const syn::Graph& g, float* llr, size_t n_filler) {
+  const size_t k = (size_t)g.k(), kp = n_filler > k ? 0 : k - n_filler;
+  for (size_t i = kp; i < k; ++i) llr[i] = 1000000.0f;
+  for (size_t i = 0; i < (size_t)(2 * g.z); ++i) llr[i] = 0.0f;
+}
+
+void nr_prologue_i16(const syn::Graph& g, int16_t* app, size_t n_filler, int16_t app_clamp) {
+  const size_t k = (size_t)g.k(), kp = n_filler > k ? 0 : k - n_filler;
+  const int16_t fill = std::max<int16_t>(app_clamp, 0);
+  for (size_t i = kp; i < k; ++i) app[i] = fill;
+  for (size_t i = 0; i < (size_t)(2 * g.z); ++i) app[i] = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* syndrome_last_error(void) { return g_last_error.c_str(); }
+
+// ------------------------------------------------------------- group 1 ------
+
+int32_t syndrome_ldpc_decoder_create(int32_t base_graph, size_t z, float offset_beta,
+                                     SyndromeLdpcDecoder** out_decoder) {
+  return guard([&]() -> int32_t {
+    if (!out_decoder) return SYNDROME_NULL_POINTER;
+    *out_decoder = nullptr;
+    if (base_graph != 0 && base_graph != 1) return fail(SYNDROME_INVALID_PARAM, "base_graph must be 0 (BG1) or 1 (BG2)");
+    syn::Graph g;
+    if (z > 384 || !syn::build_nr_graph(base_graph, (int)z, &g))
+      return fail(SYNDROME_INVALID_PARAM, "z is not a valid 3GPP lifting size");
+    return make_decoder(g, offset_beta, out_decoder);
+  });
+}
+
+void syndrome_ldpc_decoder_destroy(SyndromeLdpcDecoder* decoder) { delete decoder; }
+
+size_t syndrome_ldpc_decoder_variable_node_count(const SyndromeLdpcDecoder* d) {
+  return (size_t)d->graph.n();
+}
+size_t syndrome_ldpc_decoder_info_bit_count(const SyndromeLdpcDecoder* d) { return (size_t)d->graph.k(); }
+size_t syndrome_ldpc_decoder_required_edge_buffer(const SyndromeLdpcDecoder* d) {
+  return (size_t)d->graph.edge_buffer();
+}
+size_t syndrome_ldpc_decoder_required_layer_buffer(const SyndromeLdpcDecoder* d) {
+  return (size_t)d->graph.layer_buffer();
+}
+
+int32_t syndrome_ldpc_decode_5g(SyndromeLdpcDecoder* decoder, float* llr, size_t llr_len,
+                                size_t n_filler, float* edge_r, size_t edge_r_len,
+                                float* layer_scratch, size_t layer_scratch_len,
+                                uint8_t* hard_output, size_t hard_output_len, size_t iterations,
+                                size_t* out_iterations_used) {
+  return guard([&]() -> int32_t {
+    if (!decoder || !llr || !edge_r || !layer_scratch || !hard_output) return SYNDROME_NULL_POINTER;
+    const syn::Graph& g = decoder->graph;
+    if (llr_len != (size_t)g.n()) return fail(SYNDROME_INVALID_PARAM, "llr length must equal variable_node_count()");
+    nr_prologue_f32(g, llr, n_filler);  // init_5g_llr runs before the decode validates
+    int32_t st = validate_buffers(g, llr_len, hard_output_len, edge_r_len, layer_scratch_len);
+    if (st != SYNDROME_OK) return st;
+    return host_decode(decoder, true, llr, edge_r, hard_output, iterations, 8.0f, 0, out_iterations_used);
+  });
+}
+
+int32_t syndrome_ldpc_encoder_create(int32_t base_graph, size_t z, SyndromeLdpcEncoder** out) {
+  return guard([&]() -> int32_t {
+    if (!out) return SYNDROME_NULL_POINTER;
+    *out = nullptr;
+    if (base_graph != 0 && base_graph != 1) return fail(SYNDROME_INVALID_PARAM, "base_graph must be 0 (BG1) or 1 (BG2)");
+    syn::Graph g;
+    if (z > 384 || !syn::build_nr_graph(base_graph, (int)z, &g))
+      return fail(SYNDROME_INVALID_PARAM, "z is not a valid 3GPP lifting size");
+    auto* e = new SyndromeLdpcEncoder();
+    if (!e->enc.init(g)) {
+      delete e;
+      return fail(SYNDROME_INVALID_PARAM, "parity matrix is singular - cannot encode");
+    }
+    *out = e;
+    return SYNDROME_OK;
+  });
+}
+
+void syndrome_ldpc_encoder_destroy(SyndromeLdpcEncoder* encoder) { delete encoder; }
+
+size_t syndrome_ldpc_encoder_info_bit_count(const SyndromeLdpcEncoder* e) {
+  return (size_t)e->enc.graph().k();
+}
+size_t syndrome_ldpc_encoder_codeword_bit_count(const SyndromeLdpcEncoder* e) {
+  return (size_t)e->enc.graph().n();
+}
+
+int32_t syndrome_ldpc_encode_5g(const SyndromeLdpcEncoder* encoder, const uint8_t* info_bits,
+                                size_t info_len, size_t n_filler, uint8_t* codeword,
+                                size_t codeword_len) {
+  return guard([&]() -> int32_t {
+    if (!encoder || !info_bits || !codeword) return SYNDROME_NULL_POINTER;
+    const syn::Graph& g = encoder->enc.graph();
+    const size_t k = (size_t)g.k();
+    if (n_filler > k) return fail(SYNDROME_INVALID_PARAM, "n_filler exceeds k_bits");
+    if (info_len != k - n_filler) return fail(SYNDROME_BUFFER_TOO_SMALL, "info length must equal K - n_filler");
+    if (codeword_len != (size_t)g.n()) return fail(SYNDROME_BUFFER_TOO_SMALL, "codeword length must equal N");
+    std::vector<uint8_t> full(k, 0);
+    std::memcpy(full.data(), info_bits, info_len);
+    encoder->enc.encode(full.data(), codeword);
+    return SYNDROME_OK;
+  });
+}
+
+// ------------------------------------------------------------- group 2 ------
+
+int32_t syndrome_ldpc_decoder_create_wifi(size_t z, size_t rate_num, size_t rate_den,
+                                          float offset_beta, SyndromeLdpcDecoder** out_decoder) {
+  return guard([&]() -> int32_t {
+    if (!out_decoder) return SYNDROME_NULL_POINTER;
+    *out_decoder = nullptr;
+    syn::Graph g;
+    if (z > 384 || rate_num > 16 || rate_den > 16 || !syn::build_wifi_graph((int)z, (int)rate_num, (int)rate_den, &g))
+      return fail(SYNDROME_INVALID_PARAM, "z/rate is not one of the 12 supported 802.11 LDPC (Z, R) combinations");
+    return make_decoder(g, offset_beta, out_decoder);
+  });
+}
+
+int32_t syndrome_ldpc_decoder_create_raw(const uint8_t* rows, const uint8_t* cols,
+                                         const int16_t* shifts, size_t n_edges,
+                                         size_t num_row_blocks, size_t num_col_blocks, size_t z,
+                                         float offset_beta, SyndromeLdpcDecoder** out_decoder) {
+  return guard([&]() -> int32_t {
+    if (!out_decoder) return SYNDROME_NULL_POINTER;
+    *out_decoder = nullptr;
+    if (n_edges > 0 && (!rows || !cols || !shifts)) return SYNDROME_NULL_POINTER;
+    if (n_edges > 65536 || num_row_blocks > 255 || num_col_blocks > 255 || z > 384)
+      return fail(SYNDROME_INVALID_PARAM, "dimensions out of range");
+    std::vector<int> r(n_edges), c(n_edges), s(n_edges);
+    for (size_t i = 0; i < n_edges; ++i) {
+      r[i] = rows[i];
+      c[i] = cols[i];
+      s[i] = shifts[i];
+    }
+    syn::Graph g;
+    std::string err;
+    if (!syn::build_raw_graph(r.data(), c.data(), s.data(), (int)n_edges, (int)num_row_blocks,
+                              (int)num_col_blocks, (int)z, &g, &err))
+      return fail(SYNDROME_INVALID_PARAM, err);
+    return make_decoder(g, offset_beta, out_decoder);
+  });
+}
+
+size_t syndrome_ldpc_decoder_check_node_count(const SyndromeLdpcDecoder* d) { return (size_t)d->graph.m(); }
+
+int32_t syndrome_ldpc_decoder_dims(const SyndromeLdpcDecoder* d, size_t* out5) {
+  if (!d || !out5) return SYNDROME_NULL_POINTER;
+  out5[0] = (size_t)d->graph.z;
+  out5[1] = (size_t)d->graph.mb;
+  out5[2] = (size_t)d->graph.nb;
+  out5[3] = (size_t)d->graph.edges();
+  out5[4] = (size_t)d->graph.maxdeg;
+  return SYNDROME_OK;
+}
+
+int32_t syndrome_ldpc_init_5g_llr(const SyndromeLdpcDecoder* decoder, float* llr, size_t llr_len,
+                                  size_t n_filler) {
+  return guard([&]() -> int32_t {
+    if (!decoder || !llr) return SYNDROME_NULL_POINTER;
+    if (llr_len != (size_t)decoder->graph.n())
+      return fail(SYNDROME_INVALID_PARAM, "llr length must equal variable_node_count()");
+    nr_prologue_f32(decoder->graph, llr, n_filler);
+    return SYNDROME_OK;
+  });
+}
+
+int32_t syndrome_ldpc_decode(SyndromeLdpcDecoder* decoder, float* llr, size_t llr_len,
+                             float* edge_r, size_t edge_r_len, float* layer_scratch,
+                             size_t layer_scratch_len, uint8_t* hard_output,
+                             size_t hard_output_len, size_t iterations,
+                             size_t* out_iterations_used) {
+  return guard([&]() -> int32_t {
+    if (!decoder || !llr || !edge_r || !layer_scratch || !hard_output) return SYNDROME_NULL_POINTER;
+    int32_t st = validate_buffers(decoder->graph, llr_len, hard_output_len, edge_r_len, layer_scratch_len);
+    if (st != SYNDROME_OK) return st;
+    return host_decode(decoder, true, llr, edge_r, hard_output, iterations, 8.0f, 0, out_iterations_used);
+  });
+}
+
+int32_t syndrome_ldpc_decode_i8(SyndromeLdpcDecoder* decoder, int16_t* app, size_t app_len,
+                                int8_t* edge_r, size_t edge_r_len, int8_t* layer_scratch,
+                                size_t layer_scratch_len, uint8_t* hard_output,
+                                size_t hard_output_len, size_t iterations, float scale,
+                                int16_t app_clamp, size_t* out_iterations_used) {
+  return guard([&]() -> int32_t {
+    if (!decoder || !app || !edge_r || !layer_scratch || !hard_output) return SYNDROME_NULL_POINTER;
+    int32_t st = validate_buffers(decoder->graph, app_len, hard_output_len, edge_r_len, layer_scratch_len);
+    if (st != SYNDROME_OK) return st;
+    return host_decode(decoder, false, app, edge_r, hard_output, iterations, scale, app_clamp,
+                       out_iterations_used);
+  });
+}
+
+int32_t syndrome_ldpc_decode_5g_i8(SyndromeLdpcDecoder* decoder, int16_t* app, size_t app_len,
+                                   size_t n_filler, int8_t* edge_r, size_t edge_r_len,
+                                   int8_t* layer_scratch, size_t layer_scratch_len,
+                                   uint8_t* hard_output, size_t hard_output_len,
+                                   size_t iterations, float scale, int16_t app_clamp,
+                                   size_t* out_iterations_used) {
+  return guard([&]() -> int32_t {
+    if (!decoder || !app || !edge_r || !layer_scratch || !hard_output) return SYNDROME_NULL_POINTER;
+    if (app_len != (size_t)decoder->graph.n())
+      return fail(SYNDROME_INVALID_PARAM, "app length must equal variable_node_count()");
+    nr_prologue_i16(decoder->graph, app, n_filler, app_clamp);
+    int32_t st = validate_buffers(decoder->graph, app_len, hard_output_len, edge_r_len, layer_scratch_len);
+    if (st != SYNDROME_OK) return st;
+    return host_decode(decoder, false, app, edge_r, hard_output, iterations, scale, app_clamp,
+                       out_iterations_used);
+  });
+}
+
+int32_t syndrome_ldpc_encoder_create_wifi(size_t z, size_t rate_num, size_t rate_den,
+                                          SyndromeLdpcEncoder** out) {
+  return guard([&]() -> int32_t {
+    if (!out) return SYNDROME_NULL_POINTER;
+    *out = nullptr;
+    syn::Graph g;
+    if (z > 384 || rate_num > 16 || rate_den > 16 || !syn::build_wifi_graph((int)z, (int)rate_num, (int)rate_den, &g))
+      return fail(SYNDROME_INVALID_PARAM, "z/rate is not one of the 12 supported 802.11 LDPC (Z, R) combinations");
+    auto* e = new SyndromeLdpcEncoder();
+    if (!e->enc.init(g)) {
+      delete e;
+      return fail(SYNDROME_INVALID_PARAM, "parity matrix is singular - cannot encode");
+    }
+    *out = e;
+    return SYNDROME_OK;
+  });
+}
+
+int32_t syndrome_ldpc_encode(const SyndromeLdpcEncoder* encoder, const uint8_t* info_bits,
+                             size_t info_len, uint8_t* codeword, size_t codeword_len) {
+  return guard([&]() -> int32_t {
+    if (!encoder || !info_bits || !codeword) return SYNDROME_NULL_POINTER;
+    const syn::Graph& g = encoder->enc.graph();
+    if (info_len != (size_t)g.k()) return fail(SYNDROME_BUFFER_TOO_SMALL, "info length must equal K");
+    if (codeword_len != (size_t)g.n()) return fail(SYNDROME_BUFFER_TOO_SMALL, "codeword length must equal N");
+    encoder->enc.encode(info_bits, codeword);
+    return SYNDROME_OK;
+  });
+}
+
+int32_t syndrome_ldpc_encode_batch(const SyndromeLdpcEncoder* encoder, const uint8_t* info_bits,
+                                   size_t info_stride, uint8_t* codewords, size_t codeword_stride,
+                                   size_t count, int32_t threads) {
+  return guard([&]() -> int32_t {
+    if (!encoder || ((!info_bits || !codewords) && count)) return SYNDROME_NULL_POINTER;
+    const syn::Graph& g = encoder->enc.graph();
+    if (info_stride < (size_t)g.k() || codeword_stride < (size_t)g.n())
+      return fail(SYNDROME_BUFFER_TOO_SMALL, "row stride smaller than K or N");
+    encoder->enc.encode_batch(info_bits, (long long)info_stride, codewords, (long long)codeword_stride,
+                              (long long)count, threads);
+    return SYNDROME_OK;
+  });
+}
+
+void syndrome_quantize_llr_i16(const float* llr, int16_t* out, size_t n, float scale) {
+  for (size_t i = 0; i < n; ++i) out[i] = syn::quantize_llr_i16(llr[i], scale);
+}
+
+int32_t syndrome_beta_q(float offset_beta, float scale) { return syn::beta_q(offset_beta, scale); }
+
+void syndrome_awgn_llr(float ebno_db, float code_rate, uint64_t seed, const uint8_t* bits, size_t n,
+                       float* llr_out) {
+  syn::awgn_llr(ebno_db, code_rate, seed, bits, (long long)n, llr_out);
+}
+
+void syndrome_awgn_quantized_batch(const uint8_t* bits, size_t n, size_t bits_stride,
+                                   size_t tx_begin, const float* ebno_db, float code_rate,
+                                   const uint64_t* seeds, float scale, int8_t* out,
+                                   size_t out_stride, size_t count, int32_t threads) {
+  syn::awgn_quantized_batch(bits, (long long)n, (long long)bits_stride, (long long)tx_begin, ebno_db,
+                            code_rate, seeds, scale, out, (long long)out_stride, (long long)count,
+                            threads);
+}
+
+// ------------------------------------------------------------- group 3 ------
+
+size_t syndrome_ldpc_batch_workspace_size(const SyndromeLdpcDecoder* decoder, int32_t precision,
+                                          size_t batch) {
+  if (!decoder) return 0;
+  return decoder->dec.workspace_bytes(
+      precision == SYNDROME_PRECISION_F32 ? syn::Precision::kF32 : syn::Precision::kInt8, (long long)batch);
+}
+
+static int32_t batch_common(const SyndromeLdpcDecoder* decoder, syn::Precision p, const void* d_llr,
+                            size_t llr_stride, size_t llr_offset, size_t batch, int32_t nr_prologue,
+                            size_t n_filler, size_t iterations, float scale, int16_t app_clamp,
+                            uint32_t* d_hard_packed, size_t hard_bits, size_t hard_words_stride,
+                            int32_t* d_iters, void* d_app, size_t app_stride, void* d_edge_r,
+                            size_t edge_r_stride, uint8_t* d_hard, size_t hard_stride,
+                            void* d_workspace, size_t workspace_bytes, void* stream) {
+  if (!decoder || (!d_llr && batch)) return SYNDROME_NULL_POINTER;
+  const syn::Graph& g = decoder->graph;
+  const size_t n = (size_t)g.n();
+  if (llr_offset > n) return fail(SYNDROME_INVALID_PARAM, "llr_offset exceeds N");
+  if (llr_stride < n - llr_offset) return fail(SYNDROME_INVALID_PARAM, "llr_stride smaller than N - llr_offset");
+  if (d_app && app_stride < n) return fail(SYNDROME_INVALID_PARAM, "app_stride smaller than N");
+  if (d_hard && hard_stride < n) return fail(SYNDROME_INVALID_PARAM, "hard_stride smaller than N");
+  if (d_edge_r && edge_r_stride < (size_t)g.edge_buffer())
+    return fail(SYNDROME_INVALID_PARAM, "edge_r_stride smaller than the edge buffer");
+  if (d_hard_packed && (hard_bits > n || hard_words_stride < (hard_bits + 31) / 32))
+    return fail(SYNDROME_INVALID_PARAM, "hard_bits / hard_words_stride out of range");
+  if (iterations > (size_t)INT_MAX || batch > (size_t)LLONG_MAX / 2) return fail(SYNDROME_INVALID_PARAM, "size out of range");
+  syn::BatchRequest r;
+  r.llr = d_llr;
+  r.llr_stride = (long long)llr_stride;
+  r.llr_offset = (int)llr_offset;
+  r.batch = (long long)batch;
+  r.iterations = (int)iterations;
+  r.prologue_5g = nr_prologue ? 1 : 0;
+  r.n_filler = (long long)std::min<size_t>(n_filler, (size_t)1 << 40);
+  r.beta = decoder->dec.offset_beta();
+  r.beta_q = syn::beta_q(decoder->dec.offset_beta(), scale);
+  r.app_clamp = std::max<int>(app_clamp, 0);
+  r.hard_packed = d_hard_packed;
+  r.hard_bits = (int)hard_bits;
+  r.hard_words_stride = (long long)hard_words_stride;
+  r.iters = d_iters;
+  r.app = d_app;
+  r.app_stride = (long long)app_stride;
+  r.edge_r = d_edge_r;
+  r.edge_r_stride = (long long)edge_r_stride;
+  r.hard = d_hard;
+  r.hard_stride = (long long)hard_stride;
+  r.workspace = d_workspace;
+  r.workspace_bytes = workspace_bytes;
+  std::string msg;
+  cudaError_t e = decoder->dec.decode(p, r, static_cast<cudaStream_t>(stream), &msg);
+  return from_cuda(e, msg);
+}
+
+int32_t syndrome_ldpc_decode_batch_i8(const SyndromeLdpcDecoder* decoder, const int8_t* d_llr,
+                                      size_t llr_stride, size_t llr_offset, size_t batch,
+                                      int32_t nr_prologue, size_t n_filler, size_t iterations,
+                                      float scale, int16_t app_clamp, uint32_t* d_hard_packed,
+                                      size_t hard_bits, size_t hard_words_stride, int32_t* d_iters,
+                                      int16_t* d_app, size_t app_stride, int8_t* d_edge_r,
+                                      size_t edge_r_stride, uint8_t* d_hard, size_t hard_stride,
+                                      void* d_workspace, size_t workspace_bytes, void* stream) {
+  return guard([&]() -> int32_t {
+    return batch_common(decoder, syn::Precision::kInt8, d_llr, llr_stride, llr_offset, batch,
+                        nr_prologue, n_filler, iterations, scale, app_clamp, d_hard_packed, hard_bits,
+                        hard_words_stride, d_iters, d_app, app_stride, d_edge_r, edge_r_stride, d_hard,
+                        hard_stride, d_workspace, workspace_bytes, stream);
+  });
+}
+
+int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const float* d_llr,
+                                       size_t llr_stride, size_t llr_offset, size_t batch,
+                                       int32_t nr_prologue, size_t n_filler, size_t iterations,
+                                       uint32_t* d_hard_packed, size_t hard_bits,
+                                       size_t hard_words_stride, int32_t* d_iters, float* d_app,
+                                       size_t app_stride, float* d_edge_r, size_t edge_r_stride,
+                                       uint8_t* d_hard, size_t hard_stride, void* d_workspace,
+                                       size_t workspace_bytes, void* stream) {
+  return guard([&]() -> int32_t {
+    return batch_common(decoder, syn::Precision::kF32, d_llr, llr_stride, llr_offset, batch,
+                        nr_prologue, n_filler, iterations, 8.0f, 0, d_hard_packed, hard_bits,
+                        hard_words_stride, d_iters, d_app, app_stride, d_edge_r, edge_r_stride, d_hard,
+                        hard_stride, d_workspace, workspace_bytes, stream);
+  });
+}
+
+}  // extern "C"

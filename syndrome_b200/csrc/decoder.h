@@ -1,0 +1,89 @@
+// Batched GPU layered offset min-sum decoder (host-side interface).
+//
+// The decoder owns a copy of the code's layer tables on the device and launches
+// the sm_100a kernels in ldpc_kernels.cu.  All data buffers are device pointers
+// supplied by the caller; nothing on the decode path allocates.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "graph.h"
+
+namespace syn {
+
+// One batched decode request.  Codeword b's channel LLRs are
+// llr[b * llr_stride + j] for variables llr_offset + j, j in [0, n - llr_offset);
+// variables [0, llr_offset) start as erasures (0).  With prologue_5g the 5G NR
+// initialisation is applied on top: filler positions [K - n_filler, K) are pinned
+// (f32: 1e6, int8: app_clamp) and [0, 2Z) are erased (src/qc_ldpc.rs:711-732,
+// 1496-1513).
+struct BatchRequest {
+  const void* llr = nullptr;      // int8 or int16 (int8 path, see llr_i16) or float (f32 path)
+  int llr_i16 = 0;                // int8 path: input elements are int16 instead of int8
+  long long llr_stride = 0;       // elements between codewords
+  int llr_offset = 0;
+  long long batch = 0;
+  int iterations = 0;
+  int prologue_5g = 0;
+  long long n_filler = 0;
+  // int8 path numerics (src/quantize.rs): beta_q = round(beta * scale) clamped, app clamp.
+  int beta_q = 0;
+  int app_clamp = 32767;
+  // f32 path numerics.
+  float beta = 0.0f;
+  // Outputs (each nullable except where noted).
+  uint32_t* hard_packed = nullptr;   // [batch][hard_words_stride] LSB-first bits of variables [0, hard_bits)
+  int hard_bits = 0;
+  long long hard_words_stride = 0;
+  int32_t* iters = nullptr;          // [batch] iterations used
+  void* app = nullptr;               // [batch][app_stride] final posterior (int16 or float)
+  long long app_stride = 0;
+  uint8_t* hard = nullptr;           // [batch][hard_stride] one byte per variable
+  long long hard_stride = 0;
+  void* edge_r = nullptr;            // [batch][edge_r_stride] final C->V messages, reference layout
+  long long edge_r_stride = 0;
+  // Scratch for C->V messages when edge_r is null.
+  void* workspace = nullptr;
+  size_t workspace_bytes = 0;
+};
+
+enum class Precision { kInt8, kF32 };
+
+class Decoder {
+ public:
+  ~Decoder();
+  // Copies the layer tables to the current device.  Returns false with err set.
+  bool init(const Graph& g, float offset_beta, std::string* err);
+  const Graph& graph() const { return g_; }
+  float offset_beta() const { return beta_; }
+
+  // Scratch bytes the kernel needs for `batch` codewords when edge_r is not given.
+  size_t workspace_bytes(Precision p, long long batch) const;
+
+  // Launches the decode on `stream`.  Returns cudaSuccess or the launch error;
+  // argument errors are reported as cudaErrorInvalidValue with err set.
+  cudaError_t decode(Precision p, const BatchRequest& req, cudaStream_t stream,
+                     std::string* err) const;
+
+  // Kernel launch geometry chosen for this code (exposed for the tuner and tests).
+  struct Geometry {
+    int cpb;          // codewords per CTA
+    int threads;      // threads per CTA
+    int smem;         // dynamic shared memory bytes
+    int max_ctas;     // resident CTAs on the device
+    int maxdeg_tmpl;  // kernel instantiation
+  };
+  Geometry geometry(Precision p, long long batch) const;
+
+ private:
+  Graph g_;
+  float beta_ = 0.0f;
+  int device_ = -1;
+  uint32_t* d_edge_ = nullptr;   // [E] (col * z) << 16 | shift
+  int32_t* d_loff_ = nullptr;    // [mb + 1]
+};
+
+}  // namespace syn

@@ -1,0 +1,542 @@
+// Batched layered offset min-sum (LOMS) decoder kernels for sm_100a.
+//
+// Algorithm: syndrome src/qc_ldpc.rs:962-1221 (f32) and :1530-1758 (int8 messages,
+// int16 posterior), restated for the GPU with the reference's exact arithmetic:
+//   Q     = APP - R_old                         (int8 path: clamped to +-127)
+//   pass1 min1 / min2 / XOR of signs over the layer's edges
+//   R_new = sign * max(min_excl - beta, 0)      (min_excl = min2 on the min1 edge)
+//   APP  += R_new - R_old                       (int8 path: clamped to +-app_clamp)
+// followed by the syndrome check after every iteration (early stop), and hard
+// decisions APP < 0.
+//
+// Mapping: one CTA owns `cpb` codewords of one code; thread (slot, z) owns lifting
+// index z of codeword slot, i.e. check row (layer, z) of every layer.  The
+// posteriors of the CTA's codewords live in shared memory for the whole decode;
+// the cyclic shift of each block is index arithmetic on the shared-memory
+// address.  Layers run in order with a CTA barrier between them (the layered
+// schedule's dependency).  Check-to-variable messages live in global memory in
+// the reference's edge_r layout (edge-major, z fastest), so consecutive threads
+// touch consecutive bytes; the per-CTA scratch is small enough to stay in L2.
+//
+// The kernel is persistent over codeword groups: grid = resident CTAs, each CTA
+// walks groups blockIdx.x, blockIdx.x + gridDim.x, ...  Codewords that pass the
+// syndrome check stop updating while the other slots of their CTA continue.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cstdint>
+#include <string>
+
+#include "decoder.h"
+
+namespace syn {
+
+namespace {
+
+constexpr int kMaxThreads = 384;
+
+struct KArgs {
+  int z, mb, n_edges, n, k;
+  const uint32_t* edge;   // [E] (col * z) << 16 | shift
+  const int32_t* loff;    // [mb + 1]
+  const void* llr;
+  long long llr_stride;
+  int llr_offset;
+  int llr_i16;
+  long long batch;
+  int cpb;
+  int iterations;
+  int beta_q;
+  int app_clamp;
+  float beta;
+  int prologue;
+  long long k_prime;      // filler positions are [k_prime, k)
+  void* r_out;            // C->V messages of codeword b at r_out + b * r_out_stride
+  long long r_out_stride;
+  void* r_ws;             // else per (CTA, slot) scratch
+  uint32_t* hard_packed;
+  int hard_bits;
+  long long hard_words_stride;
+  int32_t* iters;
+  void* app_out;
+  long long app_stride;
+  uint8_t* hard_out;
+  long long hard_stride;
+};
+
+__host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
+
+__host__ __device__ inline int table_bytes(int n_edges, int mb, int cpb) {
+  return align16(n_edges * 4) + align16((mb + 1) * 4) + align16(cpb * 4);
+}
+
+template <typename App>
+struct Smem {
+  uint32_t* edge;
+  int32_t* loff;
+  int32_t* fail;
+  App* app;
+};
+
+template <typename App>
+__device__ inline Smem<App> carve(unsigned char* base, const KArgs& a) {
+  Smem<App> s;
+  s.edge = reinterpret_cast<uint32_t*>(base);
+  s.loff = reinterpret_cast<int32_t*>(base + align16(a.n_edges * 4));
+  s.fail = reinterpret_cast<int32_t*>(base + align16(a.n_edges * 4) + align16((a.mb + 1) * 4));
+  s.app = reinterpret_cast<App*>(base + table_bytes(a.n_edges, a.mb, a.cpb));
+  return s;
+}
+
+// Variable index of edge word w for check row zi: col*z + (zi + shift) mod z.
+__device__ __forceinline__ int var_index(uint32_t w, int zi, int Z) {
+  int r = zi + (int)(w & 0xFFFFu);
+  r = (r >= Z) ? r - Z : r;
+  return (int)(w >> 16) + r;
+}
+
+// ---------------------------------------------------------------- int8 path --
+
+template <int MAXDEG>
+__device__ __forceinline__ void layer_i8(const uint32_t* __restrict__ s_edge, int lb, int deg, int Z,
+                                         int zi, int16_t* __restrict__ A, int8_t* __restrict__ R,
+                                         bool first, int beta_q, int C) {
+  int vidx[MAXDEG], av[MAXDEG], qv[MAXDEG], ro[MAXDEG];
+  int m1 = 127, m2 = 127;
+  unsigned sx = 0;
+  int8_t* Rl = R + (long long)lb * Z + zi;
+#pragma unroll
+  for (int e = 0; e < MAXDEG; ++e) {
+    if (e < deg) {
+      vidx[e] = var_index(s_edge[lb + e], zi, Z);
+      av[e] = A[vidx[e]];
+      ro[e] = first ? 0 : (int)Rl[e * Z];
+      const int q = min(max(av[e] - ro[e], -127), 127);
+      qv[e] = q;
+      const int aq = abs(q);
+      sx ^= (unsigned)q;
+      const int om1 = m1;
+      m1 = min(om1, aq);
+      m2 = min(m2, max(om1, aq));
+    }
+  }
+  if (deg < 2) {
+    if (deg == 0) m1 = 0;
+    m2 = m1;
+  }
+#pragma unroll
+  for (int e = 0; e < MAXDEG; ++e) {
+    if (e < deg) {
+      const int q = qv[e];
+      const int aq = abs(q);
+      const int mex = (aq == m1) ? m2 : m1;
+      const int mag = max(mex - beta_q, 0);
+      const int nr = ((sx ^ (unsigned)q) >> 31) ? -mag : mag;
+      Rl[e * Z] = (int8_t)nr;
+      A[vidx[e]] = (int16_t)min(max(av[e] + nr - ro[e], -C), C);
+    }
+  }
+}
+
+template <typename App>
+__device__ bool syndrome_fails(const uint32_t* __restrict__ s_edge, const int32_t* __restrict__ s_loff,
+                               int mb, int Z, int zi, const App* __restrict__ A) {
+  for (int l = 0; l < mb; ++l) {
+    const int lb = s_loff[l], le = s_loff[l + 1];
+    unsigned par = 0;
+    for (int e = lb; e < le; ++e) par ^= (A[var_index(s_edge[e], zi, Z)] < (App)0) ? 1u : 0u;
+    if (par) return true;
+  }
+  return false;
+}
+
+template <typename App>
+__device__ void write_outputs(const KArgs& a, const Smem<App>& s, long long grp) {
+  const int N = a.n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int sl = 0; sl < a.cpb; ++sl) {
+    const long long cw = grp * a.cpb + sl;
+    if (cw >= a.batch) break;
+    const App* As = s.app + (long long)sl * N;
+    if (a.app_out) {
+      App* dst = reinterpret_cast<App*>(a.app_out) + cw * a.app_stride;
+      for (int j = threadIdx.x; j < N; j += blockDim.x) dst[j] = As[j];
+    }
+    if (a.hard_out) {
+      uint8_t* dst = a.hard_out + cw * a.hard_stride;
+      for (int j = threadIdx.x; j < N; j += blockDim.x) dst[j] = As[j] < (App)0 ? 1 : 0;
+    }
+    if (a.hard_packed) {
+      const int nwords = (a.hard_bits + 31) >> 5;
+      uint32_t* dst = a.hard_packed + cw * a.hard_words_stride;
+      for (int w = warp; w < nwords; w += nwarps) {
+        const int j = (w << 5) + lane;
+        const bool bit = j < a.hard_bits && As[j] < (App)0;
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+        if (lane == 0) dst[w] = m;
+      }
+    }
+  }
+}
+
+template <int MAXDEG>
+__global__ void __launch_bounds__(kMaxThreads) loms_i8_kernel(const KArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Smem<int16_t> s = carve<int16_t>(smem_raw, a);
+  for (int i = threadIdx.x; i < a.n_edges; i += blockDim.x) s.edge[i] = a.edge[i];
+  for (int i = threadIdx.x; i <= a.mb; i += blockDim.x) s.loff[i] = a.loff[i];
+
+  const int Z = a.z, N = a.n, C = a.app_clamp;
+  const int slot = threadIdx.x / Z;
+  const int zi = threadIdx.x - slot * Z;
+  const bool lane_ok = slot < a.cpb;
+  const long long ngroups = (a.batch + a.cpb - 1) / a.cpb;
+  const long long ez = (long long)a.n_edges * Z;
+
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    __syncthreads();
+    for (int sl = 0; sl < a.cpb; ++sl) {
+      const long long cw = grp * a.cpb + sl;
+      if (cw >= a.batch) break;
+      const int8_t* src8 = reinterpret_cast<const int8_t*>(a.llr) + cw * a.llr_stride;
+      const int16_t* src16 = reinterpret_cast<const int16_t*>(a.llr) + cw * a.llr_stride;
+      int16_t* dst = s.app + (long long)sl * N;
+      for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        int v = 0;
+        if (j >= a.llr_offset) v = a.llr_i16 ? (int)src16[j - a.llr_offset] : (int)src8[j - a.llr_offset];
+        if (a.prologue) {
+          if (j < 2 * Z)
+            v = 0;
+          else if (j >= a.k_prime && j < a.k)
+            v = C;
+        }
+        dst[j] = (int16_t)min(max(v, -C), C);
+      }
+    }
+    __syncthreads();
+
+    const long long cw = grp * a.cpb + slot;
+    bool active = lane_ok && cw < a.batch;
+    int8_t* R = nullptr;
+    if (active)
+      R = a.r_out ? reinterpret_cast<int8_t*>(a.r_out) + cw * a.r_out_stride
+                  : reinterpret_cast<int8_t*>(a.r_ws) + ((long long)blockIdx.x * a.cpb + slot) * ez;
+    int16_t* A = s.app + (long long)(lane_ok ? slot : 0) * N;
+    int used = 0;
+    for (int it = 0; it < a.iterations; ++it) {
+      if (!__syncthreads_or(active)) break;
+      if (active) ++used;
+      for (int l = 0; l < a.mb; ++l) {
+        if (active) {
+          const int lb = s.loff[l];
+          layer_i8<MAXDEG>(s.edge, lb, s.loff[l + 1] - lb, Z, zi, A, R, it == 0, a.beta_q, C);
+        }
+        __syncthreads();
+      }
+      if (lane_ok && zi == 0) s.fail[slot] = 0;
+      __syncthreads();
+      if (active && syndrome_fails(s.edge, s.loff, a.mb, Z, zi, A)) s.fail[slot] = 1;
+      __syncthreads();
+      if (active && s.fail[slot] == 0) active = false;
+    }
+    if (lane_ok && cw < a.batch) {
+      if (zi == 0 && a.iters) a.iters[cw] = used;
+      if (used == 0 && a.r_out) {
+        int8_t* Rz = reinterpret_cast<int8_t*>(a.r_out) + cw * a.r_out_stride;
+        for (long long j = zi; j < ez; j += Z) Rz[j] = 0;
+      }
+    }
+    __syncthreads();
+    write_outputs<int16_t>(a, s, grp);
+  }
+}
+
+// ----------------------------------------------------------------- f32 path --
+
+template <int MAXDEG>
+__device__ __forceinline__ void layer_f32(const uint32_t* __restrict__ s_edge, int lb, int deg, int Z,
+                                          int zi, float* __restrict__ A, float* __restrict__ R,
+                                          bool first, float beta) {
+  int vidx[MAXDEG];
+  float av[MAXDEG], qv[MAXDEG], ro[MAXDEG];
+  float m1 = FLT_MAX, m2 = FLT_MAX;
+  unsigned sx = 0;
+  float* Rl = R + (long long)lb * Z + zi;
+#pragma unroll
+  for (int e = 0; e < MAXDEG; ++e) {
+    if (e < deg) {
+      vidx[e] = var_index(s_edge[lb + e], zi, Z);
+      av[e] = A[vidx[e]];
+      ro[e] = first ? 0.0f : Rl[e * Z];
+      const float q = __fsub_rn(av[e], ro[e]);
+      qv[e] = q;
+      const unsigned b = __float_as_uint(q);
+      const float aq = __uint_as_float(b & 0x7FFFFFFFu);
+      sx ^= b & 0x80000000u;
+      if (aq <= m1) {
+        m2 = m1;
+        m1 = aq;
+      } else if (aq < m2) {
+        m2 = aq;
+      }
+    }
+  }
+  if (m1 == FLT_MAX) m1 = 0.0f;
+  if (m2 == FLT_MAX) m2 = m1;
+#pragma unroll
+  for (int e = 0; e < MAXDEG; ++e) {
+    if (e < deg) {
+      const unsigned b = __float_as_uint(qv[e]);
+      const float aq = __uint_as_float(b & 0x7FFFFFFFu);
+      const unsigned sgn = sx ^ (b & 0x80000000u);
+      const float mex = (aq == m1) ? m2 : m1;
+      float mag = __fsub_rn(mex, beta);
+      if (mag < 0.0f) mag = 0.0f;
+      const float nr = __uint_as_float(__float_as_uint(mag) | sgn);
+      Rl[e * Z] = nr;
+      A[vidx[e]] = __fadd_rn(av[e], __fsub_rn(nr, ro[e]));
+    }
+  }
+}
+
+template <int MAXDEG>
+__global__ void __launch_bounds__(kMaxThreads) loms_f32_kernel(const KArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Smem<float> s = carve<float>(smem_raw, a);
+  for (int i = threadIdx.x; i < a.n_edges; i += blockDim.x) s.edge[i] = a.edge[i];
+  for (int i = threadIdx.x; i <= a.mb; i += blockDim.x) s.loff[i] = a.loff[i];
+
+  const int Z = a.z, N = a.n;
+  const int slot = threadIdx.x / Z;
+  const int zi = threadIdx.x - slot * Z;
+  const bool lane_ok = slot < a.cpb;
+  const long long ngroups = (a.batch + a.cpb - 1) / a.cpb;
+  const long long ez = (long long)a.n_edges * Z;
+
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    __syncthreads();
+    for (int sl = 0; sl < a.cpb; ++sl) {
+      const long long cw = grp * a.cpb + sl;
+      if (cw >= a.batch) break;
+      const float* src = reinterpret_cast<const float*>(a.llr) + cw * a.llr_stride;
+      float* dst = s.app + (long long)sl * N;
+      for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        float v = j >= a.llr_offset ? src[j - a.llr_offset] : 0.0f;
+        if (a.prologue) {
+          if (j < 2 * Z)
+            v = 0.0f;
+          else if (j >= a.k_prime && j < a.k)
+            v = 1000000.0f;
+        }
+        dst[j] = v;
+      }
+    }
+    __syncthreads();
+
+    const long long cw = grp * a.cpb + slot;
+    bool active = lane_ok && cw < a.batch;
+    float* R = nullptr;
+    if (active)
+      R = a.r_out ? reinterpret_cast<float*>(a.r_out) + cw * a.r_out_stride
+                  : reinterpret_cast<float*>(a.r_ws) + ((long long)blockIdx.x * a.cpb + slot) * ez;
+    float* A = s.app + (long long)(lane_ok ? slot : 0) * N;
+    int used = 0;
+    for (int it = 0; it < a.iterations; ++it) {
+      if (!__syncthreads_or(active)) break;
+      if (active) ++used;
+      for (int l = 0; l < a.mb; ++l) {
+        if (active) {
+          const int lb = s.loff[l];
+          layer_f32<MAXDEG>(s.edge, lb, s.loff[l + 1] - lb, Z, zi, A, R, it == 0, a.beta);
+        }
+        __syncthreads();
+      }
+      if (lane_ok && zi == 0) s.fail[slot] = 0;
+      __syncthreads();
+      if (active && syndrome_fails(s.edge, s.loff, a.mb, Z, zi, A)) s.fail[slot] = 1;
+      __syncthreads();
+      if (active && s.fail[slot] == 0) active = false;
+    }
+    if (lane_ok && cw < a.batch) {
+      if (zi == 0 && a.iters) a.iters[cw] = used;
+      if (used == 0 && a.r_out) {
+        float* Rz = reinterpret_cast<float*>(a.r_out) + cw * a.r_out_stride;
+        for (long long j = zi; j < ez; j += Z) Rz[j] = 0.0f;
+      }
+    }
+    __syncthreads();
+    write_outputs<float>(a, s, grp);
+  }
+}
+
+typedef void (*KernelFn)(const KArgs);
+
+int pick_maxdeg(int maxdeg) {
+  if (maxdeg <= 8) return 8;
+  if (maxdeg <= 12) return 12;
+  if (maxdeg <= 16) return 16;
+  if (maxdeg <= 20) return 20;
+  if (maxdeg <= 24) return 24;
+  return -1;
+}
+
+KernelFn kernel_for(Precision p, int tmpl) {
+  if (p == Precision::kInt8) {
+    switch (tmpl) {
+      case 8: return loms_i8_kernel<8>;
+      case 12: return loms_i8_kernel<12>;
+      case 16: return loms_i8_kernel<16>;
+      case 20: return loms_i8_kernel<20>;
+      case 24: return loms_i8_kernel<24>;
+    }
+  } else {
+    switch (tmpl) {
+      case 8: return loms_f32_kernel<8>;
+      case 12: return loms_f32_kernel<12>;
+      case 16: return loms_f32_kernel<16>;
+      case 20: return loms_f32_kernel<20>;
+      case 24: return loms_f32_kernel<24>;
+    }
+  }
+  return nullptr;
+}
+
+}  // namespace
+
+Decoder::~Decoder() {
+  if (device_ >= 0) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device_);
+    cudaFree(d_edge_);
+    cudaFree(d_loff_);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+}
+
+bool Decoder::init(const Graph& g, float offset_beta, std::string* err) {
+  if (pick_maxdeg(g.maxdeg) < 0) {
+    if (err) *err = "layer degree above 24 is not supported by the GPU kernels";
+    return false;
+  }
+  if (g.n() > 65535 * 4) {
+    if (err) *err = "code too long";
+    return false;
+  }
+  // The shared-memory address arithmetic needs each column to appear at most once per layer.
+  for (int l = 0; l < g.mb; ++l)
+    for (int e = g.layer_off[l]; e < g.layer_off[l + 1]; ++e)
+      for (int f = g.layer_off[l]; f < e; ++f)
+        if (g.cols[f] == g.cols[e]) {
+          if (err) *err = "a column appears twice in one layer";
+          return false;
+        }
+  g_ = g;
+  beta_ = offset_beta;
+  if (cudaGetDevice(&device_) != cudaSuccess) {
+    if (err) *err = "no CUDA device";
+    device_ = -1;
+    return false;
+  }
+  std::vector<uint32_t> ew(g.edges());
+  for (int e = 0; e < g.edges(); ++e) ew[e] = ((uint32_t)(g.cols[e] * g.z) << 16) | (uint32_t)g.shifts[e];
+  if (cudaMalloc(&d_edge_, sizeof(uint32_t) * std::max(1, g.edges())) != cudaSuccess ||
+      cudaMalloc(&d_loff_, sizeof(int32_t) * (g.mb + 1)) != cudaSuccess) {
+    if (err) *err = "cudaMalloc failed for the layer tables";
+    return false;
+  }
+  cudaMemcpy(d_edge_, ew.data(), sizeof(uint32_t) * g.edges(), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_loff_, g.layer_off.data(), sizeof(int32_t) * (g.mb + 1), cudaMemcpyHostToDevice);
+  return cudaGetLastError() == cudaSuccess;
+}
+
+Decoder::Geometry Decoder::geometry(Precision p, long long batch) const {
+  Geometry geo{};
+  const int elem = p == Precision::kInt8 ? 2 : 4;
+  const int Z = g_.z;
+  const long long N = g_.n();
+  int cpb = std::max(1, std::min(64, kMaxThreads / Z));
+  while (cpb > 1 && table_bytes(g_.edges(), g_.mb, cpb) + (long long)cpb * N * elem > 100 * 1024) --cpb;
+  if (batch > 0) cpb = (int)std::min<long long>(cpb, batch);
+  geo.cpb = cpb;
+  geo.threads = ((cpb * Z + 31) / 32) * 32;
+  geo.smem = table_bytes(g_.edges(), g_.mb, cpb) + (int)(cpb * N * elem);
+  geo.maxdeg_tmpl = pick_maxdeg(g_.maxdeg);
+  KernelFn fn = kernel_for(p, geo.maxdeg_tmpl);
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, geo.smem);
+  int per_sm = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, geo.threads, geo.smem);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ < 0 ? 0 : device_);
+  geo.max_ctas = std::max(1, per_sm) * std::max(1, sms);
+  return geo;
+}
+
+size_t Decoder::workspace_bytes(Precision p, long long batch) const {
+  const Geometry geo = geometry(p, batch);
+  const long long groups = (batch + geo.cpb - 1) / geo.cpb;
+  const long long ctas = std::min<long long>(groups, geo.max_ctas);
+  const long long elem = p == Precision::kInt8 ? 1 : 4;
+  return (size_t)(ctas * geo.cpb * g_.edge_buffer() * elem);
+}
+
+cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t stream,
+                            std::string* err) const {
+  auto bad = [&](const char* m) {
+    if (err) *err = m;
+    return cudaErrorInvalidValue;
+  };
+  if (req.batch < 0) return bad("batch must be non-negative");
+  if (req.batch == 0) return cudaSuccess;
+  if (!req.llr) return bad("llr is null");
+  if (req.iterations < 0) return bad("iterations must be non-negative");
+  if (req.llr_offset < 0 || req.llr_offset > g_.n()) return bad("llr_offset out of range");
+  if (req.hard_packed && (req.hard_bits < 0 || req.hard_bits > g_.n() ||
+                          req.hard_words_stride < (req.hard_bits + 31) / 32))
+    return bad("hard_bits / hard_words_stride out of range");
+  if (req.app_clamp < 0 && p == Precision::kInt8) return bad("app_clamp must be non-negative");
+  const Geometry geo = geometry(p, req.batch);
+  const long long groups = (req.batch + geo.cpb - 1) / geo.cpb;
+  const long long ctas = std::min<long long>(groups, geo.max_ctas);
+  if (!req.edge_r) {
+    const long long elem = p == Precision::kInt8 ? 1 : 4;
+    const long long need = ctas * geo.cpb * g_.edge_buffer() * elem;
+    if (!req.workspace || (long long)req.workspace_bytes < need) return bad("workspace too small");
+  }
+  KArgs a{};
+  a.z = g_.z;
+  a.mb = g_.mb;
+  a.n_edges = g_.edges();
+  a.n = (int)g_.n();
+  a.k = (int)g_.k();
+  a.edge = d_edge_;
+  a.loff = d_loff_;
+  a.llr = req.llr;
+  a.llr_stride = req.llr_stride;
+  a.llr_offset = req.llr_offset;
+  a.llr_i16 = req.llr_i16;
+  a.batch = req.batch;
+  a.cpb = geo.cpb;
+  a.iterations = req.iterations;
+  a.beta_q = req.beta_q;
+  a.app_clamp = req.app_clamp;
+  a.beta = req.beta;
+  a.prologue = req.prologue_5g;
+  a.k_prime = req.n_filler > g_.k() ? 0 : g_.k() - req.n_filler;
+  a.r_out = req.edge_r;
+  a.r_out_stride = req.edge_r_stride;
+  a.r_ws = req.workspace;
+  a.hard_packed = req.hard_packed;
+  a.hard_bits = req.hard_bits;
+  a.hard_words_stride = req.hard_words_stride;
+  a.iters = req.iters;
+  a.app_out = req.app;
+  a.app_stride = req.app_stride;
+  a.hard_out = req.hard;
+  a.hard_stride = req.hard_stride;
+  KernelFn fn = kernel_for(p, geo.maxdeg_tmpl);
+  fn<<<(unsigned)ctas, geo.threads, geo.smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace syn

@@ -1,0 +1,286 @@
+"""Parity of the CUDA decoder with the oracle (the CPU restatement of the
+reference's decoder) on identical seeded inputs.
+
+int8 path: iterations used, final posterior, final C->V messages and hard
+decisions must be bit-identical (the reference's own bar for its AVX2 kernel,
+tests/ldpc_int8_kernel_equivalence.rs:140).  f32 path: iterations and hard
+decisions bit-identical; posteriors and messages within 1e-5 relative
+(F32_RTOL), the contract tolerance; the kernel is expected to be exact and the
+tests report how many values differ at all."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import _oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import syndrome_b200 as S  # noqa: E402
+from syndrome_b200 import _lib  # noqa: E402
+
+F32_RTOL = 1e-5
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def codewords(code, count, ebno, seed):
+    """Encoded random codewords and their channel LLRs (oracle encoder + channel)."""
+    rate = code.k / code.n
+    cws, llrs = [], []
+    for i in range(count):
+        s = seed + 7919 * i
+        cw = code.encode(O.random_bits(s ^ 0xA5A5A5A5, code.k))
+        cws.append(cw)
+        llrs.append(O.awgn(cw, ebno, rate, s))
+    return np.stack(cws), np.stack(llrs)
+
+
+def oracle_i8(code, apps, beta_q, iters, app_clamp=32767):
+    return [code.decode_i8(a, beta_q, iters, app_clamp) for a in apps]
+
+
+def gpu_i8(dec, llr_i8, iters, quant, **kw):
+    t = torch.from_numpy(np.ascontiguousarray(llr_i8)).cuda()
+    r = dec.decode_batch_i8(t, iters, quant=quant, want_app=True, want_edge_r=True, want_hard=True, **kw)
+    torch.cuda.synchronize()
+    return r
+
+
+def assert_i8_equal(label, ref, r):
+    it = r.iters.cpu().numpy()
+    app = r.app.cpu().numpy()
+    er = r.edge_r.cpu().numpy()
+    hard = r.hard.cpu().numpy()
+    for b, o in enumerate(ref):
+        assert it[b] == o["iters"], f"{label} cw{b}: iterations {it[b]} != {o['iters']}"
+        d = np.nonzero(app[b] != o["app"])[0]
+        assert d.size == 0, f"{label} cw{b}: posterior differs at {d[:5]} ({d.size} of {app.shape[1]})"
+        d = np.nonzero(er[b] != o["edge_r"])[0]
+        assert d.size == 0, f"{label} cw{b}: C->V message differs at {d[:5]}"
+        assert np.array_equal(hard[b], o["hard"]), f"{label} cw{b}: hard decisions differ"
+    packed = r.hard_packed.cpu().numpy().view(np.uint32)
+    bits = np.unpackbits(packed.view(np.uint8), axis=1, bitorder="little")[:, : r.hard_bits]
+    assert np.array_equal(bits, hard[:, : r.hard_bits]), f"{label}: packed hard bits differ"
+
+
+@pytest.mark.parametrize("bg,z", [(0, 7), (0, 44), (0, 96), (1, 13), (1, 52), (1, 128)])
+def test_int8_3gpp_graphs(bg, z):
+    """tests/ldpc_int8_kernel_equivalence.rs:172-200 (12 iterations, beta 0.5, scale 8)."""
+    code = O.Code.nr(bg, z)
+    dec = S.QcLdpcDecoder.with_lifting_size(bg, z, 0.5)
+    q = S.QuantParams()
+    for ebno in (0.0, 1.5, 4.0):
+        _, llr = codewords(code, 4, ebno, 0x10000 ^ (z << 8))
+        apps = np.stack([O.quantize_i16(x) for x in llr])
+        ref = oracle_i8(code, apps, O.beta_q(0.5), 12)
+        r = gpu_i8(dec, apps.astype(np.int8), 12, q)
+        assert_i8_equal(f"bg{bg + 1} z{z} {ebno}dB", ref, r)
+
+
+def test_int8_bg1_z384():
+    """tests/ldpc_int8_kernel_equivalence.rs:202-215 (BG1 Z=384 at 1 dB)."""
+    code = O.Code.nr(0, 384)
+    dec = S.QcLdpcDecoder.with_lifting_size(0, 384, 0.5)
+    _, llr = codewords(code, 3, 1.0, 0x03840000)
+    apps = np.stack([O.quantize_i16(x) for x in llr])
+    assert_i8_equal("bg1 z384", oracle_i8(code, apps, 4, 12), gpu_i8(dec, apps.astype(np.int8), 12, S.QuantParams()))
+
+
+def test_int8_wifi_matrices():
+    """tests/ldpc_int8_kernel_equivalence.rs:217-236."""
+    for z, rn, rd in ((27, 1, 2), (54, 2, 3), (81, 5, 6), (27, 3, 4)):
+        code = O.Code.wifi(z, rn, rd)
+        dec = S.wifi_ldpc_decoder(z, rn, rd, 0.5)
+        for ebno in (1.0, 3.0):
+            _, llr = codewords(code, 5, ebno, 0x01F10000 ^ (z << 4) ^ rd)
+            apps = np.stack([O.quantize_i16(x) for x in llr])
+            ref = oracle_i8(code, apps, 4, 12)
+            assert_i8_equal(f"wifi {z} {rn}/{rd}", ref, gpu_i8(dec, apps.astype(np.int8), 12, S.QuantParams()))
+
+
+def test_int8_clamped_posterior_and_offsets():
+    """:238-277: APP_CLAMP_I8, beta = 0 and a saturating beta (beta_q = 127)."""
+    cases = [((0, 44), 0.5, S.APP_CLAMP_I8), ((1, 88), 0.5, S.APP_CLAMP_I8), ((0, 60), 0.0, 32767),
+             ((1, 104), 16.0, 32767)]
+    for (bg, z), beta, clamp in cases:
+        code = O.Code.nr(bg, z)
+        dec = S.QcLdpcDecoder.with_lifting_size(bg, z, beta)
+        q = S.QuantParams().with_app_clamp(clamp)
+        _, llr = codewords(code, 3, 1.0, 0x0C1A0000 + z)
+        apps = np.stack([O.quantize_i16(x) for x in llr])
+        ref = oracle_i8(code, apps, O.beta_q(beta), 12, clamp)
+        assert_i8_equal(f"bg{bg + 1} z{z} beta{beta} clamp{clamp}", ref, gpu_i8(dec, apps.astype(np.int8), 12, q))
+
+
+def test_int8_5g_prologue_with_filler():
+    """:279-343: decode_5g_i8 with n_filler = 3Z/2, input without the punctured columns."""
+    z = 60
+    code = O.Code.nr(0, z)
+    dec = S.QcLdpcDecoder.with_lifting_size(0, z, 0.5)
+    n = code.n
+    llr = np.where(np.arange(n) % 5 == 0, -0.75, 1.25).astype(np.float32)
+    app0 = O.quantize_i16(llr)
+    n_filler = 3 * z // 2
+    for clamp in (32767, 127):
+        ref = code.decode_i8(code.prologue_5g_i8(app0, n_filler, clamp), 4, 12, clamp)
+        tx = app0[2 * z:].astype(np.int8)[None, :]
+        r = gpu_i8(dec, tx, 12, S.QuantParams().with_app_clamp(clamp), llr_offset=2 * z, nr_prologue=True,
+                   n_filler=n_filler)
+        assert_i8_equal(f"5g prologue clamp {clamp}", [ref], r)
+
+
+def test_int8_zero_iterations_and_many_codewords():
+    code = O.Code.nr(1, 16)
+    dec = S.QcLdpcDecoder.with_lifting_size(1, 16, 0.5)
+    _, llr = codewords(code, 40, 2.0, 77)
+    apps = np.stack([O.quantize_i16(x) for x in llr])
+    for iters in (0, 1, 3, 20):
+        ref = oracle_i8(code, apps, 4, iters)
+        assert_i8_equal(f"iters {iters}", ref, gpu_i8(dec, apps.astype(np.int8), iters, S.QuantParams()))
+
+
+def test_int8_host_api_drop_in():
+    """decode_layered_offset_min_sum_i8 / decode_5g_i8 through the host-buffer C entry points."""
+    code = O.Code.nr(0, 16)
+    dec = S.QcLdpcDecoder.with_lifting_size(0, 16, 0.5)
+    _, llr = codewords(code, 1, 1.0, 5)
+    app0 = O.quantize_i16(llr[0])
+    app0[::37] = 900  # int16 posteriors outside the message range are accepted and clamped
+    ref = code.decode_i8(app0, 4, 10)
+    app = app0.copy()
+    er = np.zeros(dec.required_edge_buffer(), np.int8)
+    sc = np.zeros(dec.required_layer_buffer(), np.int8)
+    hard = np.zeros(code.n, np.uint8)
+    it = dec.decode_layered_offset_min_sum_i8(app, er, sc, hard, 10, S.QuantParams())
+    assert it == ref["iters"] and np.array_equal(app, ref["app"]) and np.array_equal(er, ref["edge_r"])
+    assert np.array_equal(hard, ref["hard"])
+    app = app0.copy()
+    it = dec.decode_5g_i8(app, 8, er, sc, hard, 10, S.QuantParams())
+    ref = code.decode_i8(code.prologue_5g_i8(app0, 8), 4, 10)
+    assert it == ref["iters"] and np.array_equal(app, ref["app"])
+    with pytest.raises(S.FecError) as e:
+        dec.decode_layered_offset_min_sum_i8(app, er[:-1], sc, hard, 10)
+    assert e.value.status == _lib.BUFFER_TOO_SMALL
+    with pytest.raises(S.FecError) as e:
+        dec.decode_layered_offset_min_sum_i8(app[:-1].copy(), er, sc, hard, 10)
+    assert e.value.status == _lib.INVALID_PARAM
+
+
+# ------------------------------------------------------------------ f32 path --
+
+def assert_f32_close(label, ref, r):
+    it = r.iters.cpu().numpy()
+    app = r.app.cpu().numpy()
+    er = r.edge_r.cpu().numpy()
+    hard = r.hard.cpu().numpy()
+    for b, o in enumerate(ref):
+        assert it[b] == o["iters"], f"{label} cw{b}: iterations {it[b]} != {o['iters']}"
+        assert np.array_equal(hard[b], o["hard"]), f"{label} cw{b}: hard decisions differ"
+        np.testing.assert_allclose(app[b], o["llr"], rtol=F32_RTOL, atol=0, err_msg=f"{label} cw{b} app")
+        np.testing.assert_allclose(er[b], o["edge_r"], rtol=F32_RTOL, atol=0, err_msg=f"{label} cw{b} edge_r")
+        exact = np.array_equal(app[b].view(np.uint32), o["llr"].view(np.uint32))
+        assert exact, f"{label} cw{b}: posterior within tolerance but not bit-identical"
+
+
+def gpu_f32(dec, llr, iters, **kw):
+    t = torch.from_numpy(np.ascontiguousarray(llr, dtype=np.float32)).cuda()
+    r = dec.decode_batch_f32(t, iters, want_app=True, want_edge_r=True, want_hard=True, **kw)
+    torch.cuda.synchronize()
+    return r
+
+
+def test_f32_golden_checksum():
+    with open(os.path.join(GOLDEN, "ldpc_checksums.json")) as f:
+        want = json.load(f)["checksums"]["ldpc_rust.checksum"]
+    dec = S.QcLdpcDecoder.with_lifting_size(0, 384, 0.25)
+    n = dec.variable_node_count()
+    llr = np.where(np.arange(n) % 2 == 0, 0.5, -0.5).astype(np.float32)[None, :]
+    r = gpu_f32(dec, llr, 10)
+    assert int(r.iters[0]) == 10
+    assert "%016x" % O.fnv1a_hard(r.hard[0].cpu().numpy()) == want
+
+
+def test_f32_golden_convergence_trajectory():
+    """Running t iterations from scratch reproduces the reference's frame t."""
+    with open(os.path.join(GOLDEN, "ldpc_convergence_wifi27_r12.json")) as f:
+        g = json.load(f)
+    code = O.Code.wifi(27, 1, 2)
+    info = np.array([((i * 2654435761) >> 31) & 1 for i in range(code.k)], dtype=np.uint8)
+    llr = O.awgn(code.encode(info), 0.0, 0.5, 139)
+    dec = S.wifi_ldpc_decoder(27, 1, 2, 0.25)
+    for t in range(1, g["iterations_used"] + 1):
+        r = gpu_f32(dec, llr[None, :], t)
+        want = np.unpackbits(np.frombuffer(bytes.fromhex(g["frames"][t]["hard_bits"]), np.uint8),
+                             bitorder="little")[: g["n"]]
+        assert int(r.iters[0]) == t
+        assert np.array_equal(r.hard[0].cpu().numpy(), want), f"frame {t}"
+    r = gpu_f32(dec, llr[None, :], g["max_iterations"])
+    assert int(r.iters[0]) == g["iterations_used"]
+
+
+@pytest.mark.parametrize("kind,a,b", [("nr", 0, 32), ("nr", 1, 52), ("nr", 0, 384), ("wifi", 27, (1, 2)),
+                                      ("wifi", 81, (5, 6)), ("wifi", 54, (3, 4))])
+def test_f32_graphs(kind, a, b):
+    if kind == "nr":
+        code, dec = O.Code.nr(a, b), S.QcLdpcDecoder.with_lifting_size(a, b, 0.5)
+    else:
+        code, dec = O.Code.wifi(a, *b), S.wifi_ldpc_decoder(a, *b, 0.5)
+    for ebno in (0.5, 2.0):
+        _, llr = codewords(code, 3, ebno, 0xF320000 + code.z)
+        ref = [code.decode_f32(x, 0.5, 20) for x in llr]
+        assert_f32_close(f"{kind} {a} {b} {ebno}", ref, gpu_f32(dec, llr, 20))
+
+
+def test_f32_5g_prologue_and_drop_in():
+    """syndrome_ldpc_decode_5g (capi/src/lib.rs:290) against init_5g_llr + decode."""
+    z = 24
+    code = O.Code.nr(1, z)
+    dec = S.QcLdpcDecoder.with_lifting_size(1, z, 0.25)
+    _, llr = codewords(code, 1, 1.0, 42)
+    x = llr[0]
+    ref = code.decode_f32(code.init_5g_f32(x, 13), 0.25, 15)
+    buf = x.copy()
+    er = np.zeros(dec.required_edge_buffer(), np.float32)
+    sc = np.zeros(dec.required_layer_buffer(), np.float32)
+    hard = np.zeros(code.n, np.uint8)
+    it = dec.decode_5g(buf, 13, er, sc, hard, 15)
+    assert it == ref["iters"] and np.array_equal(hard, ref["hard"])
+    assert np.array_equal(buf.view(np.uint32), ref["llr"].view(np.uint32))
+    assert np.array_equal(er.view(np.uint32), ref["edge_r"].view(np.uint32))
+    r = gpu_f32(dec, x[None, 2 * z:], 15, llr_offset=2 * z, nr_prologue=True, n_filler=13)
+    assert int(r.iters[0]) == ref["iters"] and np.array_equal(r.hard[0].cpu().numpy(), ref["hard"])
+    with pytest.raises(S.FecError) as e:
+        dec.decode_5g(buf, 13, er, sc[:-1], hard, 15)
+    assert e.value.status == _lib.BUFFER_TOO_SMALL
+    with pytest.raises(S.FecError) as e:
+        dec.decode_5g(buf, 13, er, sc, hard[:-1].copy(), 15)
+    assert e.value.status == _lib.INVALID_PARAM
+
+
+def test_f32_adversarial_inputs():
+    """fuzz/fuzz_targets/fuzz_ldpc_decode.rs: NaN, +-inf, zeros, huge values.
+
+    Finite inputs (zeros, 1e30) must match exactly.  With NaN or infinite inputs
+    the decode must complete with sane outputs; bit parity is not claimed there
+    because a NaN created on the GPU (inf - inf) carries CUDA's canonical sign
+    bit where x86 produces a negative NaN, and the sign bit feeds the sign XOR."""
+    code = O.Code.nr(1, 8)
+    dec = S.QcLdpcDecoder.with_lifting_size(1, 8, 0.3)
+    rng = np.random.default_rng(3)
+    x = rng.normal(0, 3, (4, code.n)).astype(np.float32)
+    x[0, ::7] = np.nan
+    x[1, ::5] = np.inf
+    x[1, 1::5] = -np.inf
+    x[2] = 0.0
+    x[3, ::3] = 1e30
+    ref = [code.decode_f32(v, 0.3, 6) for v in x]
+    r = gpu_f32(dec, x, 6)
+    it, hard = r.iters.cpu().numpy(), r.hard.cpu().numpy()
+    app = r.app.cpu().numpy()
+    for b in (2, 3):
+        assert it[b] == ref[b]["iters"] and np.array_equal(hard[b], ref[b]["hard"])
+        assert np.array_equal(app[b].view(np.uint32), ref[b]["llr"].view(np.uint32))
+    for b in (0, 1):
+        assert 1 <= it[b] <= 6 and set(np.unique(hard[b])) <= {0, 1}
