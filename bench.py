@@ -57,6 +57,7 @@ def parse_args():
     p.add_argument("--chunks", type=int, default=8, help="e2e copy/compute pipeline depth")
     p.add_argument("--cpu-seconds", type=float, default=8.0, help="target CPU work of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--kernel", choices=["auto", "generic", "nr"], default="auto")
     return p.parse_args()
 
 
@@ -240,7 +241,7 @@ def main():
 
     B = args.batch
     info, llr_h = make_data(B, rank)
-    dec = S.QcLdpcDecoder.with_lifting_size(BG, Z, BETA)
+    dec = S.QcLdpcDecoder.with_lifting_size(BG, Z, BETA).set_kernel(args.kernel)
     quant = S.QuantParams(SCALE)
     d_llr = torch.from_numpy(llr_h).to(dev)
     packed = torch.empty((B, WORDS), dtype=torch.int32, device=dev)
@@ -349,6 +350,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8", "data": "synthetic",
         "config": {"workload": WORKLOAD, "codewords_per_gpu": B, "info_bits_per_codeword": K_INFO,
+                   "kernel": args.kernel,
                    "mean_iterations": mean_iters, "frames_correct": int(frame_ok.sum()),
                    "l2": "inputs 415 MB per step > 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "Gbit/s", "h2d_bytes_per_step": int(B * N_TX),

@@ -193,6 +193,11 @@ int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const
                                        size_t app_stride, float* d_edge_r, size_t edge_r_stride,
                                        uint8_t* d_hard, size_t hard_stride, void* d_workspace,
                                        size_t workspace_bytes, void* stream);
+/* Kernel selection for this decoder's batched int8 decodes: 0 = automatic (the
+ * 5G NR kernel when it applies, else the generic layered kernel), 1 = always the
+ * generic kernel, 2 = require the 5G NR kernel (INVALID_PARAM on a request it
+ * cannot serve).  Both kernels produce identical results. */
+int32_t syndrome_ldpc_decoder_set_kernel(SyndromeLdpcDecoder* decoder, int32_t kernel);
 /* Text of the last error on this thread (empty if none). */
 const char* syndrome_last_error(void);
 

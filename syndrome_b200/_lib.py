@@ -60,6 +60,7 @@ PROTOTYPES = {
                                              _vp, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _vp]),
     "syndrome_ldpc_decode_batch_f32": (_i32, [_vp, _vp, _sz, _sz, _sz, _i32, _sz, _sz,
                                               _vp, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _vp]),
+    "syndrome_ldpc_decoder_set_kernel": (_i32, [_vp, _i32]),
     "syndrome_last_error": (ctypes.c_char_p, []),
 }
 

@@ -23,6 +23,7 @@
 struct SyndromeLdpcDecoder {
   syn::Graph graph;
   syn::Decoder dec;
+  int kernel = 0;
   std::mutex mu;  // serialises the host-buffer wrappers that share the staging buffers
   void* staging = nullptr;
   size_t staging_bytes = 0;
@@ -127,6 +128,7 @@ int32_t host_decode(SyndromeLdpcDecoder* d, bool f32, void* app, void* edge_r, u
   r.hard = reinterpret_cast<uint8_t*>(base + off_hard);
   r.hard_stride = (long long)n;
   r.iters = reinterpret_cast<int32_t*>(base + off_it);
+  r.kernel = d->kernel;
   std::string msg;
   e = d->dec.decode(f32 ? syn::Precision::kF32 : syn::Precision::kInt8, r, 0, &msg);
   if (e != cudaSuccess) return from_cuda(e, msg);
@@ -171,6 +173,13 @@ void nr_prologue_i16(const syn::Graph& g, int16_t* app, size_t n_filler, int16_t
 extern "C" {
 
 const char* syndrome_last_error(void) { return g_last_error.c_str(); }
+
+int32_t syndrome_ldpc_decoder_set_kernel(SyndromeLdpcDecoder* decoder, int32_t kernel) {
+  if (!decoder) return SYNDROME_NULL_POINTER;
+  if (kernel < 0 || kernel > 2) return fail(SYNDROME_INVALID_PARAM, "kernel must be 0, 1 or 2");
+  decoder->kernel = kernel;
+  return SYNDROME_OK;
+}
 
 // ------------------------------------------------------------- group 1 ------
 
@@ -482,6 +491,7 @@ static int32_t batch_common(const SyndromeLdpcDecoder* decoder, syn::Precision p
   r.hard_stride = (long long)hard_stride;
   r.workspace = d_workspace;
   r.workspace_bytes = workspace_bytes;
+  r.kernel = decoder->kernel;
   std::string msg;
   cudaError_t e = decoder->dec.decode(p, r, static_cast<cudaStream_t>(stream), &msg);
   return from_cuda(e, msg);

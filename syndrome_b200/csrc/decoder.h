@@ -45,6 +45,8 @@ struct BatchRequest {
   long long hard_stride = 0;
   void* edge_r = nullptr;            // [batch][edge_r_stride] final C->V messages, reference layout
   long long edge_r_stride = 0;
+  // Kernel selection: 0 = automatic, 1 = generic layered kernel, 2 = 5G NR kernel.
+  int kernel = 0;
   // Scratch for C->V messages when edge_r is null.
   void* workspace = nullptr;
   size_t workspace_bytes = 0;
@@ -82,6 +84,8 @@ class Decoder {
   Graph g_;
   float beta_ = 0.0f;
   int device_ = -1;
+  int sms_ = 0;
+  int nr_bg_ = -1;               // 0/1 when the 5G NR kernel applies to this code
   uint32_t* d_edge_ = nullptr;   // [E] (col * z) << 16 | shift
   int32_t* d_loff_ = nullptr;    // [mb + 1]
 };

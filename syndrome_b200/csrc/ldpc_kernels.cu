@@ -29,6 +29,7 @@
 #include <string>
 
 #include "decoder.h"
+#include "nr_kernels.h"
 
 namespace syn {
 
@@ -447,6 +448,16 @@ bool Decoder::init(const Graph& g, float offset_beta, std::string* err) {
     return false;
   }
   cudaMemcpy(d_edge_, ew.data(), sizeof(uint32_t) * g.edges(), cudaMemcpyHostToDevice);
+  cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
+  nr_bg_ = -1;
+  if ((g.kind == GraphKind::kNrBg1 || g.kind == GraphKind::kNrBg2) && g.maxdeg <= 31) {
+    const int bg = g.kind == GraphKind::kNrBg1 ? 0 : 1;
+    bool ok = nr_layout_matches(bg, g.cols.data(), g.edges());
+    for (int l = 4; ok && l < g.mb; ++l)
+      for (int e = g.layer_off[l]; e < g.layer_off[l + 1]; ++e)
+        if (g.cols[e] == g.kb + l && g.shifts[e] != 0) ok = false;
+    if (ok) nr_bg_ = bg;
+  }
   cudaMemcpy(d_loff_, g.layer_off.data(), sizeof(int32_t) * (g.mb + 1), cudaMemcpyHostToDevice);
   return cudaGetLastError() == cudaSuccess;
 }
@@ -495,6 +506,34 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
                           req.hard_words_stride < (req.hard_bits + 31) / 32))
     return bad("hard_bits / hard_words_stride out of range");
   if (req.app_clamp < 0 && p == Precision::kInt8) return bad("app_clamp must be non-negative");
+  const bool nr_ok = p == Precision::kInt8 && nr_bg_ >= 0 && !req.llr_i16 && req.app_clamp >= 255;
+  if (req.kernel == 2 && !nr_ok) return bad("the 5G NR kernel does not apply to this request");
+  if (nr_ok && req.kernel != 1) {
+    NrCommon c{};
+    c.z = g_.z;
+    c.beta_q = req.beta_q;
+    c.app_clamp = req.app_clamp;
+    c.prologue = req.prologue_5g;
+    c.k = (int)g_.k();
+    c.k_prime = req.n_filler > g_.k() ? 0 : g_.k() - req.n_filler;
+    c.llr = static_cast<const int8_t*>(req.llr);
+    c.llr_stride = req.llr_stride;
+    c.llr_offset = req.llr_offset;
+    c.batch = req.batch;
+    c.cpb = std::min<long long>(nr_cpb(nr_bg_, g_.z), req.batch);
+    c.iterations = req.iterations;
+    c.hard_packed = req.hard_packed;
+    c.hard_bits = req.hard_bits;
+    c.hard_words_stride = req.hard_words_stride;
+    c.iters = req.iters;
+    c.app_out = static_cast<int16_t*>(req.app);
+    c.app_stride = req.app_stride;
+    c.edge_r_out = static_cast<int8_t*>(req.edge_r);
+    c.edge_r_stride = req.edge_r_stride;
+    c.hard_out = req.hard;
+    c.hard_stride = req.hard_stride;
+    return nr_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream);
+  }
   const Geometry geo = geometry(p, req.batch);
   const long long groups = (req.batch + geo.cpb - 1) / geo.cpb;
   const long long ctas = std::min<long long>(groups, geo.max_ctas);

@@ -1,0 +1,416 @@
+// int8 LOMS decode specialised for the 5G NR base graphs (BG1, BG2), sm_100a.
+//
+// Same arithmetic as the generic kernel (syndrome src/qc_ldpc.rs:1530-1758, int8
+// messages, int16 posterior), restructured around three facts of the 5G graphs:
+//
+//  1. Layers >= 4 each own one extension parity column (column kb + layer, an
+//     unshifted identity) that no other layer touches.  Its posterior is
+//     channel + (that edge's message), so its variable-to-check message is the
+//     channel value clamped to +-127 in every iteration, and it needs no shared
+//     memory: the kernel keeps the int8 channel values of these columns and
+//     rebuilds their posteriors at the end.  Valid when app_clamp >= 255 (the
+//     posterior of such a column never reaches the clamp).
+//  2. The base graph is fixed at compile time, so the layer loop and each layer's
+//     edges are fully unrolled; each thread keeps the check-to-variable messages of
+//     its check rows compressed in registers: per row min1', min2' (offset
+//     magnitudes), the argmin edge and one sign bit per edge (the reference's
+//     messages are exactly this function, ties included).  The per-Z cyclic
+//     shifts arrive as kernel parameters (constant bank) and become index
+//     arithmetic on the shared-memory posterior.
+//  3. New magnitudes need no per-edge select: with S' = min1 + min2 - beta,
+//     |R_new| = max(min1', S' - |Q|): the argmin edge (|Q| = min1) gets min2',
+//     every other edge has |Q| >= min2 and gets min1' (ties give min2' = min1').
+//     min1 / min2 / argmin come from one min-pair over keys |Q| * 32 + edge.
+//
+// One thread per lifting index z of each codeword slot; a CTA holds `cpb`
+// codewords.  The syndrome check after each iteration tests layer 0 first (it
+// almost always fails before convergence) and the remaining layers only when
+// layer 0 passes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <type_traits>
+
+#include "nr_kernels.h"
+#include "nr_layered_tables.h"
+
+namespace syn {
+namespace nr {
+
+template <int BG>
+struct Tab;
+
+template <>
+struct Tab<0> {
+  static constexpr int MB = 46, NB = 68, KB = 22, E = 316;
+  __host__ __device__ static constexpr int loff(int i) { return syn_bg1_loff(i); }
+  __host__ __device__ static constexpr int col(int e) { return syn_bg1_lcol(e); }
+};
+
+template <>
+struct Tab<1> {
+  static constexpr int MB = 42, NB = 52, KB = 10, E = 197;
+  __host__ __device__ static constexpr int loff(int i) { return syn_bg2_loff(i); }
+  __host__ __device__ static constexpr int col(int e) { return syn_bg2_lcol(e); }
+};
+
+template <int BG>
+__host__ __device__ constexpr int deg_of(int l) {
+  return Tab<BG>::loff(l + 1) - Tab<BG>::loff(l);
+}
+// Compressed state words of a layer: one when signs (deg bits) fit below bit 13.
+template <int BG>
+__host__ __device__ constexpr int words_of(int l) {
+  return deg_of<BG>(l) <= 13 ? 1 : 2;
+}
+template <int BG>
+__host__ __device__ constexpr int word_off(int l) {
+  int w = 0;
+  for (int i = 0; i < l; ++i) w += words_of<BG>(i);
+  return w;
+}
+template <int BG>
+__host__ __device__ constexpr bool is_ext(int l, int e) {
+  return l >= 4 && Tab<BG>::col(Tab<BG>::loff(l) + e) == Tab<BG>::KB + l;
+}
+
+template <int BG>
+__host__ __device__ constexpr int ext_pos(int l) {
+  for (int e = 0; e < deg_of<BG>(l); ++e)
+    if (is_ext<BG>(l, e)) return e;
+  return -1;
+}
+
+template <int I, int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (I < N) {
+    f(std::integral_constant<int, I>{});
+    static_for<I + 1, N>(f);
+  }
+}
+
+template <int BG>
+struct Args {
+  NrCommon c;
+  int pa[Tab<BG>::E];  // col * z + shift
+  int pb[Tab<BG>::E];  // col * z + shift - z
+  int th[Tab<BG>::E];  // z - shift: lifting indices >= th wrap around
+};
+
+// Meta bits of a compressed row: argmin [13,18), min1' [18,25), min2' [25,32).
+__device__ __forceinline__ uint32_t pack_meta(int idx, int m1p, int m2p) {
+  return ((uint32_t)idx << 13) | ((uint32_t)m1p << 18) | ((uint32_t)m2p << 25);
+}
+
+// Message of edge e from a compressed row (sign word, meta word).
+__device__ __forceinline__ int row_message(uint32_t signs, uint32_t meta, int e) {
+  const int idx = (meta >> 13) & 31, m1p = (meta >> 18) & 127, m2p = meta >> 25;
+  const int mag = idx == e ? m2p : m1p;
+  return ((signs >> e) & 1u) ? -mag : mag;
+}
+
+// Compressed rows live in shared memory, word-major: word w of thread t at st[w * ns + t].
+template <int BG, bool CLAMP, int L>
+__device__ __forceinline__ void layer(const Args<BG>& a, int z, int16_t* __restrict__ A,
+                                      const int8_t* __restrict__ X, uint32_t* __restrict__ st, int ns,
+                                      int beta_q, int C) {
+  using T = Tab<BG>;
+  constexpr int lb = T::loff(L), deg = deg_of<BG>(L), W = word_off<BG>(L);
+  constexpr bool two = words_of<BG>(L) == 2;
+  const uint32_t w_signs = st[W * ns];
+  const uint32_t w_meta = two ? st[(W + 1) * ns] : w_signs;
+  const int idxo = (w_meta >> 13) & 31, m1o = (w_meta >> 18) & 127, m2o = w_meta >> 25;
+  const int Z = a.c.z;
+  int vidx[deg], u[deg], ab[deg];
+  int m1k = 4095, m2k = 4095;  // (127 << 5) | 31: the message ceiling, no edge
+  int sx = 0;
+  static_for<0, deg>([&](auto ei) {
+    constexpr int e = decltype(ei)::value;
+    if constexpr (is_ext<BG>(L, e)) {
+      const int q = max((int)X[(L - 4) * Z + z], -127);
+      u[e] = q;
+      ab[e] = abs(q);
+    } else {
+      const int vi = z + ((z >= a.th[lb + e]) ? a.pb[lb + e] : a.pa[lb + e]);
+      vidx[e] = vi;
+      const int app = A[vi];
+      int ro = idxo == e ? m2o : m1o;
+      ro = ((w_signs >> e) & 1u) ? -ro : ro;
+      u[e] = app - ro;
+      ab[e] = abs(u[e]);
+    }
+    sx ^= u[e];
+    const int key = (ab[e] << 5) | e;
+    m2k = min(m2k, max(m1k, key));
+    m1k = min(m1k, key);
+  });
+  const int m1 = m1k >> 5, m2 = m2k >> 5, idx = m1k & 31;
+  const int m1p = max(m1 - beta_q, 0), m2p = max(m2 - beta_q, 0), sp = m1 + m2 - beta_q;
+  uint32_t signs = 0;
+  static_for<0, deg>([&](auto ei) {
+    constexpr int e = decltype(ei)::value;
+    const bool neg = (u[e] ^ sx) < 0;
+    signs |= (uint32_t)neg << e;
+    if constexpr (!is_ext<BG>(L, e)) {
+      const int mag = max(m1p, sp - ab[e]);
+      int v = u[e] + (neg ? -mag : mag);
+      if (CLAMP) v = min(max(v, -C), C);
+      A[vidx[e]] = (int16_t)v;
+    }
+  });
+  const uint32_t meta = pack_meta(idx, m1p, m2p);
+  if constexpr (two) {
+    st[W * ns] = signs;
+    st[(W + 1) * ns] = meta;
+  } else {
+    st[W * ns] = signs | meta;
+  }
+}
+
+// Parity of check row (L, z) under the current posteriors: true if odd.
+template <int BG, int L>
+__device__ __forceinline__ bool row_parity(const Args<BG>& a, int z, const int16_t* __restrict__ A,
+                                           const int8_t* __restrict__ X, const uint32_t* __restrict__ st,
+                                           int ns) {
+  using T = Tab<BG>;
+  constexpr int lb = T::loff(L), deg = deg_of<BG>(L), W = word_off<BG>(L);
+  constexpr bool two = words_of<BG>(L) == 2;
+  unsigned par = 0;
+  static_for<0, deg>([&](auto ei) {
+    constexpr int e = decltype(ei)::value;
+    if constexpr (is_ext<BG>(L, e)) {
+      const uint32_t w0 = st[W * ns];
+      const int r = row_message(w0, two ? st[(W + 1) * ns] : w0, e);
+      par ^= ((int)X[(L - 4) * a.c.z + z] + r) < 0 ? 1u : 0u;
+    } else {
+      const int vi = z + ((z >= a.th[lb + e]) ? a.pb[lb + e] : a.pa[lb + e]);
+      par ^= A[vi] < 0 ? 1u : 0u;
+    }
+  });
+  return par != 0;
+}
+
+__host__ __device__ inline int al16(int x) { return (x + 15) & ~15; }
+
+template <int BG>
+__host__ __device__ inline int slot_bytes(int z) {
+  using T = Tab<BG>;
+  return al16((T::KB + 4) * z * 2) + al16((T::MB - 4) * z);
+}
+
+// Compressed-row state: word_off(MB) words per thread.
+template <int BG>
+__host__ __device__ inline int state_bytes(int threads) {
+  return word_off<BG>(Tab<BG>::MB) * threads * 4;
+}
+
+template <int BG, bool CLAMP>
+__global__ void __launch_bounds__(384, 2) nr_i8_kernel(const __grid_constant__ Args<BG> a) {
+  using T = Tab<BG>;
+  constexpr int NWT = word_off<BG>(T::MB);
+  extern __shared__ __align__(16) unsigned char smem[];
+  const NrCommon& c = a.c;
+  const int Z = c.z, N = T::NB * Z;
+  const int core_n = (T::KB + 4) * Z;
+  int* s_flag = reinterpret_cast<int*>(smem);
+  uint32_t* st = reinterpret_cast<uint32_t*>(smem + al16(c.cpb * 4)) + threadIdx.x;
+  const int ns = blockDim.x;
+  unsigned char* slots = smem + al16(c.cpb * 4) + state_bytes<BG>(blockDim.x);
+  const int sb = slot_bytes<BG>(Z);
+  const int slot = threadIdx.x / Z;
+  const int z = threadIdx.x - slot * Z;
+  const bool lane_ok = slot < c.cpb;
+  int16_t* A = reinterpret_cast<int16_t*>(slots + (lane_ok ? slot : 0) * sb);
+  int8_t* X = reinterpret_cast<int8_t*>(slots + (lane_ok ? slot : 0) * sb + al16(core_n * 2));
+  const int C = c.app_clamp;
+  const long long ngroups = (c.batch + c.cpb - 1) / c.cpb;
+  const bool vec_ok = (c.llr_stride % 16 == 0) && (c.llr_offset % 16 == 0) &&
+                      ((reinterpret_cast<uintptr_t>(c.llr) & 15) == 0);
+
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    __syncthreads();
+    // ---- load: channel LLRs -> int16 core posteriors / int8 extension channel values
+    for (int sl = 0; sl < c.cpb; ++sl) {
+      const long long cw = grp * c.cpb + sl;
+      if (cw >= c.batch) break;
+      const int8_t* src = c.llr + cw * c.llr_stride;
+      int16_t* As = reinterpret_cast<int16_t*>(slots + sl * sb);
+      int8_t* Xs = reinterpret_cast<int8_t*>(slots + sl * sb + al16(core_n * 2));
+      auto put = [&](int j, int v) {
+        if (c.prologue) {
+          if (j < 2 * Z)
+            v = 0;
+          else if (j >= c.k_prime && j < c.k)
+            v = C;
+        }
+        if (j < core_n)
+          As[j] = (int16_t)min(max(v, -C), C);
+        else
+          Xs[j - core_n] = (int8_t)v;
+      };
+      for (int j = threadIdx.x; j < c.llr_offset; j += blockDim.x) put(j, 0);
+      const int n_in = N - c.llr_offset;
+      if (vec_ok) {
+        const int nvec = n_in >> 4;
+        const uint4* s4 = reinterpret_cast<const uint4*>(src);
+        for (int q = threadIdx.x; q < nvec; q += blockDim.x) {
+          const uint4 w = s4[q];
+          const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            put(c.llr_offset + (q << 4) + i, (int)(int8_t)(ws[i >> 2] >> ((i & 3) * 8)));
+        }
+        for (int j = (nvec << 4) + threadIdx.x; j < n_in; j += blockDim.x) put(c.llr_offset + j, src[j]);
+      } else {
+        for (int j = threadIdx.x; j < n_in; j += blockDim.x) put(c.llr_offset + j, src[j]);
+      }
+    }
+    __syncthreads();
+
+    const long long cw = grp * c.cpb + slot;
+    bool active = lane_ok && cw < c.batch;
+#pragma unroll 1
+    for (int i = 0; i < NWT; ++i) st[i * ns] = 0;
+    int used = 0;
+    for (int it = 0; it < c.iterations; ++it) {
+      if (!__syncthreads_or(active)) break;
+      if (active) ++used;
+      static_for<0, T::MB>([&](auto li) {
+        constexpr int L = decltype(li)::value;
+        if (active) layer<BG, CLAMP, L>(a, z, A, X, st, ns, c.beta_q, C);
+        __syncthreads();
+      });
+      if (lane_ok && z == 0) s_flag[slot] = 0;
+      __syncthreads();
+      if (active && row_parity<BG, 0>(a, z, A, X, st, ns)) s_flag[slot] = 1;
+      __syncthreads();
+      if (active && s_flag[slot] == 0) {
+        bool odd = false;
+        static_for<1, T::MB>([&](auto li) {
+          constexpr int L = decltype(li)::value;
+          odd |= row_parity<BG, L>(a, z, A, X, st, ns);
+        });
+        if (odd) s_flag[slot] = 1;
+      }
+      __syncthreads();
+      if (active && s_flag[slot] == 0) active = false;
+    }
+
+    // ---- outputs
+    __syncthreads();
+    if (lane_ok && cw < c.batch) {
+      if (z == 0 && c.iters) c.iters[cw] = used;
+      static_for<4, T::MB>([&](auto li) {
+        constexpr int L = decltype(li)::value;
+        constexpr int W = word_off<BG>(L);
+        constexpr bool two = words_of<BG>(L) == 2;
+        constexpr int e_ext = ext_pos<BG>(L);
+        static_assert(e_ext >= 0, "every layer >= 4 has an extension column");
+        const uint32_t w0 = st[W * ns];
+        const int app = (int)X[(L - 4) * Z + z] + row_message(w0, two ? st[(W + 1) * ns] : w0, e_ext);
+        if (c.app_out) c.app_out[cw * c.app_stride + core_n + (L - 4) * Z + z] = (int16_t)app;
+        X[(L - 4) * Z + z] = app < 0 ? 1 : 0;
+      });
+      if (c.edge_r_out) {
+        int8_t* R = c.edge_r_out + cw * c.edge_r_stride;
+        static_for<0, T::MB>([&](auto li) {
+          constexpr int L = decltype(li)::value;
+          constexpr int W = word_off<BG>(L), lb = T::loff(L);
+          constexpr bool two = words_of<BG>(L) == 2;
+          static_for<0, deg_of<BG>(L)>([&](auto ei) {
+            constexpr int e = decltype(ei)::value;
+            const uint32_t w0 = st[W * ns];
+            R[(long long)(lb + e) * Z + z] = (int8_t)row_message(w0, two ? st[(W + 1) * ns] : w0, e);
+          });
+        });
+      }
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int sl = 0; sl < c.cpb; ++sl) {
+      const long long cwo = grp * c.cpb + sl;
+      if (cwo >= c.batch) break;
+      const int16_t* As = reinterpret_cast<const int16_t*>(slots + sl * sb);
+      const int8_t* Hs = reinterpret_cast<const int8_t*>(slots + sl * sb + al16(core_n * 2));
+      if (c.app_out)
+        for (int j = threadIdx.x; j < core_n; j += blockDim.x) c.app_out[cwo * c.app_stride + j] = As[j];
+      if (c.hard_out)
+        for (int j = threadIdx.x; j < N; j += blockDim.x)
+          c.hard_out[cwo * c.hard_stride + j] = j < core_n ? (As[j] < 0 ? 1 : 0) : (uint8_t)Hs[j - core_n];
+      if (c.hard_packed) {
+        const int nwords = (c.hard_bits + 31) >> 5;
+        uint32_t* dst = c.hard_packed + cwo * c.hard_words_stride;
+        for (int w = warp; w < nwords; w += nwarps) {
+          const int j = (w << 5) + lane;
+          bool bit = false;
+          if (j < c.hard_bits) bit = j < core_n ? As[j] < 0 : Hs[j - core_n] != 0;
+          const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+          if (lane == 0) dst[w] = m;
+        }
+      }
+    }
+  }
+}
+
+template <int BG>
+cudaError_t launch_bg(const NrCommon& c, const int* shifts, bool clamp, int sms, cudaStream_t stream,
+                      int* ctas_out) {
+  using T = Tab<BG>;
+  Args<BG> a;
+  a.c = c;
+  for (int e = 0; e < T::E; ++e) {
+    const int cz = T::col(e) * c.z;
+    a.pa[e] = cz + shifts[e];
+    a.pb[e] = cz + shifts[e] - c.z;
+    a.th[e] = c.z - shifts[e];
+  }
+  const int threads = ((c.cpb * c.z + 31) / 32) * 32;
+  const int smem = al16(c.cpb * 4) + state_bytes<BG>(threads) + c.cpb * slot_bytes<BG>(c.z);
+  auto fn = clamp ? nr_i8_kernel<BG, true> : nr_i8_kernel<BG, false>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+  if (e != cudaSuccess) return e;
+  const long long groups = (c.batch + c.cpb - 1) / c.cpb;
+  const long long ctas = std::min<long long>(groups, (long long)std::max(per_sm, 1) * sms);
+  if (ctas_out) *ctas_out = (int)ctas;
+  if (ctas <= 0) return cudaSuccess;
+  fn<<<(unsigned)ctas, threads, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace nr
+
+bool nr_layout_matches(int bg, const int* cols, int n_edges) {
+  if (bg == 0) {
+    if (n_edges != nr::Tab<0>::E) return false;
+    for (int e = 0; e < n_edges; ++e)
+      if (cols[e] != nr::Tab<0>::col(e)) return false;
+    return true;
+  }
+  if (bg == 1) {
+    if (n_edges != nr::Tab<1>::E) return false;
+    for (int e = 0; e < n_edges; ++e)
+      if (cols[e] != nr::Tab<1>::col(e)) return false;
+    return true;
+  }
+  return false;
+}
+
+int nr_cpb(int bg, int z) {
+  (void)bg;
+  return std::max(1, std::min(64, 384 / z));
+}
+
+cudaError_t nr_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream) {
+  // Posteriors stay inside +-3938 (|channel| <= 128, <= 30 messages of <= 127 per
+  // column) unless filler bits pin some at app_clamp or the clamp is below that.
+  const bool clamp = (c.prologue && c.k_prime < c.k) || c.app_clamp < 3938;
+  if (bg == 0) return nr::launch_bg<0>(c, shifts, clamp, sms, stream, nullptr);
+  return nr::launch_bg<1>(c, shifts, clamp, sms, stream, nullptr);
+}
+
+}  // namespace syn

@@ -200,6 +200,13 @@ class QcLdpcDecoder:
         return used.value
 
     # ---- batched GPU API (no reference counterpart) ----
+    KERNELS = {"auto": 0, "generic": 1, "nr": 2}
+
+    def set_kernel(self, kernel):
+        """Kernel used by int8 decodes: "auto", "generic" or "nr" (5G NR specialised)."""
+        _lib.check(_lib.load().syndrome_ldpc_decoder_set_kernel(self._h, self.KERNELS[kernel]))
+        return self
+
     def batch_workspace_size(self, batch, precision="int8"):
         p = _lib.PRECISION_F32 if precision == "f32" else _lib.PRECISION_INT8
         return int(_lib.load().syndrome_ldpc_batch_workspace_size(self._h, p, batch))

@@ -19,6 +19,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "..", "csrc", "base_graph_tables.inc")
+OUT_LAYERED = os.path.join(HERE, "..", "csrc", "nr_layered_tables.h")
 
 WIFI_RE = re.compile(
     r"const WIFI_Z(\d+)_R(\d)_(\d)_ENTRIES: \[\(u8, u8, i16\); (\d+)\] = \[(.*?)\];", re.S)
@@ -84,14 +85,48 @@ def render(bgs, wifi):
     return "\n".join(lines) + "\n"
 
 
+def render_layered(bgs):
+    """constexpr layered layout of BG1/BG2 (rows grouped, entry order kept), for the
+    kernels that unroll the base graph at compile time."""
+    lines = [
+        "// Layered (row-grouped) layout of the 5G NR base graphs as constexpr tables.",
+        "// Generated by syndrome_b200/tables/gen_base_graphs.py; do not edit.",
+        "// For layer l, edges loff(l)..loff(l+1)-1 have column col(e) and take their",
+        "// shift from base_graph_tables.inc entry ent(e) (the order of the reference's",
+        "// build_layout, src/qc_ldpc.rs:281-319).  Functions with local constexpr",
+        "// tables so that device code can evaluate them at compile time.",
+        "#pragma once",
+        "",
+    ]
+    for name in ("bg1", "bg2"):
+        rows, cols, ents = bgs[name]
+        order = []
+        for r in range(rows):
+            order += [i for i, (rr, _, _) in enumerate(ents) if rr == r]
+        off = [0]
+        for r in range(rows):
+            off.append(off[-1] + sum(1 for rr, _, _ in ents if rr == r))
+        up = name.upper()
+        for fn, vals in (("loff", off), ("lcol", [ents[i][1] for i in order]), ("lent", order)):
+            lines.append(f"__host__ __device__ constexpr int syn_{name}_{fn}(int i) {{")
+            lines.append(f"  constexpr int t[{len(vals)}] = {{{', '.join(str(x) for x in vals)}}};")
+            lines.append("  return t[i];")
+            lines.append("}")
+        lines.append("")
+    return "\n".join(lines) + "\n"
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SYNDROME_REFERENCE_ROOT")
     if not ref_root:
         raise SystemExit("usage: gen_base_graphs.py <reference-root>")
-    text = render(load_bg(ref_root), load_wifi(ref_root))
+    bgs = load_bg(ref_root)
+    text = render(bgs, load_wifi(ref_root))
     with open(OUT, "w") as f:
         f.write(text)
-    print("wrote", os.path.normpath(OUT))
+    with open(OUT_LAYERED, "w") as f:
+        f.write(render_layered(bgs))
+    print("wrote", os.path.normpath(OUT), "and", os.path.normpath(OUT_LAYERED))
 
 
 if __name__ == "__main__":

@@ -41,11 +41,15 @@ def oracle_i8(code, apps, beta_q, iters, app_clamp=32767):
     return [code.decode_i8(a, beta_q, iters, app_clamp) for a in apps]
 
 
-def gpu_i8(dec, llr_i8, iters, quant, **kw):
+def gpu_i8(dec, llr_i8, iters, quant, kernel="auto", **kw):
     t = torch.from_numpy(np.ascontiguousarray(llr_i8)).cuda()
+    dec.set_kernel(kernel)
     r = dec.decode_batch_i8(t, iters, quant=quant, want_app=True, want_edge_r=True, want_hard=True, **kw)
     torch.cuda.synchronize()
     return r
+
+
+KERNELS = ["generic", "nr"]
 
 
 def assert_i8_equal(label, ref, r):
@@ -65,8 +69,9 @@ def assert_i8_equal(label, ref, r):
     assert np.array_equal(bits, hard[:, : r.hard_bits]), f"{label}: packed hard bits differ"
 
 
-@pytest.mark.parametrize("bg,z", [(0, 7), (0, 44), (0, 96), (1, 13), (1, 52), (1, 128)])
-def test_int8_3gpp_graphs(bg, z):
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("bg,z", [(0, 2), (0, 7), (0, 44), (0, 96), (1, 13), (1, 52), (1, 128), (1, 384)])
+def test_int8_3gpp_graphs(bg, z, kernel):
     """tests/ldpc_int8_kernel_equivalence.rs:172-200 (12 iterations, beta 0.5, scale 8)."""
     code = O.Code.nr(bg, z)
     dec = S.QcLdpcDecoder.with_lifting_size(bg, z, 0.5)
@@ -75,17 +80,52 @@ def test_int8_3gpp_graphs(bg, z):
         _, llr = codewords(code, 4, ebno, 0x10000 ^ (z << 8))
         apps = np.stack([O.quantize_i16(x) for x in llr])
         ref = oracle_i8(code, apps, O.beta_q(0.5), 12)
-        r = gpu_i8(dec, apps.astype(np.int8), 12, q)
-        assert_i8_equal(f"bg{bg + 1} z{z} {ebno}dB", ref, r)
+        r = gpu_i8(dec, apps.astype(np.int8), 12, q, kernel)
+        assert_i8_equal(f"bg{bg + 1} z{z} {ebno}dB {kernel}", ref, r)
 
 
-def test_int8_bg1_z384():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_int8_bg1_z384(kernel):
     """tests/ldpc_int8_kernel_equivalence.rs:202-215 (BG1 Z=384 at 1 dB)."""
     code = O.Code.nr(0, 384)
     dec = S.QcLdpcDecoder.with_lifting_size(0, 384, 0.5)
     _, llr = codewords(code, 3, 1.0, 0x03840000)
     apps = np.stack([O.quantize_i16(x) for x in llr])
-    assert_i8_equal("bg1 z384", oracle_i8(code, apps, 4, 12), gpu_i8(dec, apps.astype(np.int8), 12, S.QuantParams()))
+    r = gpu_i8(dec, apps.astype(np.int8), 12, S.QuantParams(), kernel)
+    assert_i8_equal(f"bg1 z384 {kernel}", oracle_i8(code, apps, 4, 12), r)
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_int8_nr_punctured_filler_and_clamps(kernel):
+    """5G input without the punctured columns, filler bits, and clamps on both sides of
+    the bounds the 5G NR kernel relies on (255 and 3938)."""
+    for bg, z, n_filler in ((0, 64, 100), (1, 96, 3 * 96 // 2), (0, 384, 0)):
+        code = O.Code.nr(bg, z)
+        dec = S.QcLdpcDecoder.with_lifting_size(bg, z, 0.5)
+        info_len = code.k - n_filler
+        for clamp in (32767, 1000, 255):
+            rows, refs = [], []
+            for i in range(3):
+                info = np.concatenate([O.random_bits(50 + i, info_len), np.zeros(n_filler, np.uint8)])
+                cw = code.encode(info)
+                app = O.quantize_i16(O.awgn(cw, 1.0 + i, code.k / code.n, 7 + 31 * i))
+                rows.append(app[2 * z:].astype(np.int8))
+                full = np.concatenate([np.zeros(2 * z, np.int16), app[2 * z:]])
+                refs.append(code.decode_i8(code.prologue_5g_i8(full, n_filler, clamp), 4, 10, clamp))
+            r = gpu_i8(dec, np.stack(rows), 10, S.QuantParams().with_app_clamp(clamp), kernel, llr_offset=2 * z,
+                       nr_prologue=True, n_filler=n_filler, hard_bits=code.k - n_filler)
+            assert_i8_equal(f"bg{bg + 1} z{z} filler{n_filler} clamp{clamp} {kernel}", refs, r)
+
+
+def test_int8_nr_kernel_rejects_what_it_cannot_serve():
+    dec = S.QcLdpcDecoder.with_lifting_size(1, 16, 0.5).set_kernel("nr")
+    t = torch.zeros((2, dec.variable_node_count()), dtype=torch.int8, device="cuda")
+    with pytest.raises(S.FecError) as e:
+        dec.decode_batch_i8(t, 5, quant=S.QuantParams().with_app_clamp(127))
+    assert e.value.status == _lib.INVALID_PARAM
+    w = S.wifi_ldpc_decoder(27, 1, 2, 0.5).set_kernel("nr")
+    with pytest.raises(S.FecError):
+        w.decode_batch_i8(torch.zeros((1, w.variable_node_count()), dtype=torch.int8, device="cuda"), 5)
 
 
 def test_int8_wifi_matrices():
@@ -131,14 +171,16 @@ def test_int8_5g_prologue_with_filler():
         assert_i8_equal(f"5g prologue clamp {clamp}", [ref], r)
 
 
-def test_int8_zero_iterations_and_many_codewords():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_int8_zero_iterations_and_many_codewords(kernel):
     code = O.Code.nr(1, 16)
     dec = S.QcLdpcDecoder.with_lifting_size(1, 16, 0.5)
     _, llr = codewords(code, 40, 2.0, 77)
     apps = np.stack([O.quantize_i16(x) for x in llr])
     for iters in (0, 1, 3, 20):
         ref = oracle_i8(code, apps, 4, iters)
-        assert_i8_equal(f"iters {iters}", ref, gpu_i8(dec, apps.astype(np.int8), iters, S.QuantParams()))
+        assert_i8_equal(f"iters {iters} {kernel}", ref, gpu_i8(dec, apps.astype(np.int8), iters, S.QuantParams(),
+                                                             kernel))
 
 
 def test_int8_host_api_drop_in():
