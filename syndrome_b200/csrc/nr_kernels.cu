@@ -23,9 +23,9 @@
 //     min1 / min2 / argmin come from one min-pair over keys |Q| * 32 + edge.
 //
 // One thread per lifting index z of each codeword slot; a CTA holds `cpb`
-// codewords.  The syndrome check after each iteration tests layer 0 first (it
-// almost always fails before convergence) and the remaining layers only when
-// layer 0 passes.
+// codewords.  The syndrome check after each iteration tests the smallest layer
+// first (it almost always fails before convergence) and the remaining layers only
+// when that one passes.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -81,6 +81,15 @@ __host__ __device__ constexpr int ext_pos(int l) {
   for (int e = 0; e < deg_of<BG>(l); ++e)
     if (is_ext<BG>(l, e)) return e;
   return -1;
+}
+
+// Layer with the fewest edges: checked first after every iteration.
+template <int BG>
+__host__ __device__ constexpr int quick_layer() {
+  int best = 0;
+  for (int l = 1; l < Tab<BG>::MB; ++l)
+    if (deg_of<BG>(l) < deg_of<BG>(best)) best = l;
+  return best;
 }
 
 template <int I, int N, class F>
@@ -207,7 +216,7 @@ __host__ __device__ inline int state_bytes(int threads) {
 }
 
 template <int BG, bool CLAMP>
-__global__ void __launch_bounds__(384, 2) nr_i8_kernel(const __grid_constant__ Args<BG> a) {
+__global__ void __launch_bounds__(768, 1) nr_i8_kernel(const __grid_constant__ Args<BG> a) {
   using T = Tab<BG>;
   constexpr int NWT = word_off<BG>(T::MB);
   extern __shared__ __align__(16) unsigned char smem[];
@@ -284,13 +293,14 @@ __global__ void __launch_bounds__(384, 2) nr_i8_kernel(const __grid_constant__ A
       });
       if (lane_ok && z == 0) s_flag[slot] = 0;
       __syncthreads();
-      if (active && row_parity<BG, 0>(a, z, A, X, st, ns)) s_flag[slot] = 1;
+      constexpr int QL = quick_layer<BG>();
+      if (active && row_parity<BG, QL>(a, z, A, X, st, ns)) s_flag[slot] = 1;
       __syncthreads();
       if (active && s_flag[slot] == 0) {
         bool odd = false;
-        static_for<1, T::MB>([&](auto li) {
+        static_for<0, T::MB>([&](auto li) {
           constexpr int L = decltype(li)::value;
-          odd |= row_parity<BG, L>(a, z, A, X, st, ns);
+          if constexpr (L != QL) odd |= row_parity<BG, L>(a, z, A, X, st, ns);
         });
         if (odd) s_flag[slot] = 1;
       }
@@ -400,9 +410,11 @@ bool nr_layout_matches(int bg, const int* cols, int n_edges) {
   return false;
 }
 
+// One 768-thread CTA per SM: every warp of the SM runs the same layer's code between
+// barriers, which keeps the unrolled base graph's instruction working set small.
 int nr_cpb(int bg, int z) {
   (void)bg;
-  return std::max(1, std::min(64, 384 / z));
+  return std::max(1, std::min(64, 768 / z));
 }
 
 cudaError_t nr_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream) {
