@@ -193,6 +193,30 @@ int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const
                                        size_t app_stride, float* d_edge_r, size_t edge_r_stride,
                                        uint8_t* d_hard, size_t hard_stride, void* d_workspace,
                                        size_t workspace_bytes, void* stream);
+/* Allocation-free batched int8 decode.  No counterpart in the reference.
+ * For callers that cannot allocate device memory while decoding: a baseband thread
+ * working to a per-slot deadline must not call cudaMalloc (it can synchronise the
+ * device and take milliseconds), and a plug-in inside an application that owns all
+ * device allocations has no allocator to call.  Same arguments and results as
+ * syndrome_ldpc_decode_batch_i8 without the workspace: the generic int8 kernel keeps
+ * its messages in a static device array of SYNDROME_NOALLOC_SCRATCH_BYTES that every
+ * GPU loading this library holds until exit.  A launch runs at most
+ * SYNDROME_NOALLOC_SCRATCH_BYTES / (codewords per CTA * edges * Z) CTAs; a code whose
+ * per-CTA messages exceed the array is rejected with SYNDROME_INVALID_PARAM.  The
+ * first call on a device looks up the array's address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture.  Nothing in the array must start at zero
+ * and it keeps the last call's contents; calls that overlap on the GPU share the
+ * array and race.  The current device must be the decoder's. */
+#define SYNDROME_NOALLOC_SCRATCH_BYTES (32u << 20)
+int32_t syndrome_ldpc_decode_batch_i8_noalloc(const SyndromeLdpcDecoder* decoder,
+                                              const int8_t* d_llr, size_t llr_stride,
+                                              size_t llr_offset, size_t batch, int32_t nr_prologue,
+                                              size_t n_filler, size_t iterations, float scale,
+                                              int16_t app_clamp, uint32_t* d_hard_packed,
+                                              size_t hard_bits, size_t hard_words_stride,
+                                              int32_t* d_iters, int16_t* d_app, size_t app_stride,
+                                              int8_t* d_edge_r, size_t edge_r_stride,
+                                              uint8_t* d_hard, size_t hard_stride, void* stream);
 /* Kernel selection for this decoder's batched int8 decodes: 0 = automatic (the
  * 5G NR kernel when it applies, else the generic layered kernel), 1 = always the
  * generic kernel, 2 = require the 5G NR kernel (INVALID_PARAM on a request it

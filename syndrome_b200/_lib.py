@@ -61,6 +61,8 @@ PROTOTYPES = {
     "syndrome_ldpc_decode_batch_f32": (_i32, [_vp, _vp, _sz, _sz, _sz, _i32, _sz, _sz,
                                               _vp, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _vp]),
     "syndrome_ldpc_decoder_set_kernel": (_i32, [_vp, _i32]),
+    "syndrome_ldpc_decode_batch_i8_noalloc": (_i32, [_vp, _vp, _sz, _sz, _sz, _i32, _sz, _sz, _f32, ctypes.c_int16,
+                                                     _vp, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz, _vp]),
     "syndrome_last_error": (ctypes.c_char_p, []),
 }
 

@@ -513,6 +513,54 @@ int32_t syndrome_ldpc_decode_batch_i8(const SyndromeLdpcDecoder* decoder, const 
   });
 }
 
+int32_t syndrome_ldpc_decode_batch_i8_noalloc(const SyndromeLdpcDecoder* decoder, const int8_t* d_llr,
+                                              size_t llr_stride, size_t llr_offset, size_t batch,
+                                              int32_t nr_prologue, size_t n_filler, size_t iterations,
+                                              float scale, int16_t app_clamp, uint32_t* d_hard_packed,
+                                              size_t hard_bits, size_t hard_words_stride, int32_t* d_iters,
+                                              int16_t* d_app, size_t app_stride, int8_t* d_edge_r,
+                                              size_t edge_r_stride, uint8_t* d_hard, size_t hard_stride,
+                                              void* stream) {
+  return guard([&]() -> int32_t {
+    if (!decoder || (!d_llr && batch)) return SYNDROME_NULL_POINTER;
+    const syn::Graph& g = decoder->graph;
+    const size_t n = (size_t)g.n();
+    if (llr_offset > n) return fail(SYNDROME_INVALID_PARAM, "llr_offset exceeds N");
+    if (llr_stride < n - llr_offset) return fail(SYNDROME_INVALID_PARAM, "llr_stride smaller than N - llr_offset");
+    if (d_app && app_stride < n) return fail(SYNDROME_INVALID_PARAM, "app_stride smaller than N");
+    if (d_hard && hard_stride < n) return fail(SYNDROME_INVALID_PARAM, "hard_stride smaller than N");
+    if (d_edge_r && edge_r_stride < (size_t)g.edge_buffer())
+      return fail(SYNDROME_INVALID_PARAM, "edge_r_stride smaller than the edge buffer");
+    if (d_hard_packed && (hard_bits > n || hard_words_stride < (hard_bits + 31) / 32))
+      return fail(SYNDROME_INVALID_PARAM, "hard_bits / hard_words_stride out of range");
+    if (iterations > (size_t)INT_MAX || batch > (size_t)LLONG_MAX / 2)
+      return fail(SYNDROME_INVALID_PARAM, "size out of range");
+    syn::BatchRequest r;
+    r.llr = d_llr;
+    r.llr_stride = (long long)llr_stride;
+    r.llr_offset = (int)llr_offset;
+    r.batch = (long long)batch;
+    r.iterations = (int)iterations;
+    r.prologue_5g = nr_prologue ? 1 : 0;
+    r.n_filler = (long long)std::min<size_t>(n_filler, (size_t)1 << 40);
+    r.beta_q = syn::beta_q(decoder->dec.offset_beta(), scale);
+    r.app_clamp = std::max<int>(app_clamp, 0);
+    r.hard_packed = d_hard_packed;
+    r.hard_bits = (int)hard_bits;
+    r.hard_words_stride = (long long)hard_words_stride;
+    r.iters = d_iters;
+    r.app = d_app;
+    r.app_stride = (long long)app_stride;
+    r.edge_r = d_edge_r;
+    r.edge_r_stride = (long long)edge_r_stride;
+    r.hard = d_hard;
+    r.hard_stride = (long long)hard_stride;
+    std::string msg;
+    cudaError_t e = decoder->dec.decode_i8_noalloc(r, static_cast<cudaStream_t>(stream), &msg);
+    return from_cuda(e, msg);
+  });
+}
+
 int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const float* d_llr,
                                        size_t llr_stride, size_t llr_offset, size_t batch,
                                        int32_t nr_prologue, size_t n_filler, size_t iterations,

@@ -70,6 +70,11 @@ class Decoder {
   cudaError_t decode(Precision p, const BatchRequest& req, cudaStream_t stream,
                      std::string* err) const;
 
+  // Generic int8 decode with its message scratch in a static device array instead
+  // of a caller workspace: allocates nothing.  See ldpc_kernels.cu for the limits.
+  cudaError_t decode_i8_noalloc(const BatchRequest& req, cudaStream_t stream, std::string* err) const;
+  static size_t noalloc_scratch_bytes();
+
   // Kernel launch geometry chosen for this code (exposed for the tuner and tests).
   struct Geometry {
     int cpb;          // codewords per CTA

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "decoder.h"
@@ -574,6 +575,116 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
   a.hard_out = req.hard;
   a.hard_stride = req.hard_stride;
   KernelFn fn = kernel_for(p, geo.maxdeg_tmpl);
+  fn<<<(unsigned)ctas, geo.threads, geo.smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry (syndrome_ldpc_decode_batch_i8_noalloc).
+//
+// Some callers cannot allocate device memory at decode time: a baseband thread
+// working to a per-slot deadline must not call cudaMalloc, which can synchronise
+// the device and take milliseconds, and a plug-in hosted by an application that
+// owns every device allocation has no allocator to call.  This entry runs the
+// generic int8 kernel above with its message scratch in the static array below,
+// which every GPU that loads this library holds until the process exits.
+//
+// The scratch holds the check-to-variable messages of the CTAs resident at once.
+// A launch uses at most kNoAllocScratchBytes / (codewords per CTA x edges x Z)
+// CTAs (the persistent kernel walks the batch with however many it gets); a code
+// whose messages for one CTA exceed the array is rejected.  The kernel writes
+// every message before it reads it within a decode, so nothing in the array has
+// to start at zero, and the array keeps the last call's contents.  Calls that
+// overlap on the GPU (different streams, or different host threads without
+// ordering) share the array and race.
+
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+static __device__ __align__(256) int8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of the static scratch on the current device, looked up once per
+// device (the first call on a device does the lookup).
+static cudaError_t noalloc_scratch(int device, void** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[device] = p;
+  }
+  *out = g_noalloc_addr[device];
+  return cudaSuccess;
+}
+
+size_t Decoder::noalloc_scratch_bytes() { return kNoAllocScratchBytes; }
+
+cudaError_t Decoder::decode_i8_noalloc(const BatchRequest& req, cudaStream_t stream, std::string* err) const {
+  auto bad = [&](const std::string& m) {
+    if (err) *err = m;
+    return cudaErrorInvalidValue;
+  };
+  if (req.batch < 0) return bad("batch must be non-negative");
+  if (req.batch == 0) return cudaSuccess;
+  if (!req.llr) return bad("llr is null");
+  if (req.iterations < 0) return bad("iterations must be non-negative");
+  if (req.llr_offset < 0 || req.llr_offset > g_.n()) return bad("llr_offset out of range");
+  if (req.hard_packed && (req.hard_bits < 0 || req.hard_bits > g_.n() ||
+                          req.hard_words_stride < (req.hard_bits + 31) / 32))
+    return bad("hard_bits / hard_words_stride out of range");
+  if (req.app_clamp < 0) return bad("app_clamp must be non-negative");
+  int cur = -1;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return e;
+  if (cur != device_) return bad("the current device is not the decoder's device");
+  void* scratch = nullptr;
+  e = noalloc_scratch(cur, &scratch);
+  if (e != cudaSuccess) return e;
+  const Geometry geo = geometry(Precision::kInt8, req.batch);
+  const long long per_cta = (long long)geo.cpb * g_.edge_buffer();
+  if (per_cta > (long long)kNoAllocScratchBytes)
+    return bad("the messages of one CTA (" + std::to_string(per_cta) + " bytes) exceed the " +
+               std::to_string(kNoAllocScratchBytes) + "-byte static scratch of the allocation-free entry");
+  const long long groups = (req.batch + geo.cpb - 1) / geo.cpb;
+  const long long fit = (long long)kNoAllocScratchBytes / per_cta;
+  const long long ctas = std::min<long long>(std::min<long long>(groups, geo.max_ctas), fit);
+  KArgs a{};
+  a.z = g_.z;
+  a.mb = g_.mb;
+  a.n_edges = g_.edges();
+  a.n = (int)g_.n();
+  a.k = (int)g_.k();
+  a.edge = d_edge_;
+  a.loff = d_loff_;
+  a.llr = req.llr;
+  a.llr_stride = req.llr_stride;
+  a.llr_offset = req.llr_offset;
+  a.llr_i16 = req.llr_i16;
+  a.batch = req.batch;
+  a.cpb = geo.cpb;
+  a.iterations = req.iterations;
+  a.beta_q = req.beta_q;
+  a.app_clamp = req.app_clamp;
+  a.beta = req.beta;
+  a.prologue = req.prologue_5g;
+  a.k_prime = req.n_filler > g_.k() ? 0 : g_.k() - req.n_filler;
+  a.r_out = req.edge_r;
+  a.r_out_stride = req.edge_r_stride;
+  a.r_ws = scratch;
+  a.hard_packed = req.hard_packed;
+  a.hard_bits = req.hard_bits;
+  a.hard_words_stride = req.hard_words_stride;
+  a.iters = req.iters;
+  a.app_out = req.app;
+  a.app_stride = req.app_stride;
+  a.hard_out = req.hard;
+  a.hard_stride = req.hard_stride;
+  KernelFn fn = kernel_for(Precision::kInt8, geo.maxdeg_tmpl);
   fn<<<(unsigned)ctas, geo.threads, geo.smem, stream>>>(a);
   return cudaGetLastError();
 }
