@@ -103,9 +103,8 @@ __device__ __forceinline__ void static_for(F&& f) {
 template <int BG>
 struct Args {
   NrCommon c;
-  int pa[Tab<BG>::E];  // col * z + shift
-  int pb[Tab<BG>::E];  // col * z + shift - z
-  int th[Tab<BG>::E];  // z - shift: lifting indices >= th wrap around
+  int sh[Tab<BG>::E];  // shift of each edge (reduced mod z)
+  int cz[Tab<BG>::E];  // col * z: first shared-memory posterior of the edge's column
 };
 
 // Meta bits of a compressed row: argmin [13,18), min1' [18,25), min2' [25,32).
@@ -120,18 +119,32 @@ __device__ __forceinline__ int row_message(uint32_t signs, uint32_t meta, int e)
   return ((signs >> e) & 1u) ? -mag : mag;
 }
 
+// Top bit of x as 0 or 1, computed as the high word of x * two (two == 2 at run time),
+// i.e. an IMAD.HI on the FMA pipe instead of a shift on the ALU pipe.
+__device__ __forceinline__ int top_bit(int x, unsigned two) { return (int)__umulhi((unsigned)x, two); }
+
 // Compressed rows live in shared memory, word-major: word w of thread t at st[w * ns + t].
+//
+// Instruction budget: on sm_100 every integer logic, shift, select, compare and
+// min/max instruction issues to the ALU pipe (two warp instructions per clock per
+// SM), as do plain integer adds, while IMAD issues to the FMA pipe at the same rate.
+// The sign algebra below therefore uses multiplications by +-1: with
+// sigma = (-1)^(sign bit of the row's XOR), R_new = sigma * (1 - 2*bit(u_e)) * mag_e,
+// and the sign bits of the new messages are accumulated as acc -= sgn_e * 2^e
+// (acc starting at 2^deg - 1 gives acc = 2 * sum(bit_e * 2^e)).
 template <int BG, bool CLAMP, int L>
 __device__ __forceinline__ void layer(const Args<BG>& a, int z, int16_t* __restrict__ A,
                                       const int8_t* __restrict__ X, uint32_t* __restrict__ st, int ns,
                                       int beta_q, int C) {
   using T = Tab<BG>;
   constexpr int lb = T::loff(L), deg = deg_of<BG>(L), W = word_off<BG>(L);
-  constexpr bool two = words_of<BG>(L) == 2;
+  constexpr bool two_words = words_of<BG>(L) == 2;
   const uint32_t w_signs = st[W * ns];
-  const uint32_t w_meta = two ? st[(W + 1) * ns] : w_signs;
+  const uint32_t w_meta = two_words ? st[(W + 1) * ns] : w_signs;
   const int idxo = (w_meta >> 13) & 31, m1o = (w_meta >> 18) & 127, m2o = w_meta >> 25;
   const int Z = a.c.z;
+  const int k32 = a.c.k32;
+  const unsigned two = (unsigned)a.c.two;
   int vidx[deg], u[deg], ab[deg];
   int m1k = 4095, m2k = 4095;  // (127 << 5) | 31: the message ceiling, no edge
   int sx = 0;
@@ -142,35 +155,40 @@ __device__ __forceinline__ void layer(const Args<BG>& a, int z, int16_t* __restr
       u[e] = q;
       ab[e] = abs(q);
     } else {
-      const int vi = z + ((z >= a.th[lb + e]) ? a.pb[lb + e] : a.pa[lb + e]);
+      // (z + shift) mod Z as an unsigned min: below Z the second candidate wraps high.
+      const unsigned r = (unsigned)(z + a.sh[lb + e]);
+      const unsigned rr = min(r, r - (unsigned)Z);
+      const int vi = (int)rr + a.cz[lb + e];
       vidx[e] = vi;
       const int app = A[vi];
-      int ro = idxo == e ? m2o : m1o;
-      ro = ((w_signs >> e) & 1u) ? -ro : ro;
-      u[e] = app - ro;
+      const int mag = idxo == e ? m2o : m1o;
+      u[e] = ((w_signs >> e) & 1u) ? app + mag : app - mag;  // app - R_old
       ab[e] = abs(u[e]);
     }
     sx ^= u[e];
-    const int key = (ab[e] << 5) | e;
+    const int key = ab[e] * k32 + e;
     m2k = min(m2k, max(m1k, key));
     m1k = min(m1k, key);
   });
   const int m1 = m1k >> 5, m2 = m2k >> 5, idx = m1k & 31;
   const int m1p = max(m1 - beta_q, 0), m2p = max(m2 - beta_q, 0), sp = m1 + m2 - beta_q;
-  uint32_t signs = 0;
+  const int sigma = 1 - 2 * top_bit(sx, two);
+  const int m2sigma = -2 * sigma;
+  int acc = (1 << deg) - 1;
   static_for<0, deg>([&](auto ei) {
     constexpr int e = decltype(ei)::value;
-    const bool neg = (u[e] ^ sx) < 0;
-    signs |= (uint32_t)neg << e;
+    const int sgn = top_bit(u[e], two) * m2sigma + sigma;  // sign of R_new
+    acc -= sgn * (1 << e);
     if constexpr (!is_ext<BG>(L, e)) {
       const int mag = max(m1p, sp - ab[e]);
-      int v = u[e] + (neg ? -mag : mag);
+      int v = mag * sgn + u[e];
       if (CLAMP) v = min(max(v, -C), C);
       A[vidx[e]] = (int16_t)v;
     }
   });
+  const uint32_t signs = (uint32_t)acc >> 1;
   const uint32_t meta = pack_meta(idx, m1p, m2p);
-  if constexpr (two) {
+  if constexpr (two_words) {
     st[W * ns] = signs;
     st[(W + 1) * ns] = meta;
   } else {
@@ -194,7 +212,8 @@ __device__ __forceinline__ bool row_parity(const Args<BG>& a, int z, const int16
       const int r = row_message(w0, two ? st[(W + 1) * ns] : w0, e);
       par ^= ((int)X[(L - 4) * a.c.z + z] + r) < 0 ? 1u : 0u;
     } else {
-      const int vi = z + ((z >= a.th[lb + e]) ? a.pb[lb + e] : a.pa[lb + e]);
+      const unsigned r = (unsigned)(z + a.sh[lb + e]);
+      const int vi = (int)min(r, r - (unsigned)a.c.z) + a.cz[lb + e];
       par ^= A[vi] < 0 ? 1u : 0u;
     }
   });
@@ -370,11 +389,11 @@ cudaError_t launch_bg(const NrCommon& c, const int* shifts, bool clamp, int sms,
   using T = Tab<BG>;
   Args<BG> a;
   a.c = c;
+  a.c.k32 = 32;
+  a.c.two = 2;
   for (int e = 0; e < T::E; ++e) {
-    const int cz = T::col(e) * c.z;
-    a.pa[e] = cz + shifts[e];
-    a.pb[e] = cz + shifts[e] - c.z;
-    a.th[e] = c.z - shifts[e];
+    a.sh[e] = shifts[e];
+    a.cz[e] = T::col(e) * c.z;
   }
   const int threads = ((c.cpb * c.z + 31) / 32) * 32;
   const int smem = al16(c.cpb * 4) + state_bytes<BG>(threads) + c.cpb * slot_bytes<BG>(c.z);

@@ -32,6 +32,9 @@ struct NrCommon {
   long long edge_r_stride;
   uint8_t* hard_out;
   long long hard_stride;
+  // Run-time constants (set by the launcher) that keep multiplies on the FMA pipe.
+  int k32;
+  int two;
 };
 
 // True if the layer-ordered column list equals the compiled BG tables.
