@@ -222,6 +222,47 @@ int32_t syndrome_ldpc_decode_batch_i8_noalloc(const SyndromeLdpcDecoder* decoder
  * generic kernel, 2 = require the 5G NR kernel (INVALID_PARAM on a request it
  * cannot serve).  Both kernels produce identical results. */
 int32_t syndrome_ldpc_decoder_set_kernel(SyndromeLdpcDecoder* decoder, int32_t kernel);
+/* ----------------------------------------------- mixed-shape batches ---- */
+/* One codeword of a mixed 5G NR int8 batch.  No counterpart in the reference
+ * (it decodes one code block per call).  Its int8 LLRs cover variables 2Z..N (the
+ * circular buffer of rate matching; the first 2Z columns are punctured) and start
+ * llr_offset bytes into the batch's LLR buffer; its hard decisions of variables
+ * 0..hard_bits-1 are written LSB-first from word out_offset of the output. */
+typedef struct {
+  int32_t base_graph; /* 0 = BG1, 1 = BG2 */
+  int32_t z;          /* lifting size */
+  int32_t n_filler;   /* filler bits K - K' (decode_5g_i8 prologue) */
+  int32_t hard_bits;  /* leading variables reported, e.g. K' information bits */
+  int64_t llr_offset;
+  int64_t out_offset;
+} SyndromeMixedCodeword;
+
+typedef struct SyndromeMixedPlan SyndromeMixedPlan;
+
+/* Plans a batch of codewords of any BG / Z mix for one persistent launch: groups
+ * equal shapes into work items of at most a tile of codewords (tile_hints: n_hints
+ * triples (base_graph, z, tile), nullable; default = what one CTA holds), orders the
+ * items by decreasing work and uploads the tables.  int8 LOMS with beta_q =
+ * round(offset_beta * scale), app_clamp >= 255, at most `iterations` iterations with
+ * early stop. */
+int32_t syndrome_mixed_plan_create(const SyndromeMixedCodeword* codewords, size_t count, float offset_beta,
+                                   float scale, int16_t app_clamp, size_t iterations,
+                                   const int32_t* tile_hints, size_t n_hints, SyndromeMixedPlan** out_plan);
+void syndrome_mixed_plan_destroy(SyndromeMixedPlan* plan);
+/* Number of work items; out_items (nullable, room for `cap` items) receives
+ * (base_graph, z, codewords) per item in launch order. */
+int32_t syndrome_mixed_plan_items(const SyndromeMixedPlan* plan, int32_t* out_items, size_t cap, size_t* n_items);
+/* Most codewords one work item of this shape can hold. */
+int32_t syndrome_mixed_tile_capacity(int32_t base_graph, int32_t z);
+/* Decodes the planned batch from device LLRs (llr_bytes long) into d_hard_packed
+ * (out_words long); d_iters (nullable, iters_len entries) receives the iterations of
+ * codeword i at index i.  Buffers shorter than the plan's offsets need give
+ * SYNDROME_BUFFER_TOO_SMALL.  use_graph != 0 captures the launch into a CUDA graph on
+ * first use (per buffer set) and replays it afterwards. */
+int32_t syndrome_mixed_decode(SyndromeMixedPlan* plan, const int8_t* d_llr, size_t llr_bytes,
+                              uint32_t* d_hard_packed, size_t out_words, int32_t* d_iters, size_t iters_len,
+                              int32_t use_graph, void* stream);
+
 /* Text of the last error on this thread (empty if none). */
 const char* syndrome_last_error(void);
 

@@ -25,4 +25,6 @@ from .qc_ldpc import (  # noqa: F401
     wifi_ldpc_encoder,
 )
 
+from .mixed import CODEWORD_DTYPE, LIFTING_SIZES, MixedBatch, code_dims, tile_capacity  # noqa: F401,E402
+
 __version__ = "0.1.0"

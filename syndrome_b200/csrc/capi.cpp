@@ -19,6 +19,7 @@
 #include "decoder.h"
 #include "encoder.h"
 #include "graph.h"
+#include "mixed.h"
 
 struct SyndromeLdpcDecoder {
   syn::Graph graph;
@@ -34,6 +35,10 @@ struct SyndromeLdpcDecoder {
 
 struct SyndromeLdpcEncoder {
   syn::Encoder enc;
+};
+
+struct SyndromeMixedPlan {
+  syn::MixedPlan plan;
 };
 
 namespace {
@@ -574,6 +579,75 @@ int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const
                         nr_prologue, n_filler, iterations, 8.0f, 0, d_hard_packed, hard_bits,
                         hard_words_stride, d_iters, d_app, app_stride, d_edge_r, edge_r_stride, d_hard,
                         hard_stride, d_workspace, workspace_bytes, stream);
+  });
+}
+
+// ------------------------------------------------------- mixed batches ------
+
+int32_t syndrome_mixed_plan_create(const SyndromeMixedCodeword* codewords, size_t count, float offset_beta,
+                                   float scale, int16_t app_clamp, size_t iterations,
+                                   const int32_t* tile_hints, size_t n_hints, SyndromeMixedPlan** out_plan) {
+  return guard([&]() -> int32_t {
+    if (!out_plan || (!codewords && count) || (!tile_hints && n_hints)) return SYNDROME_NULL_POINTER;
+    *out_plan = nullptr;
+    if (iterations > (size_t)INT_MAX || count > (size_t)INT_MAX / 2) return fail(SYNDROME_INVALID_PARAM, "size out of range");
+    std::vector<syn::MixedCodeword> cws(count);
+    for (size_t i = 0; i < count; ++i) {
+      const SyndromeMixedCodeword& c = codewords[i];
+      cws[i] = syn::MixedCodeword{c.base_graph, c.z, c.n_filler, c.hard_bits, (long long)c.llr_offset,
+                                  (long long)c.out_offset};
+    }
+    std::vector<syn::TileHint> hints(n_hints);
+    for (size_t i = 0; i < n_hints; ++i) hints[i] = syn::TileHint{tile_hints[3 * i], tile_hints[3 * i + 1], tile_hints[3 * i + 2]};
+    auto* p = new SyndromeMixedPlan();
+    std::string err;
+    if (!p->plan.init(cws, syn::beta_q(offset_beta, scale), std::max<int>(app_clamp, 0), (int)iterations, hints, &err)) {
+      delete p;
+      cudaGetLastError();
+      return fail(err.find("CUDA") != std::string::npos || err.find("cuda") != std::string::npos
+                      ? SYNDROME_CUDA_ERROR
+                      : SYNDROME_INVALID_PARAM,
+                  err);
+    }
+    *out_plan = p;
+    return SYNDROME_OK;
+  });
+}
+
+void syndrome_mixed_plan_destroy(SyndromeMixedPlan* plan) { delete plan; }
+
+int32_t syndrome_mixed_plan_items(const SyndromeMixedPlan* plan, int32_t* out_items, size_t cap, size_t* n_items) {
+  if (!plan || !n_items) return SYNDROME_NULL_POINTER;
+  const auto& items = plan->plan.item_list();
+  *n_items = items.size();
+  if (out_items)
+    for (size_t i = 0; i < items.size() && i < cap; ++i) {
+      out_items[3 * i] = items[i].bg;
+      out_items[3 * i + 1] = items[i].z;
+      out_items[3 * i + 2] = items[i].count;
+    }
+  return SYNDROME_OK;
+}
+
+int32_t syndrome_mixed_tile_capacity(int32_t base_graph, int32_t z) {
+  if ((base_graph != 0 && base_graph != 1) || syn::lifting_set_index(z) < 0) return 0;
+  return syn::mixed_slot_capacity(base_graph, z);
+}
+
+int32_t syndrome_mixed_decode(SyndromeMixedPlan* plan, const int8_t* d_llr, size_t llr_bytes,
+                              uint32_t* d_hard_packed, size_t out_words, int32_t* d_iters, size_t iters_len,
+                              int32_t use_graph, void* stream) {
+  return guard([&]() -> int32_t {
+    if (!plan || !d_llr || !d_hard_packed) return SYNDROME_NULL_POINTER;
+    if ((long long)llr_bytes < plan->plan.llr_bytes_needed())
+      return fail(SYNDROME_BUFFER_TOO_SMALL, "LLR buffer shorter than the planned offsets");
+    if ((long long)out_words < plan->plan.out_words_needed())
+      return fail(SYNDROME_BUFFER_TOO_SMALL, "output buffer shorter than the planned offsets");
+    if (d_iters && iters_len < (size_t)plan->plan.codewords())
+      return fail(SYNDROME_BUFFER_TOO_SMALL, "iteration buffer shorter than the codeword count");
+    return from_cuda(plan->plan.decode(d_llr, d_hard_packed, d_iters, use_graph != 0,
+                                       static_cast<cudaStream_t>(stream)),
+                     "");
   });
 }
 

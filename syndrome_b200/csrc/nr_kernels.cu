@@ -107,6 +107,30 @@ struct Args {
   int cz[Tab<BG>::E];  // col * z: first shared-memory posterior of the edge's column
 };
 
+// Where a layer reads its edges' cyclic shift and column base from.  The
+// single-shape kernel passes them as kernel parameters (constant bank, indexed by
+// compile-time edge numbers); the mixed-shape kernel stages them per work item in
+// shared memory.
+template <int BG>
+struct ParamEdges {
+  const Args<BG>& a;
+  __device__ __forceinline__ int sh(int e) const { return a.sh[e]; }
+  __device__ __forceinline__ int cz(int e) const { return a.cz[e]; }
+};
+
+struct SmemEdges {
+  const int* __restrict__ s_sh;
+  const int* __restrict__ s_cz;
+  __device__ __forceinline__ int sh(int e) const { return s_sh[e]; }
+  __device__ __forceinline__ int cz(int e) const { return s_cz[e]; }
+};
+
+// Per-launch scalars of a decode.
+struct RunConsts {
+  int z, beta_q, app_clamp, k32;
+  unsigned two;
+};
+
 // Meta bits of a compressed row: argmin [13,18), min1' [18,25), min2' [25,32).
 __device__ __forceinline__ uint32_t pack_meta(int idx, int m1p, int m2p) {
   return ((uint32_t)idx << 13) | ((uint32_t)m1p << 18) | ((uint32_t)m2p << 25);
@@ -132,19 +156,19 @@ __device__ __forceinline__ int top_bit(int x, unsigned two) { return (int)__umul
 // sigma = (-1)^(sign bit of the row's XOR), R_new = sigma * (1 - 2*bit(u_e)) * mag_e,
 // and the sign bits of the new messages are accumulated as acc -= sgn_e * 2^e
 // (acc starting at 2^deg - 1 gives acc = 2 * sum(bit_e * 2^e)).
-template <int BG, bool CLAMP, int L>
-__device__ __forceinline__ void layer(const Args<BG>& a, int z, int16_t* __restrict__ A,
-                                      const int8_t* __restrict__ X, uint32_t* __restrict__ st, int ns,
-                                      int beta_q, int C) {
+template <int BG, bool CLAMP, int L, class EDGES>
+__device__ __forceinline__ void layer(const EDGES ed, const RunConsts rc, int z, int16_t* __restrict__ A,
+                                      const int8_t* __restrict__ X, uint32_t* __restrict__ st, int ns) {
   using T = Tab<BG>;
+  const int beta_q = rc.beta_q, C = rc.app_clamp;
   constexpr int lb = T::loff(L), deg = deg_of<BG>(L), W = word_off<BG>(L);
   constexpr bool two_words = words_of<BG>(L) == 2;
   const uint32_t w_signs = st[W * ns];
   const uint32_t w_meta = two_words ? st[(W + 1) * ns] : w_signs;
   const int idxo = (w_meta >> 13) & 31, m1o = (w_meta >> 18) & 127, m2o = w_meta >> 25;
-  const int Z = a.c.z;
-  const int k32 = a.c.k32;
-  const unsigned two = (unsigned)a.c.two;
+  const int Z = rc.z;
+  const int k32 = rc.k32;
+  const unsigned two = rc.two;
   int vidx[deg], u[deg], ab[deg];
   int m1k = 4095, m2k = 4095;  // (127 << 5) | 31: the message ceiling, no edge
   int sx = 0;
@@ -156,9 +180,9 @@ __device__ __forceinline__ void layer(const Args<BG>& a, int z, int16_t* __restr
       ab[e] = abs(q);
     } else {
       // (z + shift) mod Z as an unsigned min: below Z the second candidate wraps high.
-      const unsigned r = (unsigned)(z + a.sh[lb + e]);
+      const unsigned r = (unsigned)(z + ed.sh(lb + e));
       const unsigned rr = min(r, r - (unsigned)Z);
-      const int vi = (int)rr + a.cz[lb + e];
+      const int vi = (int)rr + ed.cz(lb + e);
       vidx[e] = vi;
       const int app = A[vi];
       const int mag = idxo == e ? m2o : m1o;
@@ -197,8 +221,8 @@ __device__ __forceinline__ void layer(const Args<BG>& a, int z, int16_t* __restr
 }
 
 // Parity of check row (L, z) under the current posteriors: true if odd.
-template <int BG, int L>
-__device__ __forceinline__ bool row_parity(const Args<BG>& a, int z, const int16_t* __restrict__ A,
+template <int BG, int L, class EDGES>
+__device__ __forceinline__ bool row_parity(const EDGES ed, int Z, int z, const int16_t* __restrict__ A,
                                            const int8_t* __restrict__ X, const uint32_t* __restrict__ st,
                                            int ns) {
   using T = Tab<BG>;
@@ -210,14 +234,105 @@ __device__ __forceinline__ bool row_parity(const Args<BG>& a, int z, const int16
     if constexpr (is_ext<BG>(L, e)) {
       const uint32_t w0 = st[W * ns];
       const int r = row_message(w0, two ? st[(W + 1) * ns] : w0, e);
-      par ^= ((int)X[(L - 4) * a.c.z + z] + r) < 0 ? 1u : 0u;
+      par ^= ((int)X[(L - 4) * Z + z] + r) < 0 ? 1u : 0u;
     } else {
-      const unsigned r = (unsigned)(z + a.sh[lb + e]);
-      const int vi = (int)min(r, r - (unsigned)a.c.z) + a.cz[lb + e];
+      const unsigned r = (unsigned)(z + ed.sh(lb + e));
+      const int vi = (int)min(r, r - (unsigned)Z) + ed.cz(lb + e);
       par ^= A[vi] < 0 ? 1u : 0u;
     }
   });
   return par != 0;
+}
+
+// Runs up to `iterations` layered iterations with early stop on the CTA's codeword
+// slots and returns the iterations this thread's slot used.  All threads of the CTA
+// call it (it contains barriers); `active` says whether this thread owns a live
+// check row.  Compressed rows are cleared first (messages start at zero).
+template <int BG, bool CLAMP, class EDGES>
+__device__ __forceinline__ int iterate(const EDGES ed, const RunConsts rc, bool active, bool lane_ok, int slot,
+                                       int z, int16_t* __restrict__ A, const int8_t* __restrict__ X,
+                                       uint32_t* __restrict__ st, int ns, int* s_flag, int iterations) {
+  using T = Tab<BG>;
+  constexpr int NWT = word_off<BG>(T::MB);
+#pragma unroll 1
+  for (int i = 0; i < NWT; ++i) st[i * ns] = 0;
+  int used = 0;
+  for (int it = 0; it < iterations; ++it) {
+    if (!__syncthreads_or(active)) break;
+    if (active) ++used;
+    static_for<0, T::MB>([&](auto li) {
+      constexpr int L = decltype(li)::value;
+      if (active) layer<BG, CLAMP, L>(ed, rc, z, A, X, st, ns);
+      __syncthreads();
+    });
+    if (lane_ok && z == 0) s_flag[slot] = 0;
+    __syncthreads();
+    constexpr int QL = quick_layer<BG>();
+    if (active && row_parity<BG, QL>(ed, rc.z, z, A, X, st, ns)) s_flag[slot] = 1;
+    __syncthreads();
+    if (active && s_flag[slot] == 0) {
+      bool odd = false;
+      static_for<0, T::MB>([&](auto li) {
+        constexpr int L = decltype(li)::value;
+        if constexpr (L != QL) odd |= row_parity<BG, L>(ed, rc.z, z, A, X, st, ns);
+      });
+      if (odd) s_flag[slot] = 1;
+    }
+    __syncthreads();
+    if (active && s_flag[slot] == 0) active = false;
+  }
+  return used;
+}
+
+// Posteriors of the extension columns (channel + the column's one message), written
+// to app_out when given, and their hard decisions left in X for the output pass.
+template <int BG>
+__device__ __forceinline__ void finish_extension(int Z, int z, int8_t* __restrict__ X, const uint32_t* __restrict__ st,
+                                                 int ns, int16_t* app_out_core_end) {
+  using T = Tab<BG>;
+  static_for<4, T::MB>([&](auto li) {
+    constexpr int L = decltype(li)::value;
+    constexpr int W = word_off<BG>(L);
+    constexpr bool two = words_of<BG>(L) == 2;
+    constexpr int e_ext = ext_pos<BG>(L);
+    static_assert(e_ext >= 0, "every layer >= 4 has an extension column");
+    const uint32_t w0 = st[W * ns];
+    const int app = (int)X[(L - 4) * Z + z] + row_message(w0, two ? st[(W + 1) * ns] : w0, e_ext);
+    if (app_out_core_end) app_out_core_end[(L - 4) * Z + z] = (int16_t)app;
+    X[(L - 4) * Z + z] = app < 0 ? 1 : 0;
+  });
+}
+
+// Messages of every edge in the reference's edge_r layout (edge-major, z fastest).
+template <int BG>
+__device__ __forceinline__ void write_messages(int Z, int z, const uint32_t* __restrict__ st, int ns,
+                                               int8_t* __restrict__ R) {
+  using T = Tab<BG>;
+  static_for<0, T::MB>([&](auto li) {
+    constexpr int L = decltype(li)::value;
+    constexpr int W = word_off<BG>(L), lb = T::loff(L);
+    constexpr bool two = words_of<BG>(L) == 2;
+    static_for<0, deg_of<BG>(L)>([&](auto ei) {
+      constexpr int e = decltype(ei)::value;
+      const uint32_t w0 = st[W * ns];
+      R[(long long)(lb + e) * Z + z] = (int8_t)row_message(w0, two ? st[(W + 1) * ns] : w0, e);
+    });
+  });
+}
+
+// Packed hard decisions of one codeword slot (core posteriors' signs, extension
+// hard decisions from finish_extension), LSB-first words, cooperative over the CTA.
+__device__ __forceinline__ void write_packed(const int16_t* __restrict__ As, const int8_t* __restrict__ Hs, int core_n,
+                                             int hard_bits, uint32_t* __restrict__ dst) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int nwords = (hard_bits + 31) >> 5;
+  for (int w = warp; w < nwords; w += nwarps) {
+    const int j = (w << 5) + lane;
+    bool bit = false;
+    if (j < hard_bits) bit = j < core_n ? As[j] < 0 : Hs[j - core_n] != 0;
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+    if (lane == 0) dst[w] = m;
+  }
 }
 
 __host__ __device__ inline int al16(int x) { return (x + 15) & ~15; }
@@ -237,7 +352,6 @@ __host__ __device__ inline int state_bytes(int threads) {
 template <int BG, bool CLAMP>
 __global__ void __launch_bounds__(768, 1) nr_i8_kernel(const __grid_constant__ Args<BG> a) {
   using T = Tab<BG>;
-  constexpr int NWT = word_off<BG>(T::MB);
   extern __shared__ __align__(16) unsigned char smem[];
   const NrCommon& c = a.c;
   const int Z = c.z, N = T::NB * Z;
@@ -253,6 +367,7 @@ __global__ void __launch_bounds__(768, 1) nr_i8_kernel(const __grid_constant__ A
   int16_t* A = reinterpret_cast<int16_t*>(slots + (lane_ok ? slot : 0) * sb);
   int8_t* X = reinterpret_cast<int8_t*>(slots + (lane_ok ? slot : 0) * sb + al16(core_n * 2));
   const int C = c.app_clamp;
+  const RunConsts rc{Z, c.beta_q, c.app_clamp, c.k32, (unsigned)c.two};
   const long long ngroups = (c.batch + c.cpb - 1) / c.cpb;
   const bool vec_ok = (c.llr_stride % 16 == 0) && (c.llr_offset % 16 == 0) &&
                       ((reinterpret_cast<uintptr_t>(c.llr) & 15) == 0);
@@ -298,66 +413,17 @@ __global__ void __launch_bounds__(768, 1) nr_i8_kernel(const __grid_constant__ A
     __syncthreads();
 
     const long long cw = grp * c.cpb + slot;
-    bool active = lane_ok && cw < c.batch;
-#pragma unroll 1
-    for (int i = 0; i < NWT; ++i) st[i * ns] = 0;
-    int used = 0;
-    for (int it = 0; it < c.iterations; ++it) {
-      if (!__syncthreads_or(active)) break;
-      if (active) ++used;
-      static_for<0, T::MB>([&](auto li) {
-        constexpr int L = decltype(li)::value;
-        if (active) layer<BG, CLAMP, L>(a, z, A, X, st, ns, c.beta_q, C);
-        __syncthreads();
-      });
-      if (lane_ok && z == 0) s_flag[slot] = 0;
-      __syncthreads();
-      constexpr int QL = quick_layer<BG>();
-      if (active && row_parity<BG, QL>(a, z, A, X, st, ns)) s_flag[slot] = 1;
-      __syncthreads();
-      if (active && s_flag[slot] == 0) {
-        bool odd = false;
-        static_for<0, T::MB>([&](auto li) {
-          constexpr int L = decltype(li)::value;
-          if constexpr (L != QL) odd |= row_parity<BG, L>(a, z, A, X, st, ns);
-        });
-        if (odd) s_flag[slot] = 1;
-      }
-      __syncthreads();
-      if (active && s_flag[slot] == 0) active = false;
-    }
+    const int used = iterate<BG, CLAMP>(ParamEdges<BG>{a}, rc, lane_ok && cw < c.batch, lane_ok, slot, z, A,
+                                        X, st, ns, s_flag, c.iterations);
 
     // ---- outputs
     __syncthreads();
     if (lane_ok && cw < c.batch) {
       if (z == 0 && c.iters) c.iters[cw] = used;
-      static_for<4, T::MB>([&](auto li) {
-        constexpr int L = decltype(li)::value;
-        constexpr int W = word_off<BG>(L);
-        constexpr bool two = words_of<BG>(L) == 2;
-        constexpr int e_ext = ext_pos<BG>(L);
-        static_assert(e_ext >= 0, "every layer >= 4 has an extension column");
-        const uint32_t w0 = st[W * ns];
-        const int app = (int)X[(L - 4) * Z + z] + row_message(w0, two ? st[(W + 1) * ns] : w0, e_ext);
-        if (c.app_out) c.app_out[cw * c.app_stride + core_n + (L - 4) * Z + z] = (int16_t)app;
-        X[(L - 4) * Z + z] = app < 0 ? 1 : 0;
-      });
-      if (c.edge_r_out) {
-        int8_t* R = c.edge_r_out + cw * c.edge_r_stride;
-        static_for<0, T::MB>([&](auto li) {
-          constexpr int L = decltype(li)::value;
-          constexpr int W = word_off<BG>(L), lb = T::loff(L);
-          constexpr bool two = words_of<BG>(L) == 2;
-          static_for<0, deg_of<BG>(L)>([&](auto ei) {
-            constexpr int e = decltype(ei)::value;
-            const uint32_t w0 = st[W * ns];
-            R[(long long)(lb + e) * Z + z] = (int8_t)row_message(w0, two ? st[(W + 1) * ns] : w0, e);
-          });
-        });
-      }
+      finish_extension<BG>(Z, z, X, st, ns, c.app_out ? c.app_out + cw * c.app_stride + core_n : nullptr);
+      if (c.edge_r_out) write_messages<BG>(Z, z, st, ns, c.edge_r_out + cw * c.edge_r_stride);
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int sl = 0; sl < c.cpb; ++sl) {
       const long long cwo = grp * c.cpb + sl;
       if (cwo >= c.batch) break;
@@ -368,17 +434,7 @@ __global__ void __launch_bounds__(768, 1) nr_i8_kernel(const __grid_constant__ A
       if (c.hard_out)
         for (int j = threadIdx.x; j < N; j += blockDim.x)
           c.hard_out[cwo * c.hard_stride + j] = j < core_n ? (As[j] < 0 ? 1 : 0) : (uint8_t)Hs[j - core_n];
-      if (c.hard_packed) {
-        const int nwords = (c.hard_bits + 31) >> 5;
-        uint32_t* dst = c.hard_packed + cwo * c.hard_words_stride;
-        for (int w = warp; w < nwords; w += nwarps) {
-          const int j = (w << 5) + lane;
-          bool bit = false;
-          if (j < c.hard_bits) bit = j < core_n ? As[j] < 0 : Hs[j - core_n] != 0;
-          const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
-          if (lane == 0) dst[w] = m;
-        }
-      }
+      if (c.hard_packed) write_packed(As, Hs, core_n, c.hard_bits, c.hard_packed + cwo * c.hard_words_stride);
     }
   }
 }
@@ -411,7 +467,124 @@ cudaError_t launch_bg(const NrCommon& c, const int* shifts, bool clamp, int sms,
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------ mixed batches --
+//
+// One persistent launch decodes codewords of any 5G NR base graph and lifting size.
+// The host groups codewords of equal (BG, Z) into work items of up to `count`
+// codewords (the tile size, chosen per shape by the tuner) and orders items by
+// decreasing work.  Each CTA (768 threads, one per SM) takes the next item from a
+// device counter, stages that shape's shifts and column bases in shared memory and
+// runs the same layered iteration as the single-shape kernel.  Codewords carry
+// their own filler count; the posterior clamp is always applied (filler bits are
+// the common case in rate-matched code blocks).
+
+constexpr int kMixStateBytes = 50 * 768 * 4;                     // BG1 compressed rows, 768 threads
+constexpr int kMixTableInts = 320 + 320 + 64;                     // shifts, column bases, slot flags
+constexpr int kMixSmem = 232448 - 1024;                           // 227 KB per CTA less static smem
+constexpr int kMixSlotBytes = kMixSmem - kMixStateBytes - kMixTableInts * 4;
+
+static_assert(word_off<0>(Tab<0>::MB) == 50, "BG1 state words");
+static_assert(word_off<1>(Tab<1>::MB) <= 50, "BG2 state words");
+
+template <int BG>
+__device__ __forceinline__ void mixed_item(const MixArgs& m, const MixItem& it, int* s_sh, int* s_cz, int* s_flag,
+                                           uint32_t* st, unsigned char* slots) {
+  using T = Tab<BG>;
+  const int Z = it.z, N = T::NB * Z, K = T::KB * Z;
+  const int core_n = (T::KB + 4) * Z;
+  const int ns = blockDim.x;
+  const short* sh_src = m.shift_tab + (long long)(BG * kMixLiftSizes + it.zi) * kMixEdges;
+  const int* cz_src = m.colz_tab + (long long)(BG * kMixLiftSizes + it.zi) * kMixEdges;
+  for (int e = threadIdx.x; e < T::E; e += blockDim.x) {
+    s_sh[e] = sh_src[e];
+    s_cz[e] = cz_src[e];
+  }
+  const int sb = slot_bytes<BG>(Z);
+  const int C = m.app_clamp;
+  // channel LLRs of the item's codewords: variables 2Z..N (the punctured 2Z are erasures)
+  for (int sl = 0; sl < it.count; ++sl) {
+    const MixCodeword cw = m.cws[it.first + sl];
+    const int8_t* src = m.llr + cw.llr_off;
+    int16_t* As = reinterpret_cast<int16_t*>(slots + sl * sb);
+    int8_t* Xs = reinterpret_cast<int8_t*>(slots + sl * sb + al16(core_n * 2));
+    const int kp = cw.n_filler > K ? 0 : K - cw.n_filler;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+      int v = j < 2 * Z ? 0 : (int)src[j - 2 * Z];
+      if (j >= kp && j < K && j >= 2 * Z) v = C;
+      if (j < core_n)
+        As[j] = (int16_t)min(max(v, -C), C);
+      else
+        Xs[j - core_n] = (int8_t)v;
+    }
+  }
+  __syncthreads();
+  const int slot = threadIdx.x / Z;
+  const int z = threadIdx.x - slot * Z;
+  const bool lane_ok = slot < it.count;
+  int16_t* A = reinterpret_cast<int16_t*>(slots + (lane_ok ? slot : 0) * sb);
+  int8_t* X = reinterpret_cast<int8_t*>(slots + (lane_ok ? slot : 0) * sb + al16(core_n * 2));
+  const RunConsts rc{Z, m.beta_q, C, m.k32, (unsigned)m.two};
+  const int used = iterate<BG, true>(SmemEdges{s_sh, s_cz}, rc, lane_ok, lane_ok, slot, z, A, X, st, ns, s_flag,
+                                     m.iterations);
+  __syncthreads();
+  if (lane_ok) {
+    if (z == 0 && m.iters) m.iters[m.cws[it.first + slot].index] = used;
+    finish_extension<BG>(Z, z, X, st, ns, nullptr);
+  }
+  __syncthreads();
+  for (int sl = 0; sl < it.count; ++sl) {
+    const MixCodeword cw = m.cws[it.first + sl];
+    write_packed(reinterpret_cast<const int16_t*>(slots + sl * sb),
+                 reinterpret_cast<const int8_t*>(slots + sl * sb + al16(core_n * 2)), core_n, cw.hard_bits,
+                 m.out + cw.out_off);
+  }
+}
+
+__global__ void __launch_bounds__(768, 1) nr_mixed_i8_kernel(const __grid_constant__ MixArgs m) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_item;
+  int* s_sh = reinterpret_cast<int*>(smem);
+  int* s_cz = s_sh + 320;
+  int* s_flag = s_cz + 320;
+  uint32_t* st = reinterpret_cast<uint32_t*>(smem + kMixTableInts * 4) + threadIdx.x;
+  unsigned char* slots = smem + kMixTableInts * 4 + kMixStateBytes;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(m.queue, 1u);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= m.n_items) break;
+    const MixItem it = m.items[item];
+    if (it.bg == 0)
+      mixed_item<0>(m, it, s_sh, s_cz, s_flag, st, slots);
+    else
+      mixed_item<1>(m, it, s_sh, s_cz, s_flag, st, slots);
+  }
+}
+
 }  // namespace nr
+
+int mixed_slot_capacity(int bg, int z) {
+  const int sb = bg == 0 ? nr::slot_bytes<0>(z) : nr::slot_bytes<1>(z);
+  return std::max(1, std::min(std::min(64, 768 / z), nr::kMixSlotBytes / sb));
+}
+
+void mixed_column_bases(int bg, int z, int* colz_out) {
+  const int E = bg == 0 ? nr::Tab<0>::E : nr::Tab<1>::E;
+  for (int e = 0; e < E; ++e) colz_out[e] = (bg == 0 ? nr::Tab<0>::col(e) : nr::Tab<1>::col(e)) * z;
+}
+
+cudaError_t mixed_kernel_prepare() {
+  return cudaFuncSetAttribute(nr::nr_mixed_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, nr::kMixSmem);
+}
+
+cudaError_t mixed_decode_launch(const MixArgs& m, int sms, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(m.queue, 0, sizeof(unsigned), stream);
+  if (e != cudaSuccess) return e;
+  const int ctas = std::max(1, std::min(sms, m.n_items));
+  nr::nr_mixed_i8_kernel<<<ctas, 768, nr::kMixSmem, stream>>>(m);
+  return cudaGetLastError();
+}
 
 bool nr_layout_matches(int bg, const int* cols, int n_edges) {
   if (bg == 0) {

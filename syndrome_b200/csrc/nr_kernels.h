@@ -37,6 +37,53 @@ struct NrCommon {
   int two;
 };
 
+// ---- mixed batches (one persistent launch over any BG / Z mix) ----
+constexpr int kMixLiftSizes = 51;   // lifting sizes of TS 38.212 Table 5.3.2-1 (all <= 384)
+constexpr int kMixEdges = 316;      // table row length (BG1 edge count; BG2 uses the first 197)
+
+struct MixItem {
+  int bg;     // 0 = BG1, 1 = BG2
+  int z;      // lifting size
+  int zi;     // index of z in the lifting-size list
+  int count;  // codewords in this item
+  int first;  // first entry of the item in MixArgs::cws
+};
+
+struct MixCodeword {
+  long long llr_off;  // byte offset of the codeword's N - 2Z int8 LLRs in MixArgs::llr
+  long long out_off;  // word offset of its packed hard decisions in MixArgs::out
+  int n_filler;
+  int hard_bits;
+  int index;          // position of the codeword in the caller's list (iteration output)
+  int pad;
+};
+
+struct MixArgs {
+  const MixItem* items;
+  int n_items;
+  const MixCodeword* cws;
+  const int8_t* llr;
+  uint32_t* out;
+  int32_t* iters;
+  const short* shift_tab;  // [2][kMixLiftSizes][kMixEdges] shifts in layer order
+  const int* colz_tab;     // [2][kMixLiftSizes][kMixEdges] column * z
+  unsigned* queue;         // work counter, zeroed before each launch
+  int beta_q;
+  int app_clamp;
+  int iterations;
+  int k32;
+  int two;
+};
+
+// Codewords one work item of shape (bg, z) can hold in the mixed kernel.
+int mixed_slot_capacity(int bg, int z);
+// Column bases (column * z) of the compiled BG tables in layer order.
+void mixed_column_bases(int bg, int z, int* colz_out);
+// Raises the kernel's dynamic shared-memory limit (once per device, outside capture).
+cudaError_t mixed_kernel_prepare();
+// Zeroes the queue and launches the persistent kernel on `sms` CTAs.
+cudaError_t mixed_decode_launch(const MixArgs& m, int sms, cudaStream_t stream);
+
 // True if the layer-ordered column list equals the compiled BG tables.
 bool nr_layout_matches(int bg, const int* cols, int n_edges);
 // Codewords per CTA used by the kernel for lifting size z.
