@@ -45,7 +45,8 @@ struct BatchRequest {
   long long hard_stride = 0;
   void* edge_r = nullptr;            // [batch][edge_r_stride] final C->V messages, reference layout
   long long edge_r_stride = 0;
-  // Kernel selection: 0 = automatic, 1 = generic layered kernel, 2 = 5G NR kernel.
+  // Kernel selection: 0 = automatic, 1 = generic layered kernel, 2 = 5G NR kernel,
+  // 3 = paired 5G NR kernel (two codewords per 32-bit word).
   int kernel = 0;
   // Scratch for C->V messages when edge_r is null.
   void* workspace = nullptr;

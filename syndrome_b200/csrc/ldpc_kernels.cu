@@ -508,7 +508,7 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
     return bad("hard_bits / hard_words_stride out of range");
   if (req.app_clamp < 0 && p == Precision::kInt8) return bad("app_clamp must be non-negative");
   const bool nr_ok = p == Precision::kInt8 && nr_bg_ >= 0 && !req.llr_i16 && req.app_clamp >= 255;
-  if (req.kernel == 2 && !nr_ok) return bad("the 5G NR kernel does not apply to this request");
+  if ((req.kernel == 2 || req.kernel == 3) && !nr_ok) return bad("the 5G NR kernel does not apply to this request");
   if (nr_ok && req.kernel != 1) {
     NrCommon c{};
     c.z = g_.z;
@@ -533,6 +533,9 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
     c.edge_r_stride = req.edge_r_stride;
     c.hard_out = req.hard;
     c.hard_stride = req.hard_stride;
+    const bool pair_ok = nr_pair_applies(c);
+    if (req.kernel == 3 && !pair_ok) return bad("the paired 5G NR kernel needs app_clamp >= 3938 (7874 with filler)");
+    if (pair_ok && req.kernel != 2) return nr_pair_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream);
     return nr_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream);
   }
   const Geometry geo = geometry(p, req.batch);

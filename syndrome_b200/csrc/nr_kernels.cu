@@ -33,33 +33,12 @@
 #include <string>
 #include <type_traits>
 
+#include "nr_graph.cuh"
 #include "nr_kernels.h"
-#include "nr_layered_tables.h"
 
 namespace syn {
 namespace nr {
 
-template <int BG>
-struct Tab;
-
-template <>
-struct Tab<0> {
-  static constexpr int MB = 46, NB = 68, KB = 22, E = 316;
-  __host__ __device__ static constexpr int loff(int i) { return syn_bg1_loff(i); }
-  __host__ __device__ static constexpr int col(int e) { return syn_bg1_lcol(e); }
-};
-
-template <>
-struct Tab<1> {
-  static constexpr int MB = 42, NB = 52, KB = 10, E = 197;
-  __host__ __device__ static constexpr int loff(int i) { return syn_bg2_loff(i); }
-  __host__ __device__ static constexpr int col(int e) { return syn_bg2_lcol(e); }
-};
-
-template <int BG>
-__host__ __device__ constexpr int deg_of(int l) {
-  return Tab<BG>::loff(l + 1) - Tab<BG>::loff(l);
-}
 // Compressed state words of a layer: one when signs (deg bits) fit below bit 13.
 template <int BG>
 __host__ __device__ constexpr int words_of(int l) {
@@ -70,34 +49,6 @@ __host__ __device__ constexpr int word_off(int l) {
   int w = 0;
   for (int i = 0; i < l; ++i) w += words_of<BG>(i);
   return w;
-}
-template <int BG>
-__host__ __device__ constexpr bool is_ext(int l, int e) {
-  return l >= 4 && Tab<BG>::col(Tab<BG>::loff(l) + e) == Tab<BG>::KB + l;
-}
-
-template <int BG>
-__host__ __device__ constexpr int ext_pos(int l) {
-  for (int e = 0; e < deg_of<BG>(l); ++e)
-    if (is_ext<BG>(l, e)) return e;
-  return -1;
-}
-
-// Layer with the fewest edges: checked first after every iteration.
-template <int BG>
-__host__ __device__ constexpr int quick_layer() {
-  int best = 0;
-  for (int l = 1; l < Tab<BG>::MB; ++l)
-    if (deg_of<BG>(l) < deg_of<BG>(best)) best = l;
-  return best;
-}
-
-template <int I, int N, class F>
-__device__ __forceinline__ void static_for(F&& f) {
-  if constexpr (I < N) {
-    f(std::integral_constant<int, I>{});
-    static_for<I + 1, N>(f);
-  }
 }
 
 template <int BG>

@@ -91,4 +91,10 @@ int nr_cpb(int bg, int z);
 // shifts: per edge in layer order, already reduced mod z.
 cudaError_t nr_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream);
 
+// Paired kernel (nr_pair_kernels.cu, two codewords per 32-bit word): applies when
+// app_clamp >= 3938 (>= 7874 with filler bits), where no posterior of a non-filler
+// variable can reach the clamp.  c.cpb is chosen by the launcher.
+bool nr_pair_applies(const NrCommon& c);
+cudaError_t nr_pair_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream);
+
 }  // namespace syn

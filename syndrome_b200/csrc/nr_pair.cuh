@@ -1,0 +1,279 @@
+// Two-codeword (paired) int8 layered offset min-sum row update for the 5G NR base
+// graphs, shared by the sm_100a kernel (nr_pair_kernels.cu) and the host
+// emulation the tests run against the oracle.
+//
+// Arithmetic of syndrome src/qc_ldpc.rs:1530-1758 (int8 messages, int16
+// posterior, Q clamped to +-127, R = sign-excluded product * max(min_excl - beta_q, 0),
+// posterior += R_new - R_old), computed for two codewords at once: every 32-bit
+// word holds codeword A in its low 16-bit lane and codeword B in its high lane.
+//
+// Lane encodings (per 16-bit lane, all values non-negative so that one 32-bit add
+// or subtract never carries across lanes, and unsigned 16x2 min/max order them):
+//   posterior / Q      PB + v with PB = 0x4000 (|v| <= 3938 + 127, or the filler
+//                      proxy below); bit 14 of the lane is 1 iff v >= 0
+//   message table out  127 + R (R in [-127, 127]), zero-extended
+//   min-sum key        |Q| * 128 + tag(edge)
+//
+// Per check row the compressed C->V state is one meta word, bytes
+// [min1'A, min2'A, min1'B, min2'B] (offset magnitudes), and ceil(deg / 8) code
+// words with two bits per lane and edge: bit 0 = "this edge takes min2'" (the
+// argmin), bit 1 = "R >= 0".  For edge j of a code word (j < 8) lane A's code sits
+// at bit s_j = 2 * (j & 3) + 16 * (j >> 2) and lane B's at s_j + 8, so that
+// ((code >> s_j) & 0x0303) | 0xC480 is a byte-permute selector that picks both
+// lanes' messages out of the row's 8-byte table
+//   [127 - m1'A, 127 - m2'A, 127 + m1'A, 127 + m2'A, same for B]
+// (nibbles 1 and 3 replicate the sign of table bytes 0 and 4, which are < 128,
+// giving zero high bytes).  The reference's messages are exactly this function of
+// the row state: every edge gets min1' except the argmin, which gets min2', and
+// ties give min2' = min1' (qc_ldpc.rs:1700-1718).
+//
+// Filler proxy: a filler variable starts at app_clamp C and, while C >= 7874, its
+// Q is always clamped to +127 and its posterior only ever meets the upper clamp;
+// the posterior equals C - d with d the same non-negative deficit that CAPV - d
+// follows under min(., CAPV).  The kernel stores min(posterior, CAPV) (exact for
+// every non-filler variable, which never exceeds 3938) and adds C - CAPV back to
+// filler posteriors on output.
+#pragma once
+
+#include <cstdint>
+
+#include "nr_graph.cuh"
+
+namespace syn {
+namespace nrp {
+
+using nr::deg_of;
+using nr::ext_pos;
+using nr::is_ext;
+using nr::quick_layer;
+using nr::static_for;
+using nr::Tab;
+
+constexpr uint32_t kPB = 0x4000u;            // lane bias
+constexpr uint32_t kPB2 = 0x40004000u;
+constexpr int kCapV = 8192;                  // filler proxy ceiling (>= 7874)
+constexpr uint32_t kCap2 = (kPB + kCapV) * 0x10001u;
+constexpr int kMinFillerClamp = 7874;        // 30 * 254 + 2 * 127: deficit bound plus Q clamp
+constexpr int kMaxReach = 3938;              // 128 + 30 * 127: largest reachable |posterior|
+
+// ------------------------------------------------------------------ SWAR ops --
+
+__host__ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t s) {
+#ifdef __CUDA_ARCH__
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(s));
+  return d;
+#else
+  const uint64_t src = (uint64_t)a | ((uint64_t)b << 32);
+  uint32_t d = 0;
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t n = (s >> (4 * i)) & 15u;
+    uint32_t byte = (uint32_t)(src >> (8 * (n & 7))) & 0xFFu;
+    if (n & 8) byte = (byte & 0x80u) ? 0xFFu : 0u;
+    d |= byte << (8 * i);
+  }
+  return d;
+#endif
+}
+
+__host__ __device__ __forceinline__ uint32_t vmaxu2(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  uint32_t d;
+  asm("max.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+#else
+  const uint32_t lo = (a & 0xFFFFu) > (b & 0xFFFFu) ? (a & 0xFFFFu) : (b & 0xFFFFu);
+  const uint32_t hi = (a >> 16) > (b >> 16) ? (a >> 16) : (b >> 16);
+  return lo | (hi << 16);
+#endif
+}
+
+__host__ __device__ __forceinline__ uint32_t vminu2(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  uint32_t d;
+  asm("min.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+#else
+  const uint32_t lo = (a & 0xFFFFu) < (b & 0xFFFFu) ? (a & 0xFFFFu) : (b & 0xFFFFu);
+  const uint32_t hi = (a >> 16) < (b >> 16) ? (a >> 16) : (b >> 16);
+  return lo | (hi << 16);
+#endif
+}
+
+// x << n with n >= 32 (including "negative" n wrapped to large unsigned) giving 0.
+__host__ __device__ __forceinline__ uint32_t shl_sat(uint32_t x, uint32_t n) {
+#ifdef __CUDA_ARCH__
+  uint32_t d;
+  asm("shl.b32 %0, %1, %2;" : "=r"(d) : "r"(x), "r"(n));
+  return d;
+#else
+  return n >= 32 ? 0u : x << n;
+#endif
+}
+
+// ------------------------------------------------------------ row geometry --
+
+__host__ __device__ constexpr int ncw(int deg) { return (deg + 7) / 8; }
+
+// Bit offset of edge e's lane-A code inside its code word.
+__host__ __device__ constexpr int code_shift(int e) { return 2 * ((e & 7) & 3) + 16 * ((e & 7) >> 2); }
+// Min-sum key tag of edge e: code word index * 32 + code_shift.
+__host__ __device__ constexpr int key_tag(int e) { return 32 * (e >> 3) + code_shift(e); }
+
+// First state word (the meta word) of layer l; code words follow it.
+template <int BG>
+__host__ __device__ constexpr int state_off(int l) {
+  int w = 0;
+  for (int i = 0; i < l; ++i) w += 1 + ncw(deg_of<BG>(i));
+  return w;
+}
+template <int BG>
+__host__ __device__ constexpr int state_words() {
+  return state_off<BG>(Tab<BG>::MB);
+}
+// Extension-column channel registers: two layers (4 bytes: A, B, A, B) per word.
+template <int BG>
+__host__ __device__ constexpr int ext_regs() {
+  return (Tab<BG>::MB - 4 + 1) / 2;
+}
+
+// Byte-permute selector of edge e from its code word.
+__host__ __device__ __forceinline__ uint32_t code_sel(uint32_t code_word, int shift) {
+  return ((code_word >> shift) & 0x0303u) | 0xC480u;
+}
+// Message table of a meta word: lanes 127 + R after prmt(lo, hi, selector).
+__host__ __device__ __forceinline__ uint32_t table_lo(uint32_t meta) { return (meta & 0xFFFFu) * 0xFFFFu + 0x7F7F7F7Fu; }
+__host__ __device__ __forceinline__ uint32_t table_hi(uint32_t meta) { return (meta >> 16) * 0xFFFFu + 0x7F7F7F7Fu; }
+
+// Biased channel value lanes (PB + x) of extension layer index xi (= layer - 4).
+__host__ __device__ __forceinline__ uint32_t ext_lanes(uint32_t xreg, int xi) {
+  return prmt(xreg, 0u, (xi & 1) ? 0x4342u : 0x4140u) + 0x3F803F80u;
+}
+
+// ------------------------------------------------------------- row update ---
+//
+// Ctx provides, for one (codeword pair, lifting index z):
+//   template <int GE> int vb() const     byte offset in the pair's posterior array
+//                                        of edge GE's variable (column, (z + shift) mod Z)
+//   uint32_t ld_ap(int) / void st_ap(int, uint32_t)
+//   uint32_t ld_st(int w) / void st_st(int w, uint32_t)   state word w of this row group
+//   uint32_t xr(int i) const             extension channel register i
+
+template <int BG, int L, bool FILL, class C>
+__host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
+  constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L), NC = ncw(deg), W = state_off<BG>(L);
+  constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
+  const uint32_t meta = c.ld_st(W);
+  uint32_t code[NC];
+  static_for<0, NC>([&](auto ki) {
+    constexpr int k = decltype(ki)::value;
+    code[k] = c.ld_st(W + 1 + k);
+  });
+  const uint32_t tlo = table_lo(meta), thi = table_hi(meta);
+  uint32_t qu[deg];
+  int vb[deg];
+  uint32_t m1k = 0x7FFF7FFFu, m2k = 0x7FFF7FFFu, sx = 0u;
+  static_for<0, deg>([&](auto ei) {
+    constexpr int e = decltype(ei)::value;
+    if constexpr (e == ep) {
+      qu[e] = ext_lanes(c.xr((L - 4) >> 1), L - 4);  // Q of the extension edge is its channel value
+      vb[e] = 0;
+    } else {
+      vb[e] = c.template vb<lb + e>();
+      const uint32_t a = c.ld_ap(vb[e]);
+      qu[e] = a - prmt(tlo, thi, code_sel(code[e >> 3], code_shift(e))) + 0x007F007Fu;  // PB + app - R_old
+    }
+    // PB + min(|Q|, 127), then key = |Q| * 128 + tag (the 128 * PB terms cancel mod 2^32)
+    const uint32_t aq = vminu2(vmaxu2(qu[e], 0x80008000u - qu[e]), 0x407F407Fu);
+    const uint32_t key = aq * 128u + ((uint32_t)key_tag(e) * 0x10001u - 0x00200000u);
+    m2k = vminu2(m2k, vmaxu2(m1k, key));
+    m1k = vminu2(m1k, key);
+    sx ^= qu[e];
+  });
+  // Row results: offset magnitudes, new meta word and message table.
+  const uint32_t m1 = (m1k >> 7) & 0x007F007Fu, m2 = (m2k >> 7) & 0x007F007Fu;
+  const uint32_t m1p = vmaxu2(m1, bq2) - bq2, m2p = vmaxu2(m2, bq2) - bq2;
+  const uint32_t nmeta = m2p * 256u + m1p;
+  const uint32_t nlo = table_lo(nmeta), nhi = table_hi(nmeta);
+  // Code words: Q >= 0 bits (bit 6 of bytes 1 and 3 of Q) moved to each edge's sign
+  // slot, two edges per byte-permute ...
+  uint32_t nc[NC];
+  static_for<0, NC>([&](auto ki) {
+    constexpr int k = decltype(ki)::value;
+    nc[k] = 0u;
+    static_for<0, 4>([&](auto ji) {
+      constexpr int j = decltype(ji)::value;
+      constexpr int e0 = 8 * k + j, e1 = 8 * k + j + 4;
+      if constexpr (e0 < deg) {
+        uint32_t hi = 0u;
+        if constexpr (e1 < deg) hi = qu[e1];
+        const uint32_t t = prmt(qu[e0], hi, 0x7531u) & 0x40404040u;
+        if constexpr (j == 3)
+          nc[k] += t << 1;
+        else
+          nc[k] += t >> (5 - 2 * j);
+      }
+    });
+  });
+  // ... turned into R's sign (Q >= 0 xor an odd count of negative Q in the row) ...
+  const uint32_t sp = prmt(sx, 0u, 0x4431u);
+  const uint32_t sn = ((sp >> 6) & 0x0101u) ^ ((deg & 1) ? 0x0101u : 0u);
+  const uint32_t smask = sn * 0x00AA00AAu;
+  // ... plus the argmin flag from the winning key's tag.
+  const uint32_t tA = m1k & 127u, tB = (m1k >> 16) & 127u;
+  static_for<0, NC>([&](auto ki) {
+    constexpr int k = decltype(ki)::value;
+    nc[k] = (nc[k] ^ smask) | shl_sat(1u, tA - 32u * k) | shl_sat(256u, tB - 32u * k);
+  });
+  // Posterior update: app = Q + R_new.
+  static_for<0, deg>([&](auto ei) {
+    constexpr int e = decltype(ei)::value;
+    if constexpr (e != ep) {
+      uint32_t v = qu[e] + prmt(nlo, nhi, code_sel(nc[e >> 3], code_shift(e))) - 0x007F007Fu;
+      if constexpr (FILL) v = vminu2(v, kCap2);
+      c.st_ap(vb[e], v);
+    }
+  });
+  c.st_st(W, nmeta);
+  static_for<0, NC>([&](auto ki) {
+    constexpr int k = decltype(ki)::value;
+    c.st_st(W + 1 + k, nc[k]);
+  });
+}
+
+// Message lanes (127 + R) of edge e of layer L from the stored state.
+template <int BG, int L, int E, class C>
+__host__ __device__ __forceinline__ uint32_t pair_message(const C& c) {
+  constexpr int W = state_off<BG>(L);
+  const uint32_t meta = c.ld_st(W);
+  return prmt(table_lo(meta), table_hi(meta), code_sel(c.ld_st(W + 1 + (E >> 3)), code_shift(E)));
+}
+
+// Posterior lanes (PB + app) of the extension column of layer L >= 4.
+template <int BG, int L, class C>
+__host__ __device__ __forceinline__ uint32_t pair_ext_app(const C& c) {
+  constexpr int ep = ext_pos<BG>(L);
+  return ext_lanes(c.xr((L - 4) >> 1), L - 4) + pair_message<BG, L, ep>(c) - 0x007F007Fu;
+}
+
+// Parity of check row (L, z) under the current posteriors: bit 0 = lane A has an
+// odd number of negative posteriors, bit 1 = lane B.
+template <int BG, int L, class C>
+__host__ __device__ __forceinline__ uint32_t pair_parity(const C& c) {
+  constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L);
+  constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
+  uint32_t x = 0u;
+  static_for<0, deg>([&](auto ei) {
+    constexpr int e = decltype(ei)::value;
+    if constexpr (e == ep) {
+      x ^= pair_ext_app<BG, L>(c);
+    } else {
+      x ^= c.ld_ap(c.template vb<lb + e>());
+    }
+  });
+  const uint32_t nn = ((x >> 14) & 1u) | ((x >> 29) & 2u);
+  return nn ^ ((deg & 1) ? 3u : 0u);
+}
+
+}  // namespace nrp
+}  // namespace syn

@@ -1,0 +1,292 @@
+// Paired int8 LOMS decode for the 5G NR base graphs on sm_100a: two codewords per
+// 32-bit word (nr_pair.cuh), one thread per (codeword pair, lifting index z).
+//
+// Per CTA, for each of its codeword pairs, shared memory holds
+//   * the packed posteriors of the KB + 4 core columns (4 bytes per variable pair),
+//   * the compressed check-row state of every row (meta + code words, word-major
+//     per thread so that a warp's accesses are conflict-free),
+//   * a byte per extension variable for the hard decisions written on output;
+// the int8 channel values of the degree-1 extension columns stay in registers of
+// the thread that owns their row (a layer's extension column is only touched by
+// that layer, and the row of (layer, z) is the one at variable z).
+//
+// The graph is unrolled at compile time; the per-Z cyclic shifts are kernel
+// parameters (constant bank).  With ZT = 384 the column bases are immediates.
+// Each lane stops on its own zero syndrome: its outputs are written after the
+// iteration that finished it while the other lane of the pair keeps decoding.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "nr_kernels.h"
+#include "nr_pair.cuh"
+
+namespace syn {
+namespace nrp {
+
+constexpr int kPairThreads = 384;
+
+template <int BG>
+struct PairArgs {
+  NrCommon c;               // c.cpb = codeword pairs per CTA
+  int sh4[Tab<BG>::E];      // 4 * shift of each edge (reduced mod z)
+  int cz4[Tab<BG>::E];      // 4 * col * z
+};
+
+template <int BG, int ZT>
+struct DevCtx {
+  static constexpr int NX = ext_regs<BG>();
+  unsigned char* ap;
+  uint32_t* st;
+  int ns;
+  int z4;
+  int Z4;
+  const PairArgs<BG>* a;
+  uint32_t x[NX];
+
+  template <int GE>
+  __device__ __forceinline__ int vb() const {
+    // (z + shift) mod Z in bytes, as an unsigned min: below Z the second candidate wraps high.
+    const unsigned r = (unsigned)(z4 + a->sh4[GE]);
+    const unsigned rr = min(r, r - (unsigned)(ZT > 0 ? ZT * 4 : Z4));
+    if constexpr (ZT > 0)
+      return (int)rr + Tab<BG>::col(GE) * ZT * 4;
+    else
+      return (int)rr + a->cz4[GE];
+  }
+  __device__ __forceinline__ uint32_t ld_ap(int b) const { return *reinterpret_cast<const uint32_t*>(ap + b); }
+  __device__ __forceinline__ void st_ap(int b, uint32_t v) { *reinterpret_cast<uint32_t*>(ap + b) = v; }
+  __device__ __forceinline__ uint32_t ld_st(int w) const { return st[w * ns]; }
+  __device__ __forceinline__ void st_st(int w, uint32_t v) { st[w * ns] = v; }
+  __device__ __forceinline__ uint32_t xr(int i) const { return x[i]; }
+};
+
+__host__ __device__ inline int al16(int x) { return (x + 15) & ~15; }
+
+template <int BG>
+__host__ __device__ inline int pair_smem_bytes(int pairs, int z, int threads) {
+  using T = Tab<BG>;
+  return al16(8 * pairs) + pairs * (T::KB + 4) * z * 4 + state_words<BG>() * threads * 4 +
+         al16(pairs * (T::MB - 4) * z);
+}
+
+__device__ __forceinline__ int lane_of(uint32_t w, int lane) { return (int)((w >> (16 * lane)) & 0xFFFFu) - (int)kPB; }
+
+template <int BG, int ZT, bool FILL>
+__global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_constant__ PairArgs<BG> a) {
+  using T = Tab<BG>;
+  constexpr int NW = state_words<BG>(), CORE = T::KB + 4, NEXT = T::MB - 4;
+  constexpr int QL = quick_layer<BG>();
+  extern __shared__ __align__(16) unsigned char smem[];
+  const NrCommon& c = a.c;
+  const int Z = ZT > 0 ? ZT : c.z;
+  const int P = c.cpb;
+  const int ns = blockDim.x;
+  int* s_fail = reinterpret_cast<int*>(smem);
+  int* s_done = s_fail + P;
+  unsigned char* ap_base = smem + al16(8 * P);
+  const int ap_pair = CORE * Z * 4;
+  uint32_t* st_base = reinterpret_cast<uint32_t*>(ap_base + P * ap_pair);
+  uint8_t* eh_base = reinterpret_cast<uint8_t*>(st_base + NW * ns);
+  const int tid = threadIdx.x;
+  const int p = tid / Z, z = tid - p * Z;
+  const bool lane_ok = p < P;
+  const int pq = lane_ok ? p : 0;
+  DevCtx<BG, ZT> cx;
+  cx.ap = ap_base + pq * ap_pair;
+  cx.st = st_base + tid;
+  cx.ns = ns;
+  cx.z4 = z * 4;
+  cx.Z4 = Z * 4;
+  cx.a = &a;
+  uint8_t* eh = eh_base + pq * NEXT * Z;
+  const uint32_t bq2 = (uint32_t)c.beta_q * 0x10001u;
+  const int core_n = CORE * Z, K = T::KB * Z;
+  const long long npairs = (c.batch + 1) / 2;
+  const long long ngroups = (npairs + P - 1) / P;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = ns >> 5;
+
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const long long g = grp * P + p;
+    const bool va = lane_ok && 2 * g < c.batch, vbv = lane_ok && 2 * g + 1 < c.batch;
+    __syncthreads();
+    // ---- load: this thread's variables (col, z) of both codewords
+    if (lane_ok) {
+      const int8_t* sa = va ? c.llr + 2 * g * c.llr_stride - c.llr_offset : nullptr;
+      const int8_t* sb = vbv ? c.llr + (2 * g + 1) * c.llr_stride - c.llr_offset : nullptr;
+      auto fetch = [&](const int8_t* s, int j) -> int { return (s && j >= c.llr_offset) ? (int)s[j] : 0; };
+      uint32_t* apw = reinterpret_cast<uint32_t*>(cx.ap);
+      for (int col = 0; col < CORE; ++col) {
+        const int j = col * Z + z;
+        uint32_t l0 = kPB + (uint32_t)fetch(sa, j), l1 = kPB + (uint32_t)fetch(sb, j);
+        if (c.prologue) {
+          if (j < 2 * Z) {
+            l0 = l1 = kPB;
+          } else if (FILL && j >= c.k_prime && j < K) {
+            l0 = l1 = kPB + kCapV;
+          }
+        }
+        apw[j] = (l0 & 0xFFFFu) | (l1 << 16);
+      }
+      static_for<0, DevCtx<BG, ZT>::NX>([&](auto ri) {
+        constexpr int r = decltype(ri)::value;
+        uint32_t w = 0u;
+        static_for<0, 2>([&](auto hi) {
+          constexpr int h = decltype(hi)::value;
+          constexpr int xi = 2 * r + h;
+          if constexpr (xi < NEXT) {
+            const int j = (CORE + xi) * Z + z;
+            const uint32_t b0 = (uint32_t)(fetch(sa, j) + 128) & 0xFFu, b1 = (uint32_t)(fetch(sb, j) + 128) & 0xFFu;
+            w |= (b0 | (b1 << 8)) << (16 * h);
+          }
+        });
+        cx.x[r] = w;
+      });
+#pragma unroll 1
+      for (int w = 0; w < NW; ++w) st_base[w * ns + tid] = 0u;
+    }
+    __syncthreads();
+
+    // ---- layered iterations with per-lane early stop.  A lane's results are written
+    // at the top of the loop after the iteration that finished it (zero syndrome or
+    // the iteration limit); the other lane of its pair keeps decoding.
+    uint32_t act = (va ? 1u : 0u) | (vbv ? 2u : 0u);
+    uint32_t done = c.iterations <= 0 ? act : 0u;
+    int it = 0;
+    for (;;) {
+#pragma unroll 1
+      for (int X = 0; X < 2; ++X) {
+        const bool mine = ((done >> X) & 1u) != 0u;
+        if (!__syncthreads_or(mine)) continue;
+        if (lane_ok && z == 0) s_done[p] = mine ? 1 : 0;
+        if (mine) {
+          const long long cw = 2 * g + X;
+          if (z == 0 && c.iters) c.iters[cw] = it;
+          static_for<4, T::MB>([&](auto li) {
+            constexpr int L = decltype(li)::value;
+            const int v = lane_of(pair_ext_app<BG, L>(cx), X);
+            const int j = (T::KB + L) * Z + z;
+            eh[(L - 4) * Z + z] = v < 0 ? 1 : 0;
+            if (c.app_out) c.app_out[cw * c.app_stride + j] = (int16_t)v;
+            if (c.hard_out) c.hard_out[cw * c.hard_stride + j] = v < 0 ? 1 : 0;
+          });
+          if (c.edge_r_out) {
+            int8_t* er = c.edge_r_out + cw * c.edge_r_stride;
+            static_for<0, T::MB>([&](auto li) {
+              constexpr int L = decltype(li)::value;
+              static_for<0, deg_of<BG>(L)>([&](auto ei) {
+                constexpr int e = decltype(ei)::value;
+                const uint32_t m = pair_message<BG, L, e>(cx);
+                er[(long long)(T::loff(L) + e) * Z + z] = (int8_t)((int)((m >> (16 * X)) & 0xFFu) - 127);
+              });
+            });
+          }
+        }
+        __syncthreads();
+        for (int q = 0; q < P; ++q) {
+          if (!s_done[q]) continue;
+          const long long cwo = 2 * (grp * P + q) + X;
+          const uint32_t* apq = reinterpret_cast<const uint32_t*>(ap_base + q * ap_pair);
+          const uint8_t* ehq = eh_base + q * NEXT * Z;
+          if (c.app_out || c.hard_out) {
+            for (int j = tid; j < core_n; j += ns) {
+              int v = lane_of(apq[j], X);
+              if (FILL && j >= c.k_prime && j < K) v += c.app_clamp - kCapV;
+              if (c.app_out) c.app_out[cwo * c.app_stride + j] = (int16_t)v;
+              if (c.hard_out) c.hard_out[cwo * c.hard_stride + j] = v < 0 ? 1 : 0;
+            }
+          }
+          if (c.hard_packed) {
+            uint32_t* dst = c.hard_packed + cwo * c.hard_words_stride;
+            const int nwords = (c.hard_bits + 31) >> 5;
+            for (int w = warp; w < nwords; w += nwarps) {
+              const int j = (w << 5) + lane;
+              bool bit = false;
+              if (j < c.hard_bits) bit = j < core_n ? lane_of(apq[j], X) < 0 : ehq[j - core_n] != 0;
+              const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+              if (lane == 0) dst[w] = m;
+            }
+          }
+        }
+        __syncthreads();
+      }
+      act &= ~done;
+      if (!__syncthreads_or(act != 0u)) break;
+      ++it;
+      static_for<0, T::MB>([&](auto li) {
+        constexpr int L = decltype(li)::value;
+        if (lane_ok) pair_row<BG, L, FILL>(cx, bq2);
+        __syncthreads();
+      });
+      // syndrome: the smallest layer first, the others only for lanes that pass it
+      if (lane_ok && z == 0) s_fail[p] = 0;
+      __syncthreads();
+      if (act) {
+        const uint32_t odd = pair_parity<BG, QL>(cx) & act;
+        if (odd) atomicOr(&s_fail[p], (int)odd);
+      }
+      __syncthreads();
+      const uint32_t pass = act & ~(uint32_t)(lane_ok ? s_fail[p] : 0);
+      if (pass) {
+        uint32_t odd = 0u;
+        static_for<0, T::MB>([&](auto li) {
+          constexpr int L = decltype(li)::value;
+          if constexpr (L != QL) odd |= pair_parity<BG, L>(cx);
+        });
+        odd &= pass;
+        if (odd) atomicOr(&s_fail[p], (int)odd);
+      }
+      __syncthreads();
+      done = it >= c.iterations ? act : act & ~(uint32_t)(lane_ok ? s_fail[p] : 0);
+    }
+  }
+}
+
+template <int BG, int ZT, bool FILL>
+cudaError_t launch(const NrCommon& c0, const int* shifts, int sms, cudaStream_t stream) {
+  using T = Tab<BG>;
+  PairArgs<BG> a;
+  a.c = c0;
+  for (int e = 0; e < T::E; ++e) {
+    a.sh4[e] = shifts[e] * 4;
+    a.cz4[e] = T::col(e) * c0.z * 4;
+  }
+  const long long npairs = (c0.batch + 1) / 2;
+  a.c.cpb = (int)std::max<long long>(1, std::min<long long>(kPairThreads / c0.z, npairs));
+  const int threads = ((a.c.cpb * c0.z + 31) / 32) * 32;
+  const int smem = pair_smem_bytes<BG>(a.c.cpb, c0.z, threads);
+  auto fn = nr_pair_kernel<BG, ZT, FILL>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+  if (e != cudaSuccess) return e;
+  const long long groups = (npairs + a.c.cpb - 1) / a.c.cpb;
+  const long long ctas = std::min<long long>(groups, (long long)std::max(per_sm, 1) * sms);
+  if (ctas <= 0) return cudaSuccess;
+  fn<<<(unsigned)ctas, threads, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+template <int BG>
+cudaError_t launch_bg(const NrCommon& c, const int* shifts, bool fill, int sms, cudaStream_t stream) {
+  if (c.z == 384)
+    return fill ? launch<BG, 384, true>(c, shifts, sms, stream) : launch<BG, 384, false>(c, shifts, sms, stream);
+  return fill ? launch<BG, 0, true>(c, shifts, sms, stream) : launch<BG, 0, false>(c, shifts, sms, stream);
+}
+
+}  // namespace nrp
+
+bool nr_pair_applies(const NrCommon& c) {
+  const bool fill = c.prologue && c.k_prime < c.k;
+  return c.app_clamp >= (fill ? nrp::kMinFillerClamp : nrp::kMaxReach) && c.z >= 1 && c.z <= 384;
+}
+
+cudaError_t nr_pair_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream) {
+  const bool fill = c.prologue && c.k_prime < c.k;
+  if (bg == 0) return nrp::launch_bg<0>(c, shifts, fill, sms, stream);
+  return nrp::launch_bg<1>(c, shifts, fill, sms, stream);
+}
+
+}  // namespace syn

@@ -49,7 +49,7 @@ def gpu_i8(dec, llr_i8, iters, quant, kernel="auto", **kw):
     return r
 
 
-KERNELS = ["generic", "nr"]
+KERNELS = ["generic", "nr", "pair"]
 
 
 def assert_i8_equal(label, ref, r):
@@ -103,7 +103,11 @@ def test_int8_nr_punctured_filler_and_clamps(kernel):
         code = O.Code.nr(bg, z)
         dec = S.QcLdpcDecoder.with_lifting_size(bg, z, 0.5)
         info_len = code.k - n_filler
-        for clamp in (32767, 1000, 255):
+        if kernel == "pair":  # the paired kernel needs app_clamp >= 3938 (7874 with filler bits)
+            clamps = (32767, 7874 if n_filler else 3938)
+        else:
+            clamps = (32767, 1000, 255)
+        for clamp in clamps:
             rows, refs = [], []
             for i in range(3):
                 info = np.concatenate([O.random_bits(50 + i, info_len), np.zeros(n_filler, np.uint8)])
@@ -126,6 +130,42 @@ def test_int8_nr_kernel_rejects_what_it_cannot_serve():
     w = S.wifi_ldpc_decoder(27, 1, 2, 0.5).set_kernel("nr")
     with pytest.raises(S.FecError):
         w.decode_batch_i8(torch.zeros((1, w.variable_node_count()), dtype=torch.int8, device="cuda"), 5)
+
+
+def test_int8_pair_kernel_rejects_small_clamps():
+    dec = S.QcLdpcDecoder.with_lifting_size(0, 32, 0.5).set_kernel("pair")
+    n = dec.variable_node_count()
+    t = torch.zeros((3, n), dtype=torch.int8, device="cuda")
+    with pytest.raises(S.FecError) as e:
+        dec.decode_batch_i8(t, 5, quant=S.QuantParams().with_app_clamp(3937))
+    assert e.value.status == _lib.INVALID_PARAM
+    with pytest.raises(S.FecError) as e:
+        dec.decode_batch_i8(t[:, 64:], 5, llr_offset=64, nr_prologue=True, n_filler=40,
+                            quant=S.QuantParams().with_app_clamp(7873))
+    assert e.value.status == _lib.INVALID_PARAM
+    dec.decode_batch_i8(t, 5, quant=S.QuantParams().with_app_clamp(3938))
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("count", [1, 2, 5, 16])
+def test_int8_pair_kernel_lanes_finish_apart(count):
+    """Codewords of one pair converge at different iterations (SNR spread over the batch),
+    odd batch sizes leave a lane without a codeword; BG1 Z=384 takes the compile-time-Z
+    instantiation, Z=192 the run-time one with two pairs per CTA."""
+    for z in (384, 192):
+        code = O.Code.nr(0, z)
+        dec = S.QcLdpcDecoder.with_lifting_size(0, z, 0.5)
+        rows, refs = [], []
+        for i in range(count):
+            info = O.random_bits(900 + i, code.k)
+            cw = code.encode(info)
+            app = O.quantize_i16(O.awgn(cw, -0.5 + 0.4 * i, code.k / code.n, 1000 + 13 * i))
+            rows.append(app[2 * z:].astype(np.int8))
+            full = np.concatenate([np.zeros(2 * z, np.int16), app[2 * z:]])
+            refs.append(code.decode_i8(code.prologue_5g_i8(full, 0), 4, 8))
+        r = gpu_i8(dec, np.stack(rows), 8, S.QuantParams(), "pair", llr_offset=2 * z, nr_prologue=True,
+                   hard_bits=code.k)
+        assert_i8_equal(f"pair z{z} count{count}", refs, r)
 
 
 def test_int8_wifi_matrices():
