@@ -4,7 +4,8 @@
 //
 // Layer l's edges are loff(l)..loff(l+1)-1 with column col(e), in the order of
 // the reference's build_layout (src/qc_ldpc.rs:281-319).  Layers >= 4 each own
-// one degree-1 extension column, column KB + l.
+// one degree-1 extension column, column KB + l.  z384_shift(e) is edge e's cyclic
+// shift at lifting size 384.
 #pragma once
 
 #ifndef __CUDACC__
@@ -34,6 +35,7 @@ struct Tab<0> {
   static constexpr int MB = 46, NB = 68, KB = 22, E = 316;
   __host__ __device__ static constexpr int loff(int i) { return syn_bg1_loff(i); }
   __host__ __device__ static constexpr int col(int e) { return syn_bg1_lcol(e); }
+  __host__ __device__ static constexpr int z384_shift(int e) { return syn_bg1_lz384(e); }
 };
 
 template <>
@@ -41,6 +43,7 @@ struct Tab<1> {
   static constexpr int MB = 42, NB = 52, KB = 10, E = 197;
   __host__ __device__ static constexpr int loff(int i) { return syn_bg2_loff(i); }
   __host__ __device__ static constexpr int col(int e) { return syn_bg2_lcol(e); }
+  __host__ __device__ static constexpr int z384_shift(int e) { return syn_bg2_lz384(e); }
 };
 
 template <int BG>

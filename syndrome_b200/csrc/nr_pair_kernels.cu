@@ -34,9 +34,14 @@ struct PairArgs {
   int cz4[Tab<BG>::E];      // 4 * col * z
 };
 
+// ZT = 384: lifting size, shifts, column bases and the CTA width (one pair of 384
+// threads) are compile-time constants, so every shared-memory address is a register
+// plus an immediate.  ZT = 0: any Z, shifts and column bases from the kernel parameters.
 template <int BG, int ZT>
 struct DevCtx {
+  static_assert(ZT == 0 || ZT == 384, "compile-time lifting size must be 384");
   static constexpr int NX = ext_regs<BG>();
+  static constexpr int NS = ZT > 0 ? kPairThreads : 0;
   unsigned char* ap;
   uint32_t* st;
   int ns;
@@ -48,17 +53,21 @@ struct DevCtx {
   template <int GE>
   __device__ __forceinline__ int vb() const {
     // (z + shift) mod Z in bytes, as an unsigned min: below Z the second candidate wraps high.
-    const unsigned r = (unsigned)(z4 + a->sh4[GE]);
-    const unsigned rr = min(r, r - (unsigned)(ZT > 0 ? ZT * 4 : Z4));
-    if constexpr (ZT > 0)
+    if constexpr (ZT > 0) {
+      const unsigned r = (unsigned)(z4 + Tab<BG>::z384_shift(GE) * 4);
+      const unsigned rr = min(r, r - (unsigned)(ZT * 4));
       return (int)rr + Tab<BG>::col(GE) * ZT * 4;
-    else
+    } else {
+      const unsigned r = (unsigned)(z4 + a->sh4[GE]);
+      const unsigned rr = min(r, r - (unsigned)Z4);
       return (int)rr + a->cz4[GE];
+    }
   }
+  __device__ __forceinline__ int stride() const { return NS > 0 ? NS : ns; }
   __device__ __forceinline__ uint32_t ld_ap(int b) const { return *reinterpret_cast<const uint32_t*>(ap + b); }
   __device__ __forceinline__ void st_ap(int b, uint32_t v) { *reinterpret_cast<uint32_t*>(ap + b) = v; }
-  __device__ __forceinline__ uint32_t ld_st(int w) const { return st[w * ns]; }
-  __device__ __forceinline__ void st_st(int w, uint32_t v) { st[w * ns] = v; }
+  __device__ __forceinline__ uint32_t ld_st(int w) const { return st[w * stride()]; }
+  __device__ __forceinline__ void st_st(int w, uint32_t v) { st[w * stride()] = v; }
   __device__ __forceinline__ uint32_t xr(int i) const { return x[i]; }
 };
 
@@ -81,8 +90,8 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
   extern __shared__ __align__(16) unsigned char smem[];
   const NrCommon& c = a.c;
   const int Z = ZT > 0 ? ZT : c.z;
-  const int P = c.cpb;
-  const int ns = blockDim.x;
+  const int P = ZT > 0 ? 1 : c.cpb;
+  const int ns = ZT > 0 ? kPairThreads : (int)blockDim.x;
   int* s_fail = reinterpret_cast<int*>(smem);
   int* s_done = s_fail + P;
   unsigned char* ap_base = smem + al16(8 * P);

@@ -93,7 +93,8 @@ def render_layered(bgs):
         "// Generated by syndrome_b200/tables/gen_base_graphs.py; do not edit.",
         "// For layer l, edges loff(l)..loff(l+1)-1 have column col(e) and take their",
         "// shift from base_graph_tables.inc entry ent(e) (the order of the reference's",
-        "// build_layout, src/qc_ldpc.rs:281-319).  Functions with local constexpr",
+        "// build_layout, src/qc_ldpc.rs:281-319); lz384(e) is that edge's shift at",
+        "// Z = 384 (lifting set 1, reduced mod 384).  Functions with local constexpr",
         "// tables so that device code can evaluate them at compile time.",
         "#pragma once",
         "",
@@ -107,7 +108,9 @@ def render_layered(bgs):
         for r in range(rows):
             off.append(off[-1] + sum(1 for rr, _, _ in ents if rr == r))
         up = name.upper()
-        for fn, vals in (("loff", off), ("lcol", [ents[i][1] for i in order]), ("lent", order)):
+        # shifts at Z = 384 (lifting set index 1, a = 3), reduced mod 384 like build_nr_graph
+        z384 = [ents[i][2][1] % 384 for i in order]
+        for fn, vals in (("loff", off), ("lcol", [ents[i][1] for i in order]), ("lent", order), ("lz384", z384)):
             lines.append(f"__host__ __device__ constexpr int syn_{name}_{fn}(int i) {{")
             lines.append(f"  constexpr int t[{len(vals)}] = {{{', '.join(str(x) for x in vals)}}};")
             lines.append("  return t[i];")

@@ -24,7 +24,9 @@ struct EmuCtx {
   const int* sh;
   template <int GE>
   int vb() const {
-    return (Tab<BG>::col(GE) * Z + (z + sh[GE]) % Z) * 4;
+    // at Z = 384 the compile-time shift table, as in the kernel's Z = 384 instantiation
+    const int s = Z == 384 ? Tab<BG>::z384_shift(GE) : sh[GE];
+    return (Tab<BG>::col(GE) * Z + (z + s) % Z) * 4;
   }
   uint32_t ld_ap(int b) const { return ap[b / 4]; }
   void st_ap(int b, uint32_t v) { ap[b / 4] = v; }
