@@ -53,12 +53,16 @@ struct DevCtx {
   template <int GE>
   __device__ __forceinline__ int vb() const {
     // (z + shift) mod Z in bytes, as an unsigned min: below Z the second candidate wraps high.
+    // An opaque copy of z4 per edge keeps the compiler from hoisting all the loop-invariant
+    // addresses of the unrolled graph out of the iteration loop (hundreds of registers).
+    int zl = z4;
+    asm volatile("" : "+r"(zl));
     if constexpr (ZT > 0) {
-      const unsigned r = (unsigned)(z4 + Tab<BG>::z384_shift(GE) * 4);
+      const unsigned r = (unsigned)(zl + Tab<BG>::z384_shift(GE) * 4);
       const unsigned rr = min(r, r - (unsigned)(ZT * 4));
       return (int)rr + Tab<BG>::col(GE) * ZT * 4;
     } else {
-      const unsigned r = (unsigned)(z4 + a->sh4[GE]);
+      const unsigned r = (unsigned)(zl + a->sh4[GE]);
       const unsigned rr = min(r, r - (unsigned)Z4);
       return (int)rr + a->cz4[GE];
     }
@@ -81,6 +85,49 @@ __host__ __device__ inline int pair_smem_bytes(int pairs, int z, int threads) {
 }
 
 __device__ __forceinline__ int lane_of(uint32_t w, int lane) { return (int)((w >> (16 * lane)) & 0xFFFFu) - (int)kPB; }
+
+// Cold paths as separate functions (own register allocation; the caller passes a copy
+// of its context so that the hot loop's registers stay where they are).
+
+// Parity of every check row except the quick layer's (bit 0 lane A odd, bit 1 lane B).
+template <int BG, int ZT>
+__device__ __noinline__ uint32_t full_parity(const DevCtx<BG, ZT>* cx) {
+  constexpr int QL = quick_layer<BG>();
+  uint32_t odd = 0u;
+  static_for<0, Tab<BG>::MB>([&](auto li) {
+    constexpr int L = decltype(li)::value;
+    if constexpr (L != QL) odd |= pair_parity<BG, L>(*cx);
+  });
+  return odd;
+}
+
+// This thread's share of lane X's results: its extension posteriors / hard decisions
+// (also into the shared-memory byte array eh for the packed output) and the messages
+// of its check rows in the reference's edge_r layout.
+template <int BG, int ZT>
+__device__ __noinline__ void write_rows(const DevCtx<BG, ZT>* cx, const NrCommon* c, int X, long long cw, int Z,
+                                        int z, uint8_t* eh) {
+  using T = Tab<BG>;
+  static_for<4, T::MB>([&](auto li) {
+    constexpr int L = decltype(li)::value;
+    const int v = lane_of(pair_ext_app<BG, L>(*cx), X);
+    const int j = (T::KB + L) * Z + z;
+    eh[(L - 4) * Z + z] = v < 0 ? 1 : 0;
+    if (c->app_out) c->app_out[cw * c->app_stride + j] = (int16_t)v;
+    if (c->hard_out) c->hard_out[cw * c->hard_stride + j] = v < 0 ? 1 : 0;
+  });
+  if (c->edge_r_out) {
+    int8_t* er = c->edge_r_out + cw * c->edge_r_stride;
+    static_for<0, T::MB>([&](auto li) {
+      constexpr int L = decltype(li)::value;
+      static_for<0, deg_of<BG>(L)>([&](auto ei) {
+        constexpr int e = decltype(ei)::value;
+        const uint32_t m = pair_message<BG, L, e>(*cx);
+        er[(long long)(T::loff(L) + e) * Z + z] = (int8_t)((int)((m >> (16 * X)) & 0xFFu) - 127);
+      });
+    });
+  }
+}
 
 template <int BG, int ZT, bool FILL>
 __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_constant__ PairArgs<BG> a) {
@@ -172,25 +219,8 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
         if (mine) {
           const long long cw = 2 * g + X;
           if (z == 0 && c.iters) c.iters[cw] = it;
-          static_for<4, T::MB>([&](auto li) {
-            constexpr int L = decltype(li)::value;
-            const int v = lane_of(pair_ext_app<BG, L>(cx), X);
-            const int j = (T::KB + L) * Z + z;
-            eh[(L - 4) * Z + z] = v < 0 ? 1 : 0;
-            if (c.app_out) c.app_out[cw * c.app_stride + j] = (int16_t)v;
-            if (c.hard_out) c.hard_out[cw * c.hard_stride + j] = v < 0 ? 1 : 0;
-          });
-          if (c.edge_r_out) {
-            int8_t* er = c.edge_r_out + cw * c.edge_r_stride;
-            static_for<0, T::MB>([&](auto li) {
-              constexpr int L = decltype(li)::value;
-              static_for<0, deg_of<BG>(L)>([&](auto ei) {
-                constexpr int e = decltype(ei)::value;
-                const uint32_t m = pair_message<BG, L, e>(cx);
-                er[(long long)(T::loff(L) + e) * Z + z] = (int8_t)((int)((m >> (16 * X)) & 0xFFu) - 127);
-              });
-            });
-          }
+          const DevCtx<BG, ZT> copy = cx;
+          write_rows<BG, ZT>(&copy, &c, X, cw, Z, z, eh);
         }
         __syncthreads();
         for (int q = 0; q < P; ++q) {
@@ -238,12 +268,8 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
       __syncthreads();
       const uint32_t pass = act & ~(uint32_t)(lane_ok ? s_fail[p] : 0);
       if (pass) {
-        uint32_t odd = 0u;
-        static_for<0, T::MB>([&](auto li) {
-          constexpr int L = decltype(li)::value;
-          if constexpr (L != QL) odd |= pair_parity<BG, L>(cx);
-        });
-        odd &= pass;
+        const DevCtx<BG, ZT> copy = cx;
+        const uint32_t odd = full_parity<BG, ZT>(&copy) & pass;
         if (odd) atomicOr(&s_fail[p], (int)odd);
       }
       __syncthreads();
