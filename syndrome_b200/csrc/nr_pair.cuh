@@ -9,8 +9,8 @@
 //
 // Lane encodings (per 16-bit lane, all values non-negative so that one 32-bit add
 // or subtract never carries across lanes, and unsigned 16x2 min/max order them):
-//   posterior / Q      PB + v with PB = 0x4000 (|v| <= 3938 + 127, or the filler
-//                      proxy below); bit 14 of the lane is 1 iff v >= 0
+//   posterior / Q      PB + v with PB = 0x8000 (|v| <= 3938 + 127, or the filler
+//                      proxy below); the lane's top bit is 1 iff v >= 0
 //   message table out  127 + R (R in [-127, 127]), zero-extended
 //   min-sum key        |Q| * 128 + tag(edge)
 //
@@ -49,8 +49,8 @@ using nr::quick_layer;
 using nr::static_for;
 using nr::Tab;
 
-constexpr uint32_t kPB = 0x4000u;            // lane bias
-constexpr uint32_t kPB2 = 0x40004000u;
+constexpr uint32_t kPB = 0x8000u;            // lane bias
+constexpr uint32_t kPB2 = 0x80008000u;
 constexpr int kCapV = 8192;                  // filler proxy ceiling (>= 7874)
 constexpr uint32_t kCap2 = (kPB + kCapV) * 0x10001u;
 constexpr int kMinFillerClamp = 7874;        // 30 * 254 + 2 * 127: deficit bound plus Q clamp
@@ -100,6 +100,16 @@ __host__ __device__ __forceinline__ uint32_t vminu2(uint32_t a, uint32_t b) {
 #endif
 }
 
+// High word of a * b: a >> (32 - log2 b) for a power-of-two b, as a multiply (FMA pipe)
+// instead of a shift (ALU pipe).
+__host__ __device__ __forceinline__ uint32_t mulhi(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
 // x << n with n >= 32 (including "negative" n wrapped to large unsigned) giving 0.
 __host__ __device__ __forceinline__ uint32_t shl_sat(uint32_t x, uint32_t n) {
 #ifdef __CUDA_ARCH__
@@ -137,9 +147,10 @@ __host__ __device__ constexpr int ext_regs() {
   return (Tab<BG>::MB - 4 + 1) / 2;
 }
 
-// Byte-permute selector of edge e from its code word.
+// Byte-permute selector of edge e from its code word (the shift as a multiply-high).
 __host__ __device__ __forceinline__ uint32_t code_sel(uint32_t code_word, int shift) {
-  return ((code_word >> shift) & 0x0303u) | 0xC480u;
+  const uint32_t w = shift ? mulhi(code_word, 1u << (32 - shift)) : code_word;
+  return (w & 0x0303u) | 0xC480u;
 }
 // Message table of a meta word: lanes 127 + R after prmt(lo, hi, selector).
 __host__ __device__ __forceinline__ uint32_t table_lo(uint32_t meta) { return (meta & 0xFFFFu) * 0xFFFFu + 0x7F7F7F7Fu; }
@@ -147,7 +158,7 @@ __host__ __device__ __forceinline__ uint32_t table_hi(uint32_t meta) { return (m
 
 // Biased channel value lanes (PB + x) of extension layer index xi (= layer - 4).
 __host__ __device__ __forceinline__ uint32_t ext_lanes(uint32_t xreg, int xi) {
-  return prmt(xreg, 0u, (xi & 1) ? 0x4342u : 0x4140u) + 0x3F803F80u;
+  return prmt(xreg, 0u, (xi & 1) ? 0x4342u : 0x4140u) + 0x7F807F80u;
 }
 
 // ------------------------------------------------------------- row update ---
@@ -172,7 +183,7 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
   const uint32_t tlo = table_lo(meta), thi = table_hi(meta);
   uint32_t qu[deg];
   int vb[deg];
-  uint32_t m1k = 0x7FFF7FFFu, m2k = 0x7FFF7FFFu, sx = 0u;
+  uint32_t m1k = 0x7FFF7FFFu, m2k = 0x7FFF7FFFu;
   static_for<0, deg>([&](auto ei) {
     constexpr int e = decltype(ei)::value;
     if constexpr (e == ep) {
@@ -183,21 +194,23 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
       const uint32_t a = c.ld_ap(vb[e]);
       qu[e] = a - prmt(tlo, thi, code_sel(code[e >> 3], code_shift(e))) + 0x007F007Fu;  // PB + app - R_old
     }
-    // PB + min(|Q|, 127), then key = |Q| * 128 + tag (the 128 * PB terms cancel mod 2^32)
-    const uint32_t aq = vminu2(vmaxu2(qu[e], 0x80008000u - qu[e]), 0x407F407Fu);
-    const uint32_t key = aq * 128u + ((uint32_t)key_tag(e) * 0x10001u - 0x00200000u);
+    // PB + min(|Q|, 127) (0x10000 - Q32 is PB - Q in both lanes), then
+    // key = |Q| * 128 + tag (the 128 * PB terms cancel mod 2^32)
+    const uint32_t aq = vminu2(vmaxu2(qu[e], 0x00010000u - qu[e]), 0x807F807Fu);
+    const uint32_t key = aq * 128u + ((uint32_t)key_tag(e) * 0x10001u - 0x00400000u);
     m2k = vminu2(m2k, vmaxu2(m1k, key));
     m1k = vminu2(m1k, key);
-    sx ^= qu[e];
   });
   // Row results: offset magnitudes, new meta word and message table.
   const uint32_t m1 = (m1k >> 7) & 0x007F007Fu, m2 = (m2k >> 7) & 0x007F007Fu;
   const uint32_t m1p = vmaxu2(m1, bq2) - bq2, m2p = vmaxu2(m2, bq2) - bq2;
   const uint32_t nmeta = m2p * 256u + m1p;
   const uint32_t nlo = table_lo(nmeta), nhi = table_hi(nmeta);
-  // Code words: Q >= 0 bits (bit 6 of bytes 1 and 3 of Q) moved to each edge's sign
-  // slot, two edges per byte-permute ...
+  // Code words: the Q >= 0 bits (top bits of the lanes) of edges j and j + 4 spread to
+  // whole bytes by one sign-replicating byte-permute, then masked into each edge's
+  // sign slot ...
   uint32_t nc[NC];
+  uint32_t sacc = 0u;
   static_for<0, NC>([&](auto ki) {
     constexpr int k = decltype(ki)::value;
     nc[k] = 0u;
@@ -207,17 +220,15 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
       if constexpr (e0 < deg) {
         uint32_t hi = 0u;
         if constexpr (e1 < deg) hi = qu[e1];
-        const uint32_t t = prmt(qu[e0], hi, 0x7531u) & 0x40404040u;
-        if constexpr (j == 3)
-          nc[k] += t << 1;
-        else
-          nc[k] += t >> (5 - 2 * j);
+        const uint32_t t = prmt(qu[e0], hi, 0xFDB9u);  // bytes: A_j, B_j, A_j+4, B_j+4 as 0x00 / 0xFF
+        nc[k] |= t & (0x02020202u << (2 * j));
+        sacc ^= t;
       }
     });
   });
   // ... turned into R's sign (Q >= 0 xor an odd count of negative Q in the row) ...
-  const uint32_t sp = prmt(sx, 0u, 0x4431u);
-  const uint32_t sn = ((sp >> 6) & 0x0101u) ^ ((deg & 1) ? 0x0101u : 0u);
+  const uint32_t par = sacc ^ (sacc >> 16);  // byte 0: lane A parity of Q >= 0, byte 1: lane B
+  const uint32_t sn = (par & 0x0101u) ^ ((deg & 1) ? 0x0101u : 0u);
   const uint32_t smask = sn * 0x00AA00AAu;
   // ... plus the argmin flag from the winning key's tag.
   const uint32_t tA = m1k & 127u, tB = (m1k >> 16) & 127u;
@@ -271,7 +282,7 @@ __host__ __device__ __forceinline__ uint32_t pair_parity(const C& c) {
       x ^= c.ld_ap(c.template vb<lb + e>());
     }
   });
-  const uint32_t nn = ((x >> 14) & 1u) | ((x >> 29) & 2u);
+  const uint32_t nn = ((x >> 15) & 1u) | ((x >> 30) & 2u);
   return nn ^ ((deg & 1) ? 3u : 0u);
 }
 

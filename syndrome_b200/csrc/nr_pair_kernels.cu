@@ -27,6 +27,11 @@ namespace nrp {
 
 constexpr int kPairThreads = 384;
 
+// The kernel's dynamic shared memory.  The context below addresses it by byte offsets
+// from this symbol (not by pointers), so that every access compiles to a shared-memory
+// instruction also inside the non-inlined helpers.
+extern __shared__ __align__(16) unsigned char pair_smem[];
+
 template <int BG>
 struct PairArgs {
   NrCommon c;               // c.cpb = codeword pairs per CTA
@@ -42,8 +47,8 @@ struct DevCtx {
   static_assert(ZT == 0 || ZT == 384, "compile-time lifting size must be 384");
   static constexpr int NX = ext_regs<BG>();
   static constexpr int NS = ZT > 0 ? kPairThreads : 0;
-  unsigned char* ap;
-  uint32_t* st;
+  int ap;   // byte offset of this pair's posteriors in pair_smem
+  int st;   // byte offset of this thread's first state word in pair_smem
   int ns;
   int z4;
   int Z4;
@@ -68,10 +73,16 @@ struct DevCtx {
     }
   }
   __device__ __forceinline__ int stride() const { return NS > 0 ? NS : ns; }
-  __device__ __forceinline__ uint32_t ld_ap(int b) const { return *reinterpret_cast<const uint32_t*>(ap + b); }
-  __device__ __forceinline__ void st_ap(int b, uint32_t v) { *reinterpret_cast<uint32_t*>(ap + b) = v; }
-  __device__ __forceinline__ uint32_t ld_st(int w) const { return st[w * stride()]; }
-  __device__ __forceinline__ void st_st(int w, uint32_t v) { st[w * stride()] = v; }
+  __device__ __forceinline__ uint32_t ld_ap(int b) const {
+    return *reinterpret_cast<const uint32_t*>(pair_smem + ap + b);
+  }
+  __device__ __forceinline__ void st_ap(int b, uint32_t v) { *reinterpret_cast<uint32_t*>(pair_smem + ap + b) = v; }
+  __device__ __forceinline__ uint32_t ld_st(int w) const {
+    return *reinterpret_cast<const uint32_t*>(pair_smem + st + 4 * w * stride());
+  }
+  __device__ __forceinline__ void st_st(int w, uint32_t v) {
+    *reinterpret_cast<uint32_t*>(pair_smem + st + 4 * w * stride()) = v;
+  }
   __device__ __forceinline__ uint32_t xr(int i) const { return x[i]; }
 };
 
@@ -106,7 +117,8 @@ __device__ __noinline__ uint32_t full_parity(const DevCtx<BG, ZT>* cx) {
 // of its check rows in the reference's edge_r layout.
 template <int BG, int ZT>
 __device__ __noinline__ void write_rows(const DevCtx<BG, ZT>* cx, const NrCommon* c, int X, long long cw, int Z,
-                                        int z, uint8_t* eh) {
+                                        int z, int eh_off) {
+  unsigned char* eh = pair_smem + eh_off;
   using T = Tab<BG>;
   static_for<4, T::MB>([&](auto li) {
     constexpr int L = decltype(li)::value;
@@ -134,7 +146,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
   using T = Tab<BG>;
   constexpr int NW = state_words<BG>(), CORE = T::KB + 4, NEXT = T::MB - 4;
   constexpr int QL = quick_layer<BG>();
-  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char* smem = pair_smem;
   const NrCommon& c = a.c;
   const int Z = ZT > 0 ? ZT : c.z;
   const int P = ZT > 0 ? 1 : c.cpb;
@@ -150,8 +162,8 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
   const bool lane_ok = p < P;
   const int pq = lane_ok ? p : 0;
   DevCtx<BG, ZT> cx;
-  cx.ap = ap_base + pq * ap_pair;
-  cx.st = st_base + tid;
+  cx.ap = (int)(ap_base - smem) + pq * ap_pair;
+  cx.st = (int)(reinterpret_cast<unsigned char*>(st_base) - smem) + 4 * tid;
   cx.ns = ns;
   cx.z4 = z * 4;
   cx.Z4 = Z * 4;
@@ -172,7 +184,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
       const int8_t* sa = va ? c.llr + 2 * g * c.llr_stride - c.llr_offset : nullptr;
       const int8_t* sb = vbv ? c.llr + (2 * g + 1) * c.llr_stride - c.llr_offset : nullptr;
       auto fetch = [&](const int8_t* s, int j) -> int { return (s && j >= c.llr_offset) ? (int)s[j] : 0; };
-      uint32_t* apw = reinterpret_cast<uint32_t*>(cx.ap);
+      uint32_t* apw = reinterpret_cast<uint32_t*>(smem + cx.ap);
       for (int col = 0; col < CORE; ++col) {
         const int j = col * Z + z;
         uint32_t l0 = kPB + (uint32_t)fetch(sa, j), l1 = kPB + (uint32_t)fetch(sb, j);
@@ -220,7 +232,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
           const long long cw = 2 * g + X;
           if (z == 0 && c.iters) c.iters[cw] = it;
           const DevCtx<BG, ZT> copy = cx;
-          write_rows<BG, ZT>(&copy, &c, X, cw, Z, z, eh);
+          write_rows<BG, ZT>(&copy, &c, X, cw, Z, z, (int)(eh - smem));
         }
         __syncthreads();
         for (int q = 0; q < P; ++q) {
