@@ -265,6 +265,33 @@ int32_t syndrome_mixed_decode(SyndromeMixedPlan* plan, const int8_t* d_llr, size
                               uint32_t* d_hard_packed, size_t out_words, int32_t* d_iters, size_t iters_len,
                               int32_t use_graph, void* stream);
 
+/* ===================================== 4. transport blocks (DL-SCH) ===== */
+
+/* src/segmentation.rs:265 compute_segmentation.  out10 = {base graph (0 = BG1),
+ * Z, C code blocks, B = A + 24, K', K, Ncb = N - 2Z, filler bits, has CB CRC,
+ * TB bits per code block}. */
+int32_t syndrome_tb_segmentation(size_t tb_size, float target_rate, int64_t* out10);
+/* src/crc.rs:153 Crc24::compute over n bits (one per byte, LSB used): kind 0 =
+ * CRC-24A (0x864CFB), 1 = CRC-24B (0x800063).  MSB-first, zero initial value. */
+uint32_t syndrome_crc24(const uint8_t* bits, size_t n, int32_t kind);
+
+typedef struct SyndromeDlSchEncoder SyndromeDlSchEncoder;
+/* src/transport_block.rs:221 DlSchEncoder::new(tb_size, target_rate, qm, g).
+ * Additionally rejects an E per code block that the reference's rate-matching walk
+ * would not fill (code rates far below 1/5). */
+int32_t syndrome_dlsch_encoder_create(size_t tb_size, float target_rate, size_t qm, size_t g,
+                                      SyndromeDlSchEncoder** out_encoder);
+void syndrome_dlsch_encoder_destroy(SyndromeDlSchEncoder* encoder);
+/* src/transport_block.rs:275 output_bits (C * E). */
+size_t syndrome_dlsch_encoder_output_bits(const SyndromeDlSchEncoder* encoder);
+/* src/transport_block.rs:280 num_code_blocks. */
+size_t syndrome_dlsch_encoder_num_code_blocks(const SyndromeDlSchEncoder* encoder);
+/* src/transport_block.rs:303 encode: TB CRC-24A, segmentation with CRC-24B, LDPC
+ * encoding, rate matching for redundancy version rv.  tb_len must equal tb_size and
+ * out_len be at least output_bits (BUFFER_TOO_SMALL); rv > 3 is INVALID_PARAM. */
+int32_t syndrome_dlsch_encode(const SyndromeDlSchEncoder* encoder, const uint8_t* tb, size_t tb_len,
+                              size_t rv, uint8_t* out, size_t out_len);
+
 /* Text of the last error on this thread (empty if none). */
 const char* syndrome_last_error(void);
 

@@ -16,6 +16,9 @@
 //   * quantizer / beta_q        src/quantize.rs:148-155, 298-305, 331-343 (+float_ext.rs round)
 //   * encoder                   src/qc_ldpc.rs:2166-2727 (sparse core solve) and :1996-2125 (dense)
 //   * AWGN channel              src/channel_sim.rs:61-241
+//   * DL-SCH transport blocks   segmentation.rs:75-400, crc.rs:65-350, rate_matching.rs:72-700,
+//                               harq.rs:77-195, transport_block.rs:203-1053 (the decoder chain
+//                               with the int8 decode: HARQ f32 sum -> quantize -> decode_5g_i8)
 // Built with -ffp-contract=off and without -ffast-math so IEEE f32 operations
 // happen exactly as written.
 #include <cfloat>
@@ -648,6 +651,256 @@ uint64_t orc_fnv1a_hard(const uint8_t* hard, long n) {
     h *= 0x00000100000001b3ull;
   }
   return h;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ DL-SCH --
+// Transport-block chain, restated from syndrome segmentation.rs, crc.rs,
+// rate_matching.rs (the step-by-step selection walk), harq.rs and
+// transport_block.rs (DlSchEncoder::encode, DlSchDecoder::decode with its
+// sequential per-code-block loop).  The code-block decode is the int8 one:
+// HARQ-combined f32 LLRs quantized by quantize_llr_i16, then decode_5g_i8.
+
+struct OrcSeg {
+  int bg, z, c;
+  long b;
+  int kp, k, n, nf, has_crc, payload;
+};
+
+static int orc_seg(long a, float r, OrcSeg* s) {
+  static const int vz[] = {2,  3,  4,  5,  6,  7,  8,  9,   10,  11,  12,  13,  14,  15,  16,  18,  20,
+                           22, 24, 26, 28, 30, 32, 36, 40,  44,  48,  52,  56,  60,  64,  72,  80,  88,
+                           96, 104, 112, 120, 128, 144, 160, 176, 192, 208, 224, 240, 256, 288, 320, 352, 384};
+  if (a == 0 || a > 1277992) return -1;
+  const int bg2 = a <= 292 || (a <= 3824 && r <= 0.67f) || r <= 0.25f;
+  const long k_cb = bg2 ? 3840 : 8448;
+  const int n_b = bg2 ? 50 : 66;
+  const long b = a + 24;
+  long c = 1, l = 0;
+  if (b > k_cb) {
+    c = (b + (k_cb - 24) - 1) / (k_cb - 24);
+    l = 24;
+  }
+  const long bp = b + c * l;
+  const long kp = (bp + c - 1) / c;
+  int kb = 22;
+  if (bg2) kb = b > 640 ? 10 : (b > 560 ? 9 : (b > 192 ? 8 : 6));
+  int z = 0;
+  for (int v : vz)
+    if ((long)kb * v >= kp) {
+      z = v;
+      break;
+    }
+  if (!z) return -1;
+  s->bg = bg2 ? 1 : 0;
+  s->z = z;
+  s->c = (int)c;
+  s->b = b;
+  s->kp = (int)kp;
+  s->k = (bg2 ? 10 : 22) * z;
+  s->n = n_b * z;
+  s->nf = s->k - s->kp;
+  s->has_crc = l > 0;
+  s->payload = l > 0 ? s->kp - 24 : s->kp;
+  return 0;
+}
+
+// crc.rs bit_serial_step over the whole message.
+static uint32_t orc_crc_bits(const uint8_t* bits, long n, uint32_t poly) {
+  uint32_t reg = 0;
+  for (long i = 0; i < n; ++i) {
+    const uint32_t fb = ((reg >> 23) ^ (bits[i] & 1u)) & 1u;
+    const uint32_t sh = (reg << 1) & 0xFFFFFFu;
+    reg = fb ? sh ^ poly : sh;
+  }
+  return reg;
+}
+
+// rate_matching.rs selection_walk: positions of the e selected bits (0 where the
+// walk's 2 * ncb guard stopped it).
+static std::vector<long> orc_sel_walk(int bg, int z, int rv, int nf, long e) {
+  static const int k0s[2][4] = {{0, 17, 33, 56}, {0, 13, 25, 43}};
+  const long ncb = (bg == 0 ? 66L : 50L) * z, k = (bg == 0 ? 22L : 10L) * z;
+  const long kp = k > nf ? k - nf : 0, tz = 2L * z;
+  const long fs = kp > tz ? kp - tz : 0, fe = k > tz ? k - tz : 0;
+  const long k0 = (long)k0s[bg][rv] * z;
+  std::vector<long> sel(e, 0);
+  long ks = 0, j = 0;
+  while (ks < e) {
+    const long pos = (k0 + j) % ncb;
+    if (pos >= fs && pos < fe) {
+      ++j;
+      continue;
+    }
+    sel[ks] = pos;
+    ++ks;
+    ++j;
+    if (j > 2 * ncb) break;
+  }
+  return sel;
+}
+
+struct OrcDlsch {
+  OrcSeg s;
+  long tb_size, e;
+  int qm, iterations, beta_q, app_clamp;
+  float scale;
+  void* params;
+  std::vector<std::vector<float>> acc;
+  std::vector<int> tx;
+};
+
+extern "C" {
+
+// compute_segmentation: out10 = {bg, z, c, b, K', K, ncb, n_filler, has_cb_crc, payload}.
+int orc_segmentation(long a, float rate, long* out10) {
+  OrcSeg s;
+  if (orc_seg(a, rate, &s)) return -1;
+  const long v[10] = {s.bg, s.z, s.c, s.b, s.kp, s.k, s.n, s.nf, s.has_crc, s.payload};
+  for (int i = 0; i < 10; ++i) out10[i] = v[i];
+  return 0;
+}
+
+// kind 0 = CRC-24A (0x864CFB), 1 = CRC-24B (0x800063).
+unsigned orc_crc24(const uint8_t* bits, long n, int kind) {
+  return orc_crc_bits(bits, n, kind == 0 ? 0x864CFBu : 0x800063u);
+}
+
+// DlSchEncoder::new + encode: out receives C * E bits.  Returns the bit count or -1.
+long orc_dlsch_encode(long tb_size, float rate, int qm, long g, int rv, const uint8_t* tb, uint8_t* out) {
+  OrcSeg s;
+  if (tb_size <= 0 || qm <= 0 || g <= 0 || g % qm || rv < 0 || rv > 3 || orc_seg(tb_size, rate, &s)) return -1;
+  const long e = (g / s.c / qm) * qm;
+  std::vector<uint8_t> tbc(tb, tb + tb_size);
+  const uint32_t crc = orc_crc_bits(tbc.data(), tb_size, 0x864CFBu);
+  for (int i = 23; i >= 0; --i) tbc.push_back((crc >> i) & 1u);
+  void* p = orc_params_5g(s.bg, s.z);
+  const long n = (long)s.n + 2L * s.z;
+  std::vector<uint8_t> info(s.k), cw(n), ebuf(e), tmp(e);
+  const std::vector<long> sel = orc_sel_walk(s.bg, s.z, rv, s.nf, e);
+  for (int ci = 0; ci < s.c; ++ci) {
+    std::vector<uint8_t> cb;
+    const long start = (long)ci * s.payload, end = std::min(start + s.payload, s.b);
+    for (long i = start; i < end; ++i) cb.push_back(tbc[i]);
+    cb.resize(s.payload, 0);
+    if (s.has_crc) {
+      const uint32_t cc = orc_crc_bits(cb.data(), (long)cb.size(), 0x800063u);
+      for (int i = 23; i >= 0; --i) cb.push_back((cc >> i) & 1u);
+    }
+    std::fill(info.begin(), info.end(), 0);
+    std::copy(cb.begin(), cb.end(), info.begin());
+    orc_encode(p, info.data(), cw.data());
+    for (long ks = 0; ks < e; ++ks) {
+      const long idx = sel[ks] + 2L * s.z;
+      ebuf[ks] = idx < n ? cw[idx] : 0;
+    }
+    // rate_matching.rs interleave: out[col * rows + row] = e[row * qm + col]
+    const long rows = e / qm;
+    for (int col = 0; col < qm; ++col)
+      for (long row = 0; row < rows; ++row) tmp[col * rows + row] = ebuf[row * qm + col];
+    std::copy(tmp.begin(), tmp.end(), out + (long)ci * e);
+  }
+  orc_params_free(p);
+  return (long)s.c * e;
+}
+
+void* orc_dlsch_decoder_new(long tb_size, float rate, int qm, long g, int iterations, int beta_q, float scale,
+                            int app_clamp) {
+  OrcSeg s;
+  if (tb_size <= 0 || qm <= 0 || g <= 0 || g % qm || orc_seg(tb_size, rate, &s)) return nullptr;
+  OrcDlsch* d = new OrcDlsch();
+  d->s = s;
+  d->tb_size = tb_size;
+  d->e = (g / s.c / qm) * qm;
+  d->qm = qm;
+  d->iterations = iterations;
+  d->beta_q = beta_q;
+  d->scale = scale;
+  d->app_clamp = app_clamp;
+  d->params = orc_params_5g(s.bg, s.z);
+  d->acc.assign(s.c, std::vector<float>(s.n, 0.0f));
+  d->tx.assign(s.c, 0);
+  return d;
+}
+
+void orc_dlsch_decoder_free(void* h) {
+  OrcDlsch* d = static_cast<OrcDlsch*>(h);
+  if (!d) return;
+  orc_params_free(d->params);
+  delete d;
+}
+
+// DlSchDecoder::decode.  report4 = {crc_ok, max_iters_used, harq_tx_count, C};
+// cb_crc[C]; tb_out[tb_size] is written only when the CRCs pass; llr_out (nullable)
+// receives the quantized int8 decoder input of each code block (C x ncb, variables
+// 2Z..N); iters_out (nullable) the iterations of each code block.
+int orc_dlsch_decode(void* h, const float* rx, int rv, uint8_t* tb_out, int* report4, uint8_t* cb_crc,
+                     int8_t* llr_out, int* iters_out) {
+  OrcDlsch* d = static_cast<OrcDlsch*>(h);
+  const OrcSeg& s = d->s;
+  const long e = d->e, z = s.z, n = (long)s.n + 2 * z;
+  const int harq_tx = d->tx[0] + 1;
+  // RateMatchCache::dec_idx: received bit q -> selection index (q % rows) * qm + q / rows
+  const std::vector<long> sel = orc_sel_walk(s.bg, s.z, rv, s.nf, e);
+  const long rows = e / d->qm;
+  std::vector<uint8_t> all_info((size_t)s.c * s.payload, 0), hard(n);
+  std::vector<int16_t> app(n);
+  std::vector<float> llr(n);
+  int max_iters = 0;
+  bool all_cb = true;
+  for (int ci = 0; ci < s.c; ++ci) {
+    std::vector<float>& acc = d->acc[ci];
+    const float* x = rx + (long)ci * e;
+    for (long q = 0; q < e; ++q) {
+      const long idx = sel[(q % rows) * d->qm + q / rows];
+      if (idx < (long)acc.size()) acc[idx] += x[q];
+    }
+    d->tx[ci] += 1;
+    std::fill(llr.begin(), llr.end(), 0.0f);
+    std::copy(acc.begin(), acc.end(), llr.begin() + 2 * z);
+    orc_quantize_i16(llr.data(), app.data(), n, d->scale);
+    if (llr_out)
+      for (long j = 0; j < s.n; ++j) llr_out[(long)ci * s.n + j] = (int8_t)app[2 * z + j];
+    orc_prologue_5g_i8(d->params, app.data(), s.nf, d->app_clamp);
+    std::vector<int8_t> edge_r((size_t)(static_cast<Params*>(d->params)->cols.size() * z));
+    const long it = orc_decode_i8(d->params, d->beta_q, d->app_clamp, app.data(), edge_r.data(), hard.data(),
+                                  d->iterations);
+    if (iters_out) iters_out[ci] = (int)it;
+    max_iters = std::max(max_iters, (int)it);
+    bool ok = true;
+    if (s.has_crc) {  // crc.rs check: payload CRC against the trailing 24 bits
+      uint32_t rec = 0;
+      for (int i = 0; i < 24; ++i) rec = (rec << 1) | (hard[s.kp - 24 + i] & 1u);
+      ok = orc_crc_bits(hard.data(), s.kp - 24, 0x800063u) == rec;
+    }
+    cb_crc[ci] = ok ? 1 : 0;
+    all_cb = all_cb && ok;
+    std::copy(hard.begin(), hard.begin() + s.payload, all_info.begin() + (long)ci * s.payload);
+  }
+  const long ts = d->tb_size;
+  bool tb_ok = false;
+  if ((long)all_info.size() >= ts + 24) {
+    uint32_t rec = 0;
+    for (int i = 0; i < 24; ++i) rec = (rec << 1) | (all_info[ts + i] & 1u);
+    tb_ok = orc_crc_bits(all_info.data(), ts, 0x864CFBu) == rec;
+  }
+  if (all_cb && tb_ok) {
+    std::copy(all_info.begin(), all_info.begin() + ts, tb_out);
+    for (auto& a : d->acc) std::fill(a.begin(), a.end(), 0.0f);
+    std::fill(d->tx.begin(), d->tx.end(), 0);
+  }
+  report4[0] = all_cb && tb_ok;
+  report4[1] = max_iters;
+  report4[2] = harq_tx;
+  report4[3] = s.c;
+  return 0;
+}
+
+void orc_dlsch_flush(void* h) {
+  OrcDlsch* d = static_cast<OrcDlsch*>(h);
+  for (auto& a : d->acc) std::fill(a.begin(), a.end(), 0.0f);
+  std::fill(d->tx.begin(), d->tx.end(), 0);
 }
 
 }  // extern "C"

@@ -68,6 +68,13 @@ PROTOTYPES = {
     "syndrome_mixed_plan_items": (_i32, [_vp, _vp, _sz, ctypes.POINTER(_sz)]),
     "syndrome_mixed_tile_capacity": (_i32, [_i32, _i32]),
     "syndrome_mixed_decode": (_i32, [_vp, _vp, _sz, _vp, _sz, _vp, _sz, _i32, _vp]),
+    "syndrome_tb_segmentation": (_i32, [_sz, _f32, _vp]),
+    "syndrome_crc24": (ctypes.c_uint32, [_vp, _sz, _i32]),
+    "syndrome_dlsch_encoder_create": (_i32, [_sz, _f32, _sz, _sz, ctypes.POINTER(_vp)]),
+    "syndrome_dlsch_encoder_destroy": (None, [_vp]),
+    "syndrome_dlsch_encoder_output_bits": (_sz, [_vp]),
+    "syndrome_dlsch_encoder_num_code_blocks": (_sz, [_vp]),
+    "syndrome_dlsch_encode": (_i32, [_vp, _vp, _sz, _sz, _vp, _sz]),
     "syndrome_last_error": (ctypes.c_char_p, []),
 }
 

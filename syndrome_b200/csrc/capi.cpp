@@ -20,6 +20,7 @@
 #include "encoder.h"
 #include "graph.h"
 #include "mixed.h"
+#include "tb.h"
 
 struct SyndromeLdpcDecoder {
   syn::Graph graph;
@@ -39,6 +40,11 @@ struct SyndromeLdpcEncoder {
 
 struct SyndromeMixedPlan {
   syn::MixedPlan plan;
+};
+
+struct SyndromeDlSchEncoder {
+  syn::TbEncoder enc;
+  size_t tb_size = 0;
 };
 
 namespace {
@@ -648,6 +654,67 @@ int32_t syndrome_mixed_decode(SyndromeMixedPlan* plan, const int8_t* d_llr, size
     return from_cuda(plan->plan.decode(d_llr, d_hard_packed, d_iters, use_graph != 0,
                                        static_cast<cudaStream_t>(stream)),
                      "");
+  });
+}
+
+// ------------------------------------------------------- transport blocks ---
+
+int32_t syndrome_tb_segmentation(size_t tb_size, float target_rate, int64_t* out10) {
+  return guard([&]() -> int32_t {
+    if (!out10) return SYNDROME_NULL_POINTER;
+    syn::TbParams p;
+    std::string err;
+    if (!syn::compute_segmentation((long long)std::min<size_t>(tb_size, (size_t)LLONG_MAX), target_rate, &p, &err))
+      return fail(SYNDROME_INVALID_PARAM, err);
+    const int64_t v[10] = {p.bg, p.z, p.c, p.b, p.k_prime, p.k, p.ncb, p.n_filler, p.has_cb_crc ? 1 : 0, p.payload};
+    for (int i = 0; i < 10; ++i) out10[i] = v[i];
+    return SYNDROME_OK;
+  });
+}
+
+uint32_t syndrome_crc24(const uint8_t* bits, size_t n, int32_t kind) {
+  if (!bits && n) return 0;
+  return syn::crc24_bits(bits, (long long)n, kind == 0 ? syn::kCrc24A : syn::kCrc24B);
+}
+
+int32_t syndrome_dlsch_encoder_create(size_t tb_size, float target_rate, size_t qm, size_t g,
+                                      SyndromeDlSchEncoder** out) {
+  return guard([&]() -> int32_t {
+    if (!out) return SYNDROME_NULL_POINTER;
+    *out = nullptr;
+    if (tb_size > (size_t)syn::kMaxTbBits * 2 || qm > 64 || g > ((size_t)1 << 40))
+      return fail(SYNDROME_INVALID_PARAM, "argument out of range");
+    auto* e = new SyndromeDlSchEncoder();
+    std::string err;
+    if (!e->enc.init((long long)tb_size, target_rate, (int)qm, (long long)g, &err)) {
+      delete e;
+      return fail(SYNDROME_INVALID_PARAM, err);
+    }
+    e->tb_size = tb_size;
+    *out = e;
+    return SYNDROME_OK;
+  });
+}
+
+void syndrome_dlsch_encoder_destroy(SyndromeDlSchEncoder* encoder) { delete encoder; }
+
+size_t syndrome_dlsch_encoder_output_bits(const SyndromeDlSchEncoder* e) {
+  return e ? (size_t)e->enc.output_bits() : 0;
+}
+
+size_t syndrome_dlsch_encoder_num_code_blocks(const SyndromeDlSchEncoder* e) {
+  return e ? (size_t)e->enc.params().c : 0;
+}
+
+int32_t syndrome_dlsch_encode(const SyndromeDlSchEncoder* e, const uint8_t* tb, size_t tb_len, size_t rv, uint8_t* out,
+                              size_t out_len) {
+  return guard([&]() -> int32_t {
+    if (!e || !tb || !out) return SYNDROME_NULL_POINTER;
+    if (tb_len != e->tb_size) return fail(SYNDROME_BUFFER_TOO_SMALL, "tb length must equal tb_size");
+    if (out_len < (size_t)e->enc.output_bits()) return fail(SYNDROME_BUFFER_TOO_SMALL, "output shorter than output_bits");
+    if (rv > 3) return fail(SYNDROME_INVALID_PARAM, "RV must be 0..=3");
+    e->enc.encode(tb, (int)rv, out);
+    return SYNDROME_OK;
   });
 }
 

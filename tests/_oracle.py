@@ -56,6 +56,21 @@ def lib():
         L.orc_awgn_sigma.argtypes = [ctypes.c_float, ctypes.c_float]
         L.orc_awgn_transmit.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_uint64,
                                         ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p]
+        L.orc_segmentation.restype = ctypes.c_int
+        L.orc_segmentation.argtypes = [ctypes.c_long, ctypes.c_float, ctypes.c_void_p]
+        L.orc_crc24.restype = ctypes.c_uint
+        L.orc_crc24.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int]
+        L.orc_dlsch_encode.restype = ctypes.c_long
+        L.orc_dlsch_encode.argtypes = [ctypes.c_long, ctypes.c_float, ctypes.c_int, ctypes.c_long, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_dlsch_decoder_new.restype = ctypes.c_void_p
+        L.orc_dlsch_decoder_new.argtypes = [ctypes.c_long, ctypes.c_float, ctypes.c_int, ctypes.c_long, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_float, ctypes.c_int]
+        L.orc_dlsch_decoder_free.argtypes = [ctypes.c_void_p]
+        L.orc_dlsch_decode.restype = ctypes.c_int
+        L.orc_dlsch_decode.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_dlsch_flush.argtypes = [ctypes.c_void_p]
         L.orc_fnv1a_hard.restype = ctypes.c_uint64
         L.orc_fnv1a_hard.argtypes = [ctypes.c_void_p, ctypes.c_long]
         _LIB = L
@@ -179,3 +194,59 @@ def random_bits(seed, n):
         s ^= (s << 17) & M
         out[i] = (s >> 27) & 1
     return out
+
+
+# ------------------------------------------------------------------ DL-SCH --
+
+def segmentation(a, rate):
+    """compute_segmentation: (bg, z, c, b, k_prime, k, ncb, n_filler, has_cb_crc, payload) or None."""
+    out = np.zeros(10, dtype=np.int64)
+    if lib().orc_segmentation(a, rate, out.ctypes.data):
+        return None
+    return tuple(int(x) for x in out)
+
+
+def crc24(bits, kind=0):
+    b = np.ascontiguousarray(bits, dtype=np.uint8)
+    return int(lib().orc_crc24(b.ctypes.data, b.size, kind))
+
+
+def dlsch_encode(tb, rate, qm, g, rv):
+    tb = np.ascontiguousarray(tb, dtype=np.uint8)
+    out = np.zeros(g, dtype=np.uint8)
+    n = lib().orc_dlsch_encode(tb.size, rate, qm, g, rv, tb.ctypes.data, out.ctypes.data)
+    assert n >= 0
+    return out[:n]
+
+
+class DlSchDecoder:
+    """transport_block.rs DlSchDecoder with the int8 code-block decode (HARQ f32 sum,
+    quantize_llr_i16, decode_5g_i8)."""
+
+    def __init__(self, tb_size, rate, qm, g, iterations=8, beta_q=4, scale=8.0, app_clamp=32767):
+        self.h = lib().orc_dlsch_decoder_new(tb_size, rate, qm, g, iterations, beta_q, scale, app_clamp)
+        assert self.h
+        self.tb_size = tb_size
+        self.seg = segmentation(tb_size, rate)
+
+    def __del__(self):
+        try:
+            lib().orc_dlsch_decoder_free(self.h)
+        except Exception:
+            pass
+
+    def decode(self, rx, rv):
+        rx = np.ascontiguousarray(rx, dtype=np.float32)
+        c, ncb = self.seg[2], self.seg[6]
+        tb = np.zeros(self.tb_size, np.uint8)
+        rep = np.zeros(4, np.int32)
+        cb = np.zeros(c, np.uint8)
+        llr = np.zeros((c, ncb), np.int8)
+        its = np.zeros(c, np.int32)
+        lib().orc_dlsch_decode(self.h, rx.ctypes.data, rv, tb.ctypes.data, rep.ctypes.data, cb.ctypes.data,
+                               llr.ctypes.data, its.ctypes.data)
+        return dict(crc_ok=bool(rep[0]), max_iters=int(rep[1]), harq_tx=int(rep[2]), cb_crc=cb.astype(bool),
+                    tb=tb if rep[0] else None, llr=llr, iters=its)
+
+    def flush(self):
+        lib().orc_dlsch_flush(self.h)
