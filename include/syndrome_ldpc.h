@@ -292,6 +292,62 @@ size_t syndrome_dlsch_encoder_num_code_blocks(const SyndromeDlSchEncoder* encode
 int32_t syndrome_dlsch_encode(const SyndromeDlSchEncoder* encoder, const uint8_t* tb, size_t tb_len,
                               size_t rv, uint8_t* out, size_t out_len);
 
+/* ============================================ 5. transport-block serving ===== */
+/* A device-resident serving engine for DL-SCH transmissions.  No single counterpart
+ * in the reference: it replaces DlSchDecoder::decode (src/transport_block.rs:829)
+ * driven by LdpcPipeline (src/ldpc_pipeline.rs) with continuous batching on one GPU.
+ * Per transmission the results are those of DlSchDecoder::decode with the int8
+ * code-block decode: HARQ soft combining (src/harq.rs:142) in f32 accumulators that
+ * stay in device memory across retransmissions, quantize_llr_i16, decode_5g_i8,
+ * CRC-24B per code block, CRC-24A per transport block, accumulators flushed when
+ * both pass.  A worker thread forms GPU steps from the submission queue in arrival
+ * order while earlier steps run; a new transport block is admitted when its HARQ
+ * accumulators fit the HBM budget (otherwise it and the new blocks behind it wait;
+ * retransmissions of blocks that hold accumulators go ahead). */
+typedef struct SyndromeServer SyndromeServer;
+typedef struct {
+  uint32_t max_step_code_blocks; /* code blocks per GPU step, >= 160 (0 = 2048) */
+  uint32_t steps_in_flight;      /* 1..4 (0 = 2) */
+  uint64_t harq_bytes;           /* device memory for HARQ accumulators (0 = 2 GiB) */
+  uint64_t staging_bytes;        /* device staging for host-memory LLRs, per step (0 = 256 MiB) */
+  int32_t iterations;            /* maximum LOMS iterations (early stop on a zero syndrome) */
+  float offset_beta;             /* beta_q = round(offset_beta * scale) clamped to [0, 127] */
+  float scale;                   /* LLR quantizer scale (src/quantize.rs DEFAULT_SCALE = 8) */
+  int32_t app_clamp;             /* posterior clamp, >= 255 */
+} SyndromeServeConfig;
+typedef struct {
+  uint64_t tb_id;
+  int32_t crc_ok;                /* DecodeReport::crc_ok */
+  int32_t max_iters_used;        /* DecodeReport::max_iters_used */
+  int32_t harq_tx_count;         /* DecodeReport::harq_tx_count */
+  int32_t num_code_blocks;
+  uint32_t cb_crc[5];            /* DecodeReport::cb_crc: bit i = code block i passed */
+  uint32_t reserved;
+  double latency_us;             /* submit to completion */
+} SyndromeServeResult;
+int32_t syndrome_serve_create(const SyndromeServeConfig* config, SyndromeServer** out_server);
+void syndrome_serve_destroy(SyndromeServer* server);
+/* Queues one transmission of transport block tb_id (DlSchDecoder::new parameters
+ * tb_size, target_rate, qm, g plus the redundancy version rv): llr holds C * E f32
+ * channel LLRs (E = floor(g / C / qm) * qm), in device memory when llr_on_device,
+ * else host memory.  The buffer must stay valid until this transmission's result
+ * has been polled.  A new tb_id starts with empty accumulators; a tb_id whose last
+ * transmission failed keeps them (retransmission).  Reusing a tb_id with other
+ * parameters, or while one of its transmissions is in flight, is INVALID_PARAM. */
+int32_t syndrome_serve_submit(SyndromeServer* server, uint64_t tb_id, size_t tb_size, float target_rate,
+                              size_t qm, size_t g, size_t rv, const float* llr, size_t llr_len,
+                              int32_t llr_on_device);
+/* Up to cap completed transmissions, waiting up to timeout_us for the first. */
+int32_t syndrome_serve_poll(SyndromeServer* server, SyndromeServeResult* out, size_t cap, size_t* n_out,
+                            int64_t timeout_us);
+/* Payload of tb_id's last decode, one bit per byte (the tb_out of a passing decode). */
+int32_t syndrome_serve_fetch(SyndromeServer* server, uint64_t tb_id, uint8_t* tb_bits, size_t tb_len);
+/* Forgets tb_id and frees its accumulators (after success, or when giving up). */
+int32_t syndrome_serve_release(SyndromeServer* server, uint64_t tb_id);
+/* out8 = {steps, code blocks, transmissions, HARQ bytes in use, queued, steps in flight,
+ * transport blocks held, largest queue seen}. */
+int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out8);
+
 /* Text of the last error on this thread (empty if none). */
 const char* syndrome_last_error(void);
 

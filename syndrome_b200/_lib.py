@@ -75,6 +75,13 @@ PROTOTYPES = {
     "syndrome_dlsch_encoder_output_bits": (_sz, [_vp]),
     "syndrome_dlsch_encoder_num_code_blocks": (_sz, [_vp]),
     "syndrome_dlsch_encode": (_i32, [_vp, _vp, _sz, _sz, _vp, _sz]),
+    "syndrome_serve_create": (_i32, [_vp, ctypes.POINTER(_vp)]),
+    "syndrome_serve_destroy": (None, [_vp]),
+    "syndrome_serve_submit": (_i32, [_vp, ctypes.c_uint64, _sz, _f32, _sz, _sz, _sz, _vp, _sz, _i32]),
+    "syndrome_serve_poll": (_i32, [_vp, _vp, _sz, ctypes.POINTER(_sz), ctypes.c_int64]),
+    "syndrome_serve_fetch": (_i32, [_vp, ctypes.c_uint64, _vp, _sz]),
+    "syndrome_serve_release": (_i32, [_vp, ctypes.c_uint64]),
+    "syndrome_serve_stats": (_i32, [_vp, _vp]),
     "syndrome_last_error": (ctypes.c_char_p, []),
 }
 

@@ -20,6 +20,7 @@
 #include "encoder.h"
 #include "graph.h"
 #include "mixed.h"
+#include "serve.h"
 #include "tb.h"
 
 struct SyndromeLdpcDecoder {
@@ -40,6 +41,10 @@ struct SyndromeLdpcEncoder {
 
 struct SyndromeMixedPlan {
   syn::MixedPlan plan;
+};
+
+struct SyndromeServer {
+  syn::ServeEngine engine;
 };
 
 struct SyndromeDlSchEncoder {
@@ -714,6 +719,105 @@ int32_t syndrome_dlsch_encode(const SyndromeDlSchEncoder* e, const uint8_t* tb, 
     if (out_len < (size_t)e->enc.output_bits()) return fail(SYNDROME_BUFFER_TOO_SMALL, "output shorter than output_bits");
     if (rv > 3) return fail(SYNDROME_INVALID_PARAM, "RV must be 0..=3");
     e->enc.encode(tb, (int)rv, out);
+    return SYNDROME_OK;
+  });
+}
+
+// ----------------------------------------------------------------- serving ---
+
+int32_t syndrome_serve_create(const SyndromeServeConfig* config, SyndromeServer** out) {
+  return guard([&]() -> int32_t {
+    if (!out) return SYNDROME_NULL_POINTER;
+    *out = nullptr;
+    syn::ServeConfig c;
+    if (config) {
+      if (config->max_step_code_blocks) c.max_step_cbs = (int)std::min<uint32_t>(config->max_step_code_blocks, 65535);
+      if (config->steps_in_flight) c.slots = (int)std::min<uint32_t>(config->steps_in_flight, 4);
+      if (config->harq_bytes) c.harq_bytes = (long long)config->harq_bytes;
+      if (config->staging_bytes) c.staging_bytes = (long long)config->staging_bytes;
+      c.iterations = config->iterations;
+      c.beta = config->offset_beta;
+      c.scale = config->scale;
+      c.app_clamp = config->app_clamp;
+    }
+    auto* s = new SyndromeServer();
+    std::string err;
+    if (!s->engine.init(c, &err)) {
+      delete s;
+      cudaGetLastError();
+      return fail(err.find("alloc") != std::string::npos || err.find("CUDA") != std::string::npos
+                      ? SYNDROME_CUDA_ERROR
+                      : SYNDROME_INVALID_PARAM,
+                  err);
+    }
+    *out = s;
+    return SYNDROME_OK;
+  });
+}
+
+void syndrome_serve_destroy(SyndromeServer* server) { delete server; }
+
+int32_t syndrome_serve_submit(SyndromeServer* server, uint64_t tb_id, size_t tb_size, float target_rate, size_t qm,
+                              size_t g, size_t rv, const float* llr, size_t llr_len, int32_t llr_on_device) {
+  return guard([&]() -> int32_t {
+    if (!server || !llr) return SYNDROME_NULL_POINTER;
+    if (tb_size > (size_t)syn::kMaxTbBits * 2 || qm > 64 || g > ((size_t)1 << 40) || rv > 3 ||
+        llr_len > ((size_t)1 << 40))
+      return fail(SYNDROME_INVALID_PARAM, "argument out of range");
+    std::string err;
+    const int r = server->engine.submit(tb_id, (long long)tb_size, target_rate, (int)qm, (long long)g, (int)rv, llr,
+                                        (long long)llr_len, llr_on_device != 0, &err);
+    return r == SYNDROME_OK ? SYNDROME_OK : fail(r, err);
+  });
+}
+
+int32_t syndrome_serve_poll(SyndromeServer* server, SyndromeServeResult* out, size_t cap, size_t* n_out,
+                            int64_t timeout_us) {
+  return guard([&]() -> int32_t {
+    if (!server || !n_out || (!out && cap)) return SYNDROME_NULL_POINTER;
+    std::vector<syn::ServeResult> buf(std::min<size_t>(cap, 4096));
+    const int n = server->engine.poll(buf.data(), (int)buf.size(), timeout_us);
+    for (int i = 0; i < n; ++i) {
+      SyndromeServeResult& r = out[i];
+      std::memset(&r, 0, sizeof(r));
+      r.tb_id = buf[i].id;
+      r.crc_ok = buf[i].crc_ok;
+      r.max_iters_used = buf[i].max_iters;
+      r.harq_tx_count = buf[i].harq_tx;
+      r.num_code_blocks = buf[i].n_cb;
+      for (int w = 0; w < 5; ++w) r.cb_crc[w] = buf[i].cb_crc[w];
+      r.latency_us = buf[i].latency_us;
+    }
+    *n_out = (size_t)n;
+    return SYNDROME_OK;
+  });
+}
+
+int32_t syndrome_serve_fetch(SyndromeServer* server, uint64_t tb_id, uint8_t* tb_bits, size_t tb_len) {
+  return guard([&]() -> int32_t {
+    if (!server || !tb_bits) return SYNDROME_NULL_POINTER;
+    std::string err;
+    const int r = server->engine.fetch(tb_id, tb_bits, (long long)std::min<size_t>(tb_len, (size_t)1 << 40), &err);
+    return r == SYNDROME_OK ? SYNDROME_OK : fail(r, err);
+  });
+}
+
+int32_t syndrome_serve_release(SyndromeServer* server, uint64_t tb_id) {
+  return guard([&]() -> int32_t {
+    if (!server) return SYNDROME_NULL_POINTER;
+    std::string err;
+    const int r = server->engine.release(tb_id, &err);
+    return r == SYNDROME_OK ? SYNDROME_OK : fail(r, err);
+  });
+}
+
+int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out8) {
+  return guard([&]() -> int32_t {
+    if (!server || !out8) return SYNDROME_NULL_POINTER;
+    const syn::ServeStats s = server->engine.stats();
+    const int64_t v[8] = {s.steps, s.code_blocks, s.transmissions, s.harq_bytes_used, s.pending, s.in_flight,
+                          s.tbs_held, s.max_pending};
+    for (int i = 0; i < 8; ++i) out8[i] = v[i];
     return SYNDROME_OK;
   });
 }

@@ -1,0 +1,143 @@
+// Transport-block serving engine: continuous batching of 5G NR DL-SCH
+// transmissions on one GPU (serve.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "nr_kernels.h"
+#include "serve_kernels.h"
+#include "tb.h"
+
+namespace syn {
+
+struct ServeConfig {
+  int max_step_cbs = 2048;               // code blocks per GPU step (at least one whole TB)
+  int slots = 2;                         // steps in flight
+  long long harq_bytes = 2LL << 30;      // device memory for HARQ accumulators
+  long long staging_bytes = 256LL << 20; // device staging of host-memory LLRs, per step
+  int iterations = 8;
+  float beta = 0.5f;
+  float scale = 8.0f;
+  int app_clamp = 32767;
+};
+
+struct ServeResult {
+  uint64_t id = 0;
+  int crc_ok = 0;
+  int max_iters = 0;
+  int harq_tx = 0;
+  int n_cb = 0;
+  uint32_t cb_crc[5] = {0, 0, 0, 0, 0};
+  double latency_us = 0.0;  // submit to completion
+};
+
+struct ServeStats {
+  long long steps = 0, code_blocks = 0, transmissions = 0, harq_bytes_used = 0, pending = 0, in_flight = 0;
+  long long tbs_held = 0, max_pending = 0;
+};
+
+class ServeEngine {
+ public:
+  ~ServeEngine();
+  bool init(const ServeConfig& cfg, std::string* err);
+  // Queues one transmission (redundancy version rv) of transport block id.  llr holds
+  // C * E f32 channel LLRs (host memory unless on_device); it must stay valid until
+  // the transmission's result has been polled.  Returns a SyndromeStatus code.
+  int submit(uint64_t id, long long tb_size, float rate, int qm, long long g, int rv, const float* llr,
+             long long llr_len, bool on_device, std::string* err);
+  // Completed transmissions in completion order; waits up to timeout_us for the first.
+  int poll(ServeResult* out, int cap, long long timeout_us);
+  // Payload bits of the last decode of id (valid when its result had crc_ok).
+  int fetch(uint64_t id, uint8_t* bits, long long len, std::string* err);
+  // Drops the state of id (HARQ accumulators included).  Not while a transmission is in flight.
+  int release(uint64_t id, std::string* err);
+  ServeStats stats();
+
+ private:
+  struct Tb {
+    TbParams p;
+    long long tb_size = 0, g = 0, e = 0;
+    float rate = 0.0f;
+    int qm = 1;
+    long long harq_off = -1;  // bytes into the HARQ arena, -1 = none
+    int tx_count = 0;
+    bool busy = false;
+    std::vector<uint32_t> bits;  // last decode's payload, LSB-first words
+  };
+  struct Pending {
+    uint64_t id;
+    int rv;
+    const float* llr;
+    bool on_device;
+    std::chrono::steady_clock::time_point t0;
+  };
+  struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    bool busy = false;
+    // device
+    int8_t* d_llr = nullptr;
+    uint32_t* d_hard = nullptr;
+    int32_t* d_iters = nullptr;
+    ServeCb* d_cbs = nullptr;
+    ServeCbCrc* d_crc = nullptr;
+    ServeTb* d_tbs = nullptr;
+    int32_t* d_res = nullptr;
+    uint32_t* d_bits = nullptr;
+    MixItem* d_items = nullptr;
+    MixCodeword* d_cws = nullptr;
+    unsigned* d_queue = nullptr;
+    float* d_stage = nullptr;
+    // pinned host
+    ServeCb* h_cbs = nullptr;
+    ServeTb* h_tbs = nullptr;
+    MixItem* h_items = nullptr;
+    MixCodeword* h_cws = nullptr;
+    int32_t* h_res = nullptr;
+    uint32_t* h_bits = nullptr;
+    // step contents
+    std::vector<Pending> txs;
+    std::vector<long long> bits_off;
+    int n_cbs = 0;
+  };
+
+  void worker();
+  bool launch_step(Slot& s);
+  void finish_step(Slot& s);
+  long long harq_alloc(long long bytes);
+  void harq_free(long long off);
+
+  ServeConfig cfg_;
+  int device_ = 0, sms_ = 0, max_words_ = 0, max_tb_words_ = 0, beta_q_ = 0;
+  char* d_harq_ = nullptr;
+  short* d_shift_ = nullptr;
+  int* d_colz_ = nullptr;
+  std::map<long long, long long> free_;       // HARQ arena free list: offset -> bytes
+  std::unordered_map<long long, long long> used_;
+  long long harq_used_ = 0;
+  std::vector<Slot> slots_;
+  std::deque<int> order_;                    // busy slots in launch order (worker thread only)
+  int inflight_ = 0;                         // order_.size(), readable under mu_
+  std::mutex mu_;
+  std::condition_variable cv_work_, cv_done_;
+  std::unordered_map<uint64_t, Tb> tbs_;
+  std::deque<Pending> pending_;
+  std::deque<ServeResult> done_;
+  ServeStats stats_;
+  bool stop_ = false;
+  std::thread thread_;
+  std::string fatal_;
+};
+
+}  // namespace syn

@@ -1,0 +1,113 @@
+"""Transport-block serving on the GPU: continuous batching of DL-SCH transmissions with
+device-resident HARQ accumulators (include/syndrome_ldpc.h section 5).
+
+Per transmission the results are those of syndrome's DlSchDecoder::decode
+(src/transport_block.rs:829) with the int8 code-block decode; the engine replaces the
+reference's LdpcPipeline worker threads (src/ldpc_pipeline.rs) with one GPU work queue
+fed by a worker thread that batches whatever has arrived."""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("max_step_code_blocks", ctypes.c_uint32), ("steps_in_flight", ctypes.c_uint32),
+                ("harq_bytes", ctypes.c_uint64), ("staging_bytes", ctypes.c_uint64), ("iterations", ctypes.c_int32),
+                ("offset_beta", ctypes.c_float), ("scale", ctypes.c_float), ("app_clamp", ctypes.c_int32)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("tb_id", ctypes.c_uint64), ("crc_ok", ctypes.c_int32), ("max_iters_used", ctypes.c_int32),
+                ("harq_tx_count", ctypes.c_int32), ("num_code_blocks", ctypes.c_int32),
+                ("cb_crc", ctypes.c_uint32 * 5), ("reserved", ctypes.c_uint32), ("latency_us", ctypes.c_double)]
+
+
+class Server:
+    """A serving engine on the current CUDA device.  Zero-valued sizes take the
+    library defaults (2048 code blocks per step, 2 steps in flight, 2 GiB of HARQ
+    accumulators, 256 MiB of staging for host-memory LLRs)."""
+
+    def __init__(self, max_step_code_blocks=0, steps_in_flight=0, harq_bytes=0, staging_bytes=0, iterations=8,
+                 offset_beta=0.5, scale=8.0, app_clamp=32767):
+        cfg = _Config(max_step_code_blocks, steps_in_flight, harq_bytes, staging_bytes, iterations, offset_beta,
+                      scale, app_clamp)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().syndrome_serve_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h.value
+        self._keep = {}
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            _lib.load().syndrome_serve_destroy(h)
+        self._keep = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, tb_id, tb_size, target_rate, qm, g, rv, llr):
+        """Queues one transmission.  llr: C * E f32 LLRs as a numpy array (host) or a
+        CUDA tensor; it is kept alive until the transmission's result is polled."""
+        try:
+            import torch
+            on_dev = isinstance(llr, torch.Tensor) and llr.is_cuda
+        except ImportError:
+            on_dev = False
+        if on_dev:
+            if llr.dtype != torch.float32 or not llr.is_contiguous():
+                raise TypeError("llr must be a contiguous float32 tensor")
+            ptr, n = llr.data_ptr(), llr.numel()
+        else:
+            llr = np.ascontiguousarray(llr, dtype=np.float32)
+            ptr, n = llr.ctypes.data, llr.size
+        _lib.check(_lib.load().syndrome_serve_submit(self._h, tb_id, tb_size, target_rate, qm, g, rv,
+                                                     ctypes.c_void_p(ptr), n, int(on_dev)))
+        self._keep.setdefault(tb_id, []).append(llr)
+
+    def poll(self, timeout_us=0, cap=1024):
+        """Completed transmissions: dicts with the DecodeReport fields and latency_us."""
+        buf = (_Result * cap)()
+        n = ctypes.c_size_t(0)
+        _lib.check(_lib.load().syndrome_serve_poll(self._h, buf, cap, ctypes.byref(n), int(timeout_us)))
+        out = []
+        for r in buf[: n.value]:
+            keep = self._keep.get(r.tb_id)
+            if keep:
+                keep.pop(0)
+                if not keep:
+                    del self._keep[r.tb_id]
+            cb = [bool((r.cb_crc[i // 32] >> (i % 32)) & 1) for i in range(r.num_code_blocks)]
+            out.append(dict(tb_id=r.tb_id, crc_ok=bool(r.crc_ok), max_iters_used=r.max_iters_used,
+                            harq_tx_count=r.harq_tx_count, cb_crc=cb, latency_us=r.latency_us))
+        return out
+
+    def wait(self, count, timeout_s=60.0):
+        """Polls until `count` results arrived (raises TimeoutError otherwise)."""
+        import time
+
+        out, t_end = [], time.time() + timeout_s
+        while len(out) < count:
+            if time.time() > t_end:
+                raise TimeoutError(f"{len(out)} of {count} results after {timeout_s} s")
+            out += self.poll(timeout_us=20000)
+        return out
+
+    def fetch(self, tb_id, tb_size):
+        bits = np.zeros(tb_size, dtype=np.uint8)
+        _lib.check(_lib.load().syndrome_serve_fetch(self._h, tb_id, bits.ctypes.data, tb_size))
+        return bits
+
+    def release(self, tb_id):
+        _lib.check(_lib.load().syndrome_serve_release(self._h, tb_id))
+
+    def stats(self):
+        v = np.zeros(8, dtype=np.int64)
+        _lib.check(_lib.load().syndrome_serve_stats(self._h, v.ctypes.data))
+        keys = ("steps", "code_blocks", "transmissions", "harq_bytes_used", "pending", "in_flight", "tbs_held",
+                "max_pending")
+        return dict(zip(keys, (int(x) for x in v)))

@@ -93,3 +93,38 @@ def test_tb_encoder_errors():
     with pytest.raises(S.SyndromeError) as e:
         enc.encode(np.zeros(100, np.uint8), 4)
     assert e.value.status == _lib.INVALID_PARAM
+
+
+def _llr(bits, ebno, rate, seed):
+    return S.AwgnChannel(ebno, rate, seed).transmit(bits)
+
+
+def test_oracle_chain_decodes_the_encoder_output():
+    """transport_block.rs encoder_decoder_noiseless_roundtrip and
+    harq_combining_recovers_a_block_that_fails_alone, on the oracle chain fed by this
+    library's encoder (the oracle decoder is what the GPU engine is checked against)."""
+    rng = np.random.default_rng(11)
+    for a, rate, qm, g in ((100, 0.5, 1, 248), (8425, 0.5, 2, 17000), (30000, 0.8, 4, 37500)):
+        tb = rng.integers(0, 2, a, dtype=np.uint8)
+        enc = S.DlSchEncoder(a, rate, qm, g)
+        bits = enc.encode(tb, 0)
+        dec = O.DlSchDecoder(a, rate, qm, g, iterations=8)
+        noiseless = np.where(bits == 0, 4.0, -4.0).astype(np.float32)
+        r = dec.decode(noiseless, 0)
+        assert r["crc_ok"] and np.array_equal(r["tb"], tb) and r["harq_tx"] == 1 and all(r["cb_crc"])
+    # a block that fails alone is recovered by combining a second redundancy version
+    a, rate, qm, g = 3000, 0.85, 1, 3530
+    tb = rng.integers(0, 2, a, dtype=np.uint8)
+    enc = S.DlSchEncoder(a, rate, qm, g)
+    for seed in range(20):
+        dec = O.DlSchDecoder(a, rate, qm, g, iterations=8)
+        first = dec.decode(_llr(enc.encode(tb, 0), 1.0, rate, seed), 0)
+        if first["crc_ok"]:
+            continue
+        second = dec.decode(_llr(enc.encode(tb, 2), 1.0, rate, 1000 + seed), 2)
+        assert second["harq_tx"] == 2
+        if second["crc_ok"]:
+            assert np.array_equal(second["tb"], tb)
+            break
+    else:
+        pytest.fail("no seed showed HARQ combining recovering a failed block")
