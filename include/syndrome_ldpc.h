@@ -348,6 +348,35 @@ int32_t syndrome_serve_release(SyndromeServer* server, uint64_t tb_id);
  * transport blocks held, largest queue seen}. */
 int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out8);
 
+/* Open-loop load test of a server (the serving benchmark; no counterpart in the
+ * reference).  Transport blocks arrive as a Poisson process of offered_tb_per_s for
+ * duration_s; arrival i is pool entry i % pool_n, whose llr[rv index] are device
+ * pointers to the C * E LLRs of its transmissions with redundancy versions 0, 2, 3, 1.
+ * A failed transmission is retransmitted at once with the next version, up to
+ * max_transmissions.  A block's latency runs from its scheduled arrival to the result
+ * of its last transmission; latencies_us (nullable) receives them in arrival order. */
+typedef struct {
+  size_t tb_size;
+  float target_rate;
+  size_t qm;
+  size_t g;
+  const float* llr[4];
+  size_t llr_len;
+} SyndromeLoadTb;
+typedef struct {
+  double offered_tb_per_s;
+  double duration_s;
+  uint32_t max_transmissions;
+  uint64_t seed;
+} SyndromeLoadSpec;
+typedef struct {
+  uint64_t tbs, tbs_ok, transmissions;
+  double wall_s, info_bits_ok, p50_us, p99_us, mean_us, max_us;
+} SyndromeLoadReport;
+int32_t syndrome_serve_run_load(SyndromeServer* server, const SyndromeLoadTb* pool, size_t pool_n,
+                                const SyndromeLoadSpec* spec, SyndromeLoadReport* report,
+                                double* latencies_us, size_t latencies_cap);
+
 /* Text of the last error on this thread (empty if none). */
 const char* syndrome_last_error(void);
 

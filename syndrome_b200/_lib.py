@@ -82,6 +82,7 @@ PROTOTYPES = {
     "syndrome_serve_fetch": (_i32, [_vp, ctypes.c_uint64, _vp, _sz]),
     "syndrome_serve_release": (_i32, [_vp, ctypes.c_uint64]),
     "syndrome_serve_stats": (_i32, [_vp, _vp]),
+    "syndrome_serve_run_load": (_i32, [_vp, _vp, _sz, _vp, _vp, _vp, _sz]),
     "syndrome_last_error": (ctypes.c_char_p, []),
 }
 

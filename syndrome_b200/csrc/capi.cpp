@@ -822,4 +822,20 @@ int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out8) {
   });
 }
 
+int32_t syndrome_serve_run_load(SyndromeServer* server, const SyndromeLoadTb* pool, size_t pool_n,
+                                const SyndromeLoadSpec* spec, SyndromeLoadReport* report, double* latencies_us,
+                                size_t latencies_cap) {
+  return guard([&]() -> int32_t {
+    if (!server || !pool || !spec || !report) return SYNDROME_NULL_POINTER;
+    if (pool_n == 0 || !(spec->offered_tb_per_s > 0.0) || !(spec->duration_s >= 0.0) || spec->duration_s > 3600.0)
+      return fail(SYNDROME_INVALID_PARAM, "empty pool or bad rate / duration");
+    for (size_t i = 0; i < pool_n; ++i)
+      for (int k = 0; k < 4; ++k)
+        if (!pool[i].llr[k]) return fail(SYNDROME_NULL_POINTER, "pool LLR pointer is null");
+    std::string err;
+    const int r = syn::run_load(server->engine, pool, pool_n, *spec, report, latencies_us, latencies_cap, &err);
+    return r == SYNDROME_OK ? SYNDROME_OK : fail(r, err);
+  });
+}
+
 }  // extern "C"

@@ -15,6 +15,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "../../include/syndrome_ldpc.h"
 #include "nr_kernels.h"
 #include "serve_kernels.h"
 #include "tb.h"
@@ -139,5 +140,9 @@ class ServeEngine {
   std::thread thread_;
   std::string fatal_;
 };
+
+// Open-loop Poisson load against an engine (serve_load.cpp, syndrome_serve_run_load).
+int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const SyndromeLoadSpec& spec,
+             SyndromeLoadReport* rep, double* lat_out, size_t lat_cap, std::string* err);
 
 }  // namespace syn

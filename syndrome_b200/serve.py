@@ -24,6 +24,22 @@ class _Result(ctypes.Structure):
                 ("cb_crc", ctypes.c_uint32 * 5), ("reserved", ctypes.c_uint32), ("latency_us", ctypes.c_double)]
 
 
+class _LoadTb(ctypes.Structure):
+    _fields_ = [("tb_size", ctypes.c_size_t), ("target_rate", ctypes.c_float), ("qm", ctypes.c_size_t),
+                ("g", ctypes.c_size_t), ("llr", ctypes.c_void_p * 4), ("llr_len", ctypes.c_size_t)]
+
+
+class _LoadSpec(ctypes.Structure):
+    _fields_ = [("offered_tb_per_s", ctypes.c_double), ("duration_s", ctypes.c_double),
+                ("max_transmissions", ctypes.c_uint32), ("seed", ctypes.c_uint64)]
+
+
+class _LoadReport(ctypes.Structure):
+    _fields_ = [("tbs", ctypes.c_uint64), ("tbs_ok", ctypes.c_uint64), ("transmissions", ctypes.c_uint64),
+                ("wall_s", ctypes.c_double), ("info_bits_ok", ctypes.c_double), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double)]
+
+
 class Server:
     """A serving engine on the current CUDA device.  Zero-valued sizes take the
     library defaults (2048 code blocks per step, 2 steps in flight, 2 GiB of HARQ
@@ -111,3 +127,29 @@ class Server:
         keys = ("steps", "code_blocks", "transmissions", "harq_bytes_used", "pending", "in_flight", "tbs_held",
                 "max_pending")
         return dict(zip(keys, (int(x) for x in v)))
+
+    def run_load(self, pool, offered_tb_per_s, duration_s, max_transmissions=4, seed=0, latencies=False):
+        """Open-loop Poisson load (syndrome_serve_run_load).  pool: list of dicts with
+        tb_size, target_rate, qm, g and llrs = four contiguous float32 CUDA tensors (the
+        transmissions with RV 0, 2, 3, 1).  Returns the report as a dict (plus the
+        per-block latencies in arrival order when latencies=True)."""
+        arr = (_LoadTb * len(pool))()
+        for i, p in enumerate(pool):
+            arr[i].tb_size, arr[i].target_rate, arr[i].qm, arr[i].g = p["tb_size"], p["target_rate"], p["qm"], p["g"]
+            for k in range(4):
+                t = p["llrs"][k]
+                if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
+                    raise TypeError("pool LLRs must be contiguous float32 CUDA tensors")
+                arr[i].llr[k] = t.data_ptr()
+            arr[i].llr_len = p["llrs"][0].numel()
+        spec = _LoadSpec(offered_tb_per_s, duration_s, max_transmissions, seed)
+        rep = _LoadReport()
+        cap = int(offered_tb_per_s * duration_s * 2 + 1024) if latencies else 0
+        lat = np.zeros(cap, dtype=np.float64)
+        _lib.check(_lib.load().syndrome_serve_run_load(self._h, arr, len(pool), ctypes.byref(spec), ctypes.byref(rep),
+                                                       lat.ctypes.data if cap else None, cap))
+        out = {k: getattr(rep, k) for k, _ in _LoadReport._fields_}
+        if latencies:
+            out["latencies_us"] = lat[: rep.tbs]
+        return out
+

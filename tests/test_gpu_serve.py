@@ -157,3 +157,19 @@ def test_serve_errors():
         s.submit(11, a, r, qm, g, 4, llrs[0])
     s.release(9)
     s.close()
+
+
+def test_serve_open_loop_load():
+    """Poisson arrivals over a small pool with retransmissions: every arrival completes,
+    latencies are positive and ordered percentiles come back."""
+    pool = []
+    for i, (a, r, qm, g, eb) in enumerate(CASES[:5]):
+        tb, llrs = make_tb(a, r, qm, g, eb + 1.0, 500 + i)
+        pool.append(dict(tb_size=a, target_rate=r, qm=qm, g=g, llrs=[torch.from_numpy(x).cuda() for x in llrs]))
+    s = S.Server(max_step_code_blocks=256)
+    rep = s.run_load(pool, offered_tb_per_s=2000.0, duration_s=0.25, seed=3, latencies=True)
+    assert rep["tbs"] > 100 and rep["transmissions"] >= rep["tbs"]
+    lat = rep["latencies_us"]
+    assert (lat > 0).all() and 0 < rep["p50_us"] <= rep["p99_us"] <= rep["max_us"]
+    assert s.stats()["tbs_held"] == 0 and s.stats()["harq_bytes_used"] == 0
+    s.close()
