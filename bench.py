@@ -57,7 +57,12 @@ def parse_args():
     p.add_argument("--chunks", type=int, default=8, help="e2e copy/compute pipeline depth")
     p.add_argument("--cpu-seconds", type=float, default=8.0, help="target CPU work of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--kernel", choices=["auto", "generic", "nr"], default="auto")
+    p.add_argument("--kernel", choices=["auto", "generic", "nr", "pair"], default="auto")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
+    p.add_argument("--serve-pool", type=int, default=48)
+    p.add_argument("--serve-seconds", type=float, default=1.0)
+    p.add_argument("--serve-step-cbs", type=int, default=1024)
+    p.add_argument("--serve-loads", type=float, nargs="+", default=[0.25, 0.5, 1.0])
     return p.parse_args()
 
 
@@ -213,6 +218,63 @@ def run_reference(args):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+SERVE_WORKLOAD = ("5G NR DL-SCH serving: Poisson arrivals of transport blocks, size log-uniform in [1000, 1.2M] "
+                  "bits, target rate uniform in [1/5, 8/9], BPSK (Qm 1), G = ceil(A / R), Eb/N0 uniform in "
+                  "[-1, 3] dB; CRC-24A, segmentation with CRC-24B, RV 0/2/3/1 with HARQ soft combining in device "
+                  "memory, int8 LOMS <= 8 iterations")
+
+
+def make_serving_pool(count, seed, dev):
+    """Transport blocks of the serving workload with the f32 LLRs of their four
+    transmissions (RV 0, 2, 3, 1) on the device; this library's DL-SCH encoder and
+    the reference channel."""
+    import torch
+
+    import syndrome_b200 as S
+
+    rng = np.random.default_rng(seed)
+    pool = []
+    for i in range(count):
+        a = int(np.exp(rng.uniform(np.log(1000.0), np.log(1.2e6))))
+        r = float(rng.uniform(0.2, 8.0 / 9.0))
+        g = int(np.ceil(a / r))
+        eb = float(rng.uniform(-1.0, 3.0))
+        tb = rng.integers(0, 2, a, dtype=np.uint8)
+        enc = S.DlSchEncoder(a, r, 1, g)
+        llrs = [torch.from_numpy(S.AwgnChannel(eb, r, seed * 100003 + i * 4 + k).transmit(enc.encode(tb, rv))).to(dev)
+                for k, rv in enumerate((0, 2, 3, 1))]
+        pool.append(dict(tb_size=a, target_rate=r, qm=1, g=g, llrs=llrs, ebno=eb))
+    return pool
+
+
+def serve_section(batch_gbps, dev, args):
+    """Open-loop serving at fractions of the measured batch throughput."""
+    import syndrome_b200 as S
+
+    pool = make_serving_pool(args.serve_pool, 0x5E4E, dev)
+    mean_bits = float(np.mean([p["tb_size"] for p in pool]))
+    server = S.Server(max_step_code_blocks=args.serve_step_cbs, iterations=ITERS, offset_beta=BETA, scale=SCALE)
+    server.run_load(pool, offered_tb_per_s=200.0, duration_s=0.05, seed=1)  # warm-up
+    points = []
+    for frac in args.serve_loads:
+        lam = frac * batch_gbps * 1e9 / mean_bits
+        rep = server.run_load(pool, offered_tb_per_s=lam, duration_s=args.serve_seconds, seed=int(frac * 1000))
+        points.append({"offered_frac_of_batch": frac, "offered_tb_per_s": lam, "tbs": rep["tbs"],
+                       "tb_ok_frac": rep["tbs_ok"] / max(rep["tbs"], 1),
+                       "transmissions_per_tb": rep["transmissions"] / max(rep["tbs"], 1),
+                       "p50_us": rep["p50_us"], "p99_us": rep["p99_us"], "mean_us": rep["mean_us"],
+                       "max_us": rep["max_us"], "wall_s": rep["wall_s"],
+                       "decoded_gbps": rep["info_bits_decoded"] / rep["wall_s"] / 1e9,
+                       "goodput_gbps": rep["info_bits_ok"] / rep["wall_s"] / 1e9})
+    st = server.stats()
+    server.close()
+    best = max(p["decoded_gbps"] for p in points)
+    return {"workload": SERVE_WORKLOAD, "pool_tbs": len(pool), "mean_tb_bits": mean_bits,
+            "step_code_blocks": args.serve_step_cbs, "points": points,
+            "max_decoded_gbps": best, "max_decoded_vs_batch": best / batch_gbps,
+            "steps": st["steps"], "mean_code_blocks_per_step": st["code_blocks"] / max(st["steps"], 1)}
 
 
 def main():
@@ -371,6 +433,8 @@ def main():
         line["clocks"] = clk
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(llr_h, args.cpu_seconds)
+    if rank == 0 and world == 1 and not args.no_serve:
+        line["serve"] = serve_section(value, dev, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -371,7 +371,10 @@ typedef struct {
 } SyndromeLoadSpec;
 typedef struct {
   uint64_t tbs, tbs_ok, transmissions;
-  double wall_s, info_bits_ok, p50_us, p99_us, mean_us, max_us;
+  double wall_s;
+  double info_bits_ok;       /* payload bits of the blocks whose CRCs passed */
+  double info_bits_decoded;  /* payload bits over all transmissions (decode work done) */
+  double p50_us, p99_us, mean_us, max_us;
 } SyndromeLoadReport;
 int32_t syndrome_serve_run_load(SyndromeServer* server, const SyndromeLoadTb* pool, size_t pool_n,
                                 const SyndromeLoadSpec* spec, SyndromeLoadReport* report,

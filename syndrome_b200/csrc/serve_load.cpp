@@ -35,7 +35,7 @@ int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const 
   std::vector<ServeResult> res(1024);
   size_t next = 0, finished = 0;
   long long transmissions = 0;
-  double info_ok = 0.0;
+  double info_ok = 0.0, info_decoded = 0.0;
   const auto t0 = clock::now();
   auto now_s = [&] { return std::chrono::duration<double>(clock::now() - t0).count(); };
   auto send = [&](size_t i) -> int {
@@ -50,6 +50,7 @@ int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const 
     }
     tx[i] = k + 1;
     ++transmissions;
+    info_decoded += (double)p.tb_size;
     return SYNDROME_OK;
   };
   while (finished < n) {
@@ -92,6 +93,7 @@ int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const 
   rep->transmissions = (uint64_t)transmissions;
   rep->wall_s = wall;
   rep->info_bits_ok = info_ok;
+  rep->info_bits_decoded = info_decoded;
   rep->p50_us = pct(0.50);
   rep->p99_us = pct(0.99);
   rep->mean_us = n ? mean / (double)n : 0.0;

@@ -36,7 +36,8 @@ class _LoadSpec(ctypes.Structure):
 
 class _LoadReport(ctypes.Structure):
     _fields_ = [("tbs", ctypes.c_uint64), ("tbs_ok", ctypes.c_uint64), ("transmissions", ctypes.c_uint64),
-                ("wall_s", ctypes.c_double), ("info_bits_ok", ctypes.c_double), ("p50_us", ctypes.c_double),
+                ("wall_s", ctypes.c_double), ("info_bits_ok", ctypes.c_double),
+                ("info_bits_decoded", ctypes.c_double), ("p50_us", ctypes.c_double),
                 ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double)]
 
 
