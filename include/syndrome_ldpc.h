@@ -254,7 +254,8 @@ void syndrome_mixed_plan_destroy(SyndromeMixedPlan* plan);
 /* Number of work items; out_items (nullable, room for `cap` items) receives
  * (base_graph, z, codewords) per item in launch order. */
 int32_t syndrome_mixed_plan_items(const SyndromeMixedPlan* plan, int32_t* out_items, size_t cap, size_t* n_items);
-/* Most codewords one work item of this shape can hold. */
+/* Most codewords one work item of this shape can hold with the default app_clamp
+ * (paired kernel; plans with app_clamp below 7874 use smaller items). */
 int32_t syndrome_mixed_tile_capacity(int32_t base_graph, int32_t z);
 /* Decodes the planned batch from device LLRs (llr_bytes long) into d_hard_packed
  * (out_words long); d_iters (nullable, iters_len entries) receives the iterations of

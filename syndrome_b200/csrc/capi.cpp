@@ -642,7 +642,7 @@ int32_t syndrome_mixed_plan_items(const SyndromeMixedPlan* plan, int32_t* out_it
 
 int32_t syndrome_mixed_tile_capacity(int32_t base_graph, int32_t z) {
   if ((base_graph != 0 && base_graph != 1) || syn::lifting_set_index(z) < 0) return 0;
-  return syn::mixed_slot_capacity(base_graph, z);
+  return syn::pair_mixed_capacity(base_graph, z);
 }
 
 int32_t syndrome_mixed_decode(SyndromeMixedPlan* plan, const int8_t* d_llr, size_t llr_bytes,

@@ -2,10 +2,12 @@
 //
 // A plan is built once per batch layout (the list of codewords with their base
 // graph, lifting size, filler count, input and output offsets).  It groups codewords
-// of equal shape into work items of `tile` codewords (default: as many as one
-// 768-thread CTA holds; a tuner may choose smaller tiles per shape), orders items by
+// of equal shape into work items of `tile` codewords (default: as many as one CTA
+// holds; a tuner may choose smaller tiles per shape), orders items by
 // decreasing work so the longest start first, and uploads the items, the per-codeword
-// records and the shift / column-base tables of every (BG, Z) used.  decode() zeroes
+// records and the shift / column-base tables of every (BG, Z) used.  With app_clamp
+// >= 7874 the items go to the paired kernel (two codewords per 32-bit word,
+// nr_pair_kernels.cu), otherwise to the one-codeword-per-thread kernel (nr_kernels.cu).  decode() zeroes
 // the device work counter and launches one CTA per SM; with use_graph the two
 // operations are captured once into a CUDA graph and replayed.
 #include "mixed.h"
@@ -75,12 +77,14 @@ bool MixedPlan::init(const std::vector<MixedCodeword>& cws, int beta_q, int app_
     need_out = std::max(need_out, c.out_offset + (c.hard_bits + 31) / 32);
     groups[{c.bg, c.z}].push_back((int)i);
   }
+  // two codewords per 32-bit word when no non-filler posterior can reach the clamp
+  const bool paired = app_clamp >= 7874;
   std::vector<MixItem> items;
   std::vector<MixCodeword> recs;
   recs.reserve(cws.size());
   for (auto& kv : groups) {
     const int bg = kv.first.first, z = kv.first.second;
-    const int cap = mixed_slot_capacity(bg, z);
+    const int cap = paired ? pair_mixed_capacity(bg, z) : mixed_slot_capacity(bg, z);
     int tile = cap;
     auto it = tile_of.find(kv.first);
     if (it != tile_of.end()) tile = std::max(1, std::min(cap, it->second));
@@ -131,7 +135,9 @@ bool MixedPlan::init(const std::vector<MixedCodeword>& cws, int beta_q, int app_
   iterations_ = iterations;
   if (cudaGetDevice(&device_) != cudaSuccess) return fail("no CUDA device");
   cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
-  if (mixed_kernel_prepare() != cudaSuccess) return fail("cannot configure the mixed-batch kernel");
+  paired_ = paired;
+  if ((paired ? pair_mixed_prepare() : mixed_kernel_prepare()) != cudaSuccess)
+    return fail("cannot configure the mixed-batch kernel");
   if (cudaMalloc(&d_items_, sizeof(MixItem) * std::max<size_t>(items.size(), 1)) != cudaSuccess ||
       cudaMalloc(&d_cws_, sizeof(MixCodeword) * std::max<size_t>(recs.size(), 1)) != cudaSuccess ||
       cudaMalloc(&d_queue_, sizeof(unsigned)) != cudaSuccess ||
@@ -172,7 +178,8 @@ cudaError_t MixedPlan::decode(const int8_t* d_llr, uint32_t* d_out, int32_t* d_i
                               cudaStream_t stream) {
   if (n_items_ == 0) return cudaSuccess;
   const MixArgs m = args(d_llr, d_out, d_iters);
-  if (!use_graph) return mixed_decode_launch(m, sms_, stream);
+  auto launch = [&](cudaStream_t st) { return paired_ ? pair_mixed_launch(m, sms_, st) : mixed_decode_launch(m, sms_, st); };
+  if (!use_graph) return launch(stream);
   if (!exec_ || g_llr_ != d_llr || g_out_ != d_out || g_iters_ != d_iters) {
     if (exec_) cudaGraphExecDestroy(exec_);
     exec_ = nullptr;
@@ -182,7 +189,7 @@ cudaError_t MixedPlan::decode(const int8_t* d_llr, uint32_t* d_out, int32_t* d_i
     cudaGraph_t graph = nullptr;
     e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      const cudaError_t le = mixed_decode_launch(m, sms_, cap);
+      const cudaError_t le = launch(cap);
       e = cudaStreamEndCapture(cap, &graph);
       if (le != cudaSuccess) e = le;
     }

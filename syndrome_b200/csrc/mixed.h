@@ -44,6 +44,7 @@ class MixedPlan {
   void release();
   MixArgs args(const int8_t* d_llr, uint32_t* d_out, int32_t* d_iters) const;
   int device_ = -1, sms_ = 0, n_items_ = 0, n_codewords_ = 0;
+  bool paired_ = false;  // paired kernel (app_clamp >= 7874) or one codeword per thread
   int beta_q_ = 0, app_clamp_ = 32767, iterations_ = 0;
   long long need_llr_ = 0, need_out_ = 0;
   MixItem* d_items_ = nullptr;

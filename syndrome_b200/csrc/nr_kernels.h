@@ -95,6 +95,11 @@ cudaError_t nr_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, 
 // app_clamp >= 3938 (>= 7874 with filler bits), where no posterior of a non-filler
 // variable can reach the clamp.  c.cpb is chosen by the launcher.
 bool nr_pair_applies(const NrCommon& c);
+// Paired mixed-shape kernel (same MixArgs as mixed_decode_launch; needs app_clamp >=
+// 7874).  Work items hold up to pair_mixed_capacity codewords of one shape.
+int pair_mixed_capacity(int bg, int z);
+cudaError_t pair_mixed_prepare();
+cudaError_t pair_mixed_launch(const MixArgs& m, int sms, cudaStream_t stream);
 cudaError_t nr_pair_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream);
 
 }  // namespace syn

@@ -42,11 +42,14 @@ struct PairArgs {
 // ZT = 384: lifting size, shifts, column bases and the CTA width (one pair of 384
 // threads) are compile-time constants, so every shared-memory address is a register
 // plus an immediate.  ZT = 0: any Z, shifts and column bases from the kernel parameters.
+// ZT = -1 (mixed-shape kernel): any Z, shifts and column bases from per-item tables in
+// shared memory.
 template <int BG, int ZT>
 struct DevCtx {
-  static_assert(ZT == 0 || ZT == 384, "compile-time lifting size must be 384");
+  static_assert(ZT == 0 || ZT == 384 || ZT == -1, "compile-time lifting size must be 384");
   static constexpr int NX = ext_regs<BG>();
   static constexpr int NS = ZT > 0 ? kPairThreads : 0;
+  int tab;  // ZT = -1: byte offset in pair_smem of the 4 * shift table (4 * col * z follows)
   int ap;   // byte offset of this pair's posteriors in pair_smem
   int st;   // byte offset of this thread's first state word in pair_smem
   int ns;
@@ -66,6 +69,11 @@ struct DevCtx {
       const unsigned r = (unsigned)(zl + Tab<BG>::z384_shift(GE) * 4);
       const unsigned rr = min(r, r - (unsigned)(ZT * 4));
       return (int)rr + Tab<BG>::col(GE) * ZT * 4;
+    } else if constexpr (ZT < 0) {
+      const int* t = reinterpret_cast<const int*>(pair_smem + tab);
+      const unsigned r = (unsigned)(zl + t[GE]);
+      const unsigned rr = min(r, r - (unsigned)Z4);
+      return (int)rr + t[Tab<BG>::E + GE];
     } else {
       const unsigned r = (unsigned)(zl + a->sh4[GE]);
       const unsigned rr = min(r, r - (unsigned)Z4);
@@ -323,6 +331,168 @@ cudaError_t launch_bg(const NrCommon& c, const int* shifts, bool fill, int sms, 
   return fill ? launch<BG, 0, true>(c, shifts, sms, stream) : launch<BG, 0, false>(c, shifts, sms, stream);
 }
 
+// ------------------------------------------------------------ mixed shapes --
+//
+// Persistent paired decode of a mixed batch (the work items and per-codeword records
+// of nr_kernels.h MixArgs): each CTA takes the next item from the device counter, an
+// item being up to 2 * floor(384 / Z) codewords of one (BG, Z), decoded as consecutive
+// pairs (codeword 2q in lane A, 2q + 1 in lane B).  The item's shifts and column bases
+// are staged in shared memory (DevCtx<BG, -1>).  Every codeword gets the 5G prologue
+// with its own filler count (the filler proxy is always on; it never touches a variable
+// that is not filler) and writes its iterations and packed hard decisions.
+
+constexpr int kPairMixTab = 2 * 316 * 4;  // 4 * shift and 4 * col * z of the largest graph
+constexpr int kPairMixSmem = 232448 - 1024;
+
+template <int BG>
+__device__ __forceinline__ void pair_mixed_item(const MixArgs& m, const MixItem& it, int tab_off) {
+  using T = Tab<BG>;
+  constexpr int NW = state_words<BG>(), CORE = T::KB + 4, NEXT = T::MB - 4;
+  constexpr int QL = quick_layer<BG>();
+  unsigned char* smem = pair_smem;
+  const int Z = it.z, ns = (int)blockDim.x, tid = (int)threadIdx.x;
+  const int P = (it.count + 1) / 2;
+  {
+    int* t = reinterpret_cast<int*>(smem + tab_off);
+    const short* sh = m.shift_tab + (long long)(BG * kMixLiftSizes + it.zi) * kMixEdges;
+    const int* cz = m.colz_tab + (long long)(BG * kMixLiftSizes + it.zi) * kMixEdges;
+    for (int e = tid; e < T::E; e += ns) {
+      t[e] = 4 * (int)sh[e];
+      t[T::E + e] = 4 * cz[e];
+    }
+  }
+  const int base = tab_off + kPairMixTab;
+  int* s_fail = reinterpret_cast<int*>(smem + base);
+  int* s_done = s_fail + P;
+  const int ap_base = base + al16(8 * P);
+  const int ap_pair = CORE * Z * 4;
+  const int st_base = ap_base + P * ap_pair;
+  const int eh_base = st_base + NW * ns * 4;
+  const int p = tid / Z, z = tid - p * Z;
+  const bool lane_ok = p < P;
+  const int pq = lane_ok ? p : 0;
+  DevCtx<BG, -1> cx;
+  cx.tab = tab_off;
+  cx.ap = ap_base + pq * ap_pair;
+  cx.st = st_base + 4 * tid;
+  cx.ns = ns;
+  cx.z4 = z * 4;
+  cx.Z4 = Z * 4;
+  cx.a = nullptr;
+  const int eh_off = eh_base + pq * NEXT * Z;
+  const uint32_t bq2 = (uint32_t)m.beta_q * 0x10001u;
+  const int core_n = CORE * Z, K = T::KB * Z;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = ns >> 5;
+  const bool va = lane_ok && 2 * p < it.count, vbv = lane_ok && 2 * p + 1 < it.count;
+  // ---- load: channel LLRs of variables 2Z..N; the punctured 2Z are erasures
+  if (lane_ok) {
+    const MixCodeword ca = m.cws[it.first + 2 * p];
+    const MixCodeword cb = vbv ? m.cws[it.first + 2 * p + 1] : ca;
+    const int8_t* sa = va ? m.llr + ca.llr_off - 2 * Z : nullptr;
+    const int8_t* sb = vbv ? m.llr + cb.llr_off - 2 * Z : nullptr;
+    const int kpa = ca.n_filler > K ? 0 : K - ca.n_filler, kpb = cb.n_filler > K ? 0 : K - cb.n_filler;
+    auto fetch = [&](const int8_t* s, int j) -> int { return (s && j >= 2 * Z) ? (int)s[j] : 0; };
+    uint32_t* apw = reinterpret_cast<uint32_t*>(smem + cx.ap);
+    for (int col = 0; col < CORE; ++col) {
+      const int j = col * Z + z;
+      uint32_t l0 = kPB + (uint32_t)fetch(sa, j), l1 = kPB + (uint32_t)fetch(sb, j);
+      if (j >= kpa && j < K) l0 = kPB + kCapV;
+      if (j >= kpb && j < K) l1 = kPB + kCapV;
+      apw[j] = (l0 & 0xFFFFu) | (l1 << 16);
+    }
+    static_for<0, DevCtx<BG, -1>::NX>([&](auto ri) {
+      constexpr int r = decltype(ri)::value;
+      uint32_t w = 0u;
+      static_for<0, 2>([&](auto hi) {
+        constexpr int h = decltype(hi)::value;
+        constexpr int xi = 2 * r + h;
+        if constexpr (xi < NEXT) {
+          const int j = (CORE + xi) * Z + z;
+          const uint32_t b0 = (uint32_t)(fetch(sa, j) + 128) & 0xFFu, b1 = (uint32_t)(fetch(sb, j) + 128) & 0xFFu;
+          w |= (b0 | (b1 << 8)) << (16 * h);
+        }
+      });
+      cx.x[r] = w;
+    });
+#pragma unroll 1
+    for (int w = 0; w < NW; ++w) *reinterpret_cast<uint32_t*>(smem + st_base + 4 * (w * ns + tid)) = 0u;
+  }
+  __syncthreads();
+  NrCommon none{};  // the mixed outputs are the packed hard decisions and iterations only
+  uint32_t act = (va ? 1u : 0u) | (vbv ? 2u : 0u);
+  uint32_t done = m.iterations <= 0 ? act : 0u;
+  int itn = 0;
+  for (;;) {
+#pragma unroll 1
+    for (int X = 0; X < 2; ++X) {
+      const bool mine = ((done >> X) & 1u) != 0u;
+      if (!__syncthreads_or(mine)) continue;
+      if (lane_ok && z == 0) s_done[p] = mine ? 1 : 0;
+      if (mine) {
+        if (z == 0 && m.iters) m.iters[m.cws[it.first + 2 * p + X].index] = itn;
+        const DevCtx<BG, -1> copy = cx;
+        write_rows<BG, -1>(&copy, &none, X, 0, Z, z, eh_off);
+      }
+      __syncthreads();
+      for (int q = 0; q < P; ++q) {
+        if (!s_done[q]) continue;
+        const MixCodeword cw = m.cws[it.first + 2 * q + X];
+        const uint32_t* apq = reinterpret_cast<const uint32_t*>(smem + ap_base + q * ap_pair);
+        const uint8_t* ehq = smem + eh_base + q * NEXT * Z;
+        uint32_t* dst = m.out + cw.out_off;
+        const int nwords = (cw.hard_bits + 31) >> 5;
+        for (int w = warp; w < nwords; w += nwarps) {
+          const int j = (w << 5) + lane;
+          bool bit = false;
+          if (j < cw.hard_bits) bit = j < core_n ? lane_of(apq[j], X) < 0 : ehq[j - core_n] != 0;
+          const uint32_t mm = __ballot_sync(0xFFFFFFFFu, bit);
+          if (lane == 0) dst[w] = mm;
+        }
+      }
+      __syncthreads();
+    }
+    act &= ~done;
+    if (!__syncthreads_or(act != 0u)) break;
+    ++itn;
+    static_for<0, T::MB>([&](auto li) {
+      constexpr int L = decltype(li)::value;
+      if (lane_ok) pair_row<BG, L, true>(cx, bq2);
+      __syncthreads();
+    });
+    if (lane_ok && z == 0) s_fail[p] = 0;
+    __syncthreads();
+    if (act) {
+      const uint32_t odd = pair_parity<BG, QL>(cx) & act;
+      if (odd) atomicOr(&s_fail[p], (int)odd);
+    }
+    __syncthreads();
+    const uint32_t pass = act & ~(uint32_t)(lane_ok ? s_fail[p] : 0);
+    if (pass) {
+      const DevCtx<BG, -1> copy = cx;
+      const uint32_t odd = full_parity<BG, -1>(&copy) & pass;
+      if (odd) atomicOr(&s_fail[p], (int)odd);
+    }
+    __syncthreads();
+    done = itn >= m.iterations ? act : act & ~(uint32_t)(lane_ok ? s_fail[p] : 0);
+  }
+}
+
+__global__ void __launch_bounds__(kPairThreads, 1) nr_pair_mixed_kernel(const __grid_constant__ MixArgs m) {
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(m.queue, 1u);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= m.n_items) break;
+    const MixItem it = m.items[item];
+    if (it.bg == 0)
+      pair_mixed_item<0>(m, it, 0);
+    else
+      pair_mixed_item<1>(m, it, 0);
+  }
+}
+
 }  // namespace nrp
 
 bool nr_pair_applies(const NrCommon& c) {
@@ -336,4 +506,23 @@ cudaError_t nr_pair_decode_i8(int bg, const NrCommon& c, const int* shifts, int 
   return nrp::launch_bg<1>(c, shifts, fill, sms, stream);
 }
 
+int pair_mixed_capacity(int bg, int z) {
+  (void)bg;
+  return 2 * std::max(1, nrp::kPairThreads / std::max(z, 1));
+}
+
+cudaError_t pair_mixed_prepare() {
+  return cudaFuncSetAttribute(nrp::nr_pair_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              nrp::kPairMixSmem);
+}
+
+cudaError_t pair_mixed_launch(const MixArgs& m, int sms, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(m.queue, 0, sizeof(unsigned), stream);
+  if (e != cudaSuccess) return e;
+  const int ctas = std::max(1, std::min(sms, m.n_items));
+  nrp::nr_pair_mixed_kernel<<<ctas, nrp::kPairThreads, nrp::kPairMixSmem, stream>>>(m);
+  return cudaGetLastError();
+}
+
 }  // namespace syn
+

@@ -99,7 +99,9 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
   beta_q_ = syn::beta_q(cfg_.beta, cfg_.scale);
   if (cudaGetDevice(&device_) != cudaSuccess) return fail("no CUDA device");
   cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
-  if (mixed_kernel_prepare() != cudaSuccess) return fail("cannot configure the decode kernel");
+  paired_ = cfg_.app_clamp >= 7874;
+  if ((paired_ ? pair_mixed_prepare() : mixed_kernel_prepare()) != cudaSuccess)
+    return fail("cannot configure the decode kernel");
   // shift and column-base tables of every 5G NR shape
   std::vector<short> shift((size_t)2 * kMixLiftSizes * kMixEdges, 0);
   std::vector<int> colz((size_t)2 * kMixLiftSizes * kMixEdges, 0);
@@ -343,7 +345,8 @@ bool ServeEngine::launch_step(Slot& s) {
   std::vector<MixCodeword> ordered;
   ordered.reserve(n_cbs);
   for (auto& kv : shapes) {
-    const int bg = kv.first.first, z = kv.first.second, cap = mixed_slot_capacity(bg, z);
+    const int bg = kv.first.first, z = kv.first.second;
+    const int cap = paired_ ? pair_mixed_capacity(bg, z) : mixed_slot_capacity(bg, z);
     const std::vector<int>& idx = kv.second;
     for (size_t a = 0; a < idx.size(); a += cap) {
       MixItem m{};
@@ -384,7 +387,7 @@ bool ServeEngine::launch_step(Slot& s) {
   m.iterations = cfg_.iterations;
   m.k32 = 32;
   m.two = 2;
-  if (e == cudaSuccess) e = mixed_decode_launch(m, sms_, st);
+  if (e == cudaSuccess) e = paired_ ? pair_mixed_launch(m, sms_, st) : mixed_decode_launch(m, sms_, st);
   if (e == cudaSuccess) e = serve_cb_crc_launch(s.d_cbs, n_cbs, s.d_crc, st);
   if (e == cudaSuccess) e = serve_tb_finish_launch(s.d_tbs, n_tb, s.d_cbs, s.d_crc, s.d_iters, st);
   if (e == cudaSuccess)

@@ -121,6 +121,7 @@ class ServeEngine {
 
   ServeConfig cfg_;
   int device_ = 0, sms_ = 0, max_words_ = 0, max_tb_words_ = 0, beta_q_ = 0;
+  bool paired_ = false;  // paired mixed-shape decode (app_clamp >= 7874)
   char* d_harq_ = nullptr;
   short* d_shift_ = nullptr;
   int* d_colz_ = nullptr;

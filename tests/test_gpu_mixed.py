@@ -69,6 +69,23 @@ def test_mixed_batch_matches_oracle():
     check(batch, buf, n_words, refs)
 
 
+def test_mixed_batch_one_codeword_per_thread_kernel():
+    """app_clamp below 7874 selects the one-codeword-per-thread mixed kernel."""
+    rng = np.random.default_rng(8)
+    shapes = [(int(rng.integers(0, 2)), int(z)) for z in rng.choice([4, 26, 96, 384], 16)]
+    recs, buf, n_words, refs = build_mix(shapes, 41, clamp=1000)
+    batch = S.MixedBatch(recs, 0.5, S.QuantParams().with_app_clamp(1000), 8)
+    check(batch, buf, n_words, refs)
+
+
+def test_mixed_batch_odd_counts_per_shape():
+    """Paired items with an odd codeword count leave one lane empty."""
+    shapes = [(0, 384)] * 3 + [(1, 384)] * 5 + [(0, 7)] * 9 + [(1, 2)] * 1
+    recs, buf, n_words, refs = build_mix(shapes, 57)
+    batch = S.MixedBatch(recs, 0.5, S.QuantParams(), 8)
+    check(batch, buf, n_words, refs)
+
+
 def test_mixed_batch_graph_replay_and_tiles():
     shapes = [(1, 13)] * 30 + [(0, 16)] * 20 + [(1, 52)] * 7
     recs, buf, n_words, refs = build_mix(shapes, 23)
