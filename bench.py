@@ -259,8 +259,15 @@ def serve_section(batch_gbps, dev, args):
     server = S.Server(max_step_code_blocks=args.serve_step_cbs, iterations=ITERS, offset_beta=BETA, scale=SCALE)
     server.run_load(pool, offered_tb_per_s=200.0, duration_s=0.05, seed=1)  # warm-up
     # capacity: offered load well above what the engine sustains, blocks per second served
+    st0 = server.stats()
     sat = server.run_load(pool, offered_tb_per_s=2.0 * batch_gbps * 1e9 / mean_bits, duration_s=0.5, seed=2)
+    st1 = server.stats()
     capacity = sat["tbs"] / sat["wall_s"]
+    sat_items = max(st1["items"] - st0["items"], 1)
+    sat_diag = {"steps": st1["steps"] - st0["steps"],
+                "code_blocks_per_step": (st1["code_blocks"] - st0["code_blocks"]) / max(st1["steps"] - st0["steps"], 1),
+                "item_thread_occupancy": (st1["item_threads"] - st0["item_threads"]) / (384.0 * sat_items),
+                "decode_gpu_s": (st1["decode_us"] - st0["decode_us"]) * 1e-6, "wall_s": sat["wall_s"]}
     points = []
     for frac in args.serve_loads:
         lam = frac * capacity
@@ -279,7 +286,7 @@ def serve_section(batch_gbps, dev, args):
             "step_code_blocks": args.serve_step_cbs, "points": points,
             "capacity_tb_per_s": capacity, "saturated_decoded_gbps": sat_gbps,
             "saturated_goodput_gbps": sat["info_bits_ok"] / sat["wall_s"] / 1e9,
-            "saturated_decoded_vs_batch": sat_gbps / batch_gbps,
+            "saturated_decoded_vs_batch": sat_gbps / batch_gbps, "saturation_diag": sat_diag,
             "steps": st["steps"], "mean_code_blocks_per_step": st["code_blocks"] / max(st["steps"], 1)}
 
 

@@ -77,6 +77,8 @@ ServeEngine::~ServeEngine() {
     cudaFreeHost(s.h_res);
     cudaFreeHost(s.h_bits);
     if (s.done) cudaEventDestroy(s.done);
+    if (s.t0) cudaEventDestroy(s.t0);
+    if (s.t1) cudaEventDestroy(s.t1);
     if (s.stream) cudaStreamDestroy(s.stream);
   }
   cudaFree(d_harq_);
@@ -130,6 +132,7 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
     if (!ok) break;
     ok = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) == cudaSuccess &&
          cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreate(&s.t0) == cudaSuccess && cudaEventCreate(&s.t1) == cudaSuccess &&
          cudaMalloc(&s.d_llr, (size_t)M * 25344) == cudaSuccess &&
          cudaMalloc(&s.d_hard, sizeof(uint32_t) * (size_t)M * max_words_) == cudaSuccess &&
          cudaMalloc(&s.d_iters, sizeof(int32_t) * M) == cudaSuccess &&
@@ -387,7 +390,9 @@ bool ServeEngine::launch_step(Slot& s) {
   m.iterations = cfg_.iterations;
   m.k32 = 32;
   m.two = 2;
+  if (e == cudaSuccess) e = cudaEventRecord(s.t0, st);
   if (e == cudaSuccess) e = paired_ ? pair_mixed_launch(m, sms_, st) : mixed_decode_launch(m, sms_, st);
+  if (e == cudaSuccess) e = cudaEventRecord(s.t1, st);
   if (e == cudaSuccess) e = serve_cb_crc_launch(s.d_cbs, n_cbs, s.d_crc, st);
   if (e == cudaSuccess) e = serve_tb_finish_launch(s.d_tbs, n_tb, s.d_cbs, s.d_crc, s.d_iters, st);
   if (e == cudaSuccess)
@@ -399,16 +404,23 @@ bool ServeEngine::launch_step(Slot& s) {
     std::lock_guard<std::mutex> lk(mu_);
     fatal_ = std::string("serving step launch failed: ") + cudaGetErrorString(e);
   }
+  long long threads = 0;
+  for (const MixItem& it : items) threads += (long long)(paired_ ? (it.count + 1) / 2 : it.count) * it.z;
   std::lock_guard<std::mutex> lk(mu_);
   stats_.steps += 1;
   stats_.code_blocks += n_cbs;
   stats_.transmissions += n_tb;
+  stats_.items += (long long)items.size();
+  stats_.item_threads += threads;
   return true;
 }
 
 void ServeEngine::finish_step(Slot& s) {
   const auto now = std::chrono::steady_clock::now();
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, s.t0, s.t1);
   std::lock_guard<std::mutex> lk(mu_);
+  stats_.decode_ms += ms;
   for (size_t j = 0; j < s.txs.size(); ++j) {
     Tb& t = tbs_[s.txs[j].id];
     const int32_t* r = s.h_res + kResWords * j;

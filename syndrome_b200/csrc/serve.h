@@ -46,6 +46,8 @@ struct ServeResult {
 struct ServeStats {
   long long steps = 0, code_blocks = 0, transmissions = 0, harq_bytes_used = 0, pending = 0, in_flight = 0;
   long long tbs_held = 0, max_pending = 0;
+  long long items = 0, item_threads = 0;  // work items launched and threads they occupy (of 384 each)
+  double decode_ms = 0.0;                 // GPU time of the decode launches (CUDA events)
 };
 
 class ServeEngine {
@@ -86,6 +88,7 @@ class ServeEngine {
   struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;  // around the decode launch
     bool busy = false;
     // device
     int8_t* d_llr = nullptr;
