@@ -267,7 +267,10 @@ def serve_section(batch_gbps, dev, args):
     sat_diag = {"steps": st1["steps"] - st0["steps"],
                 "code_blocks_per_step": (st1["code_blocks"] - st0["code_blocks"]) / max(st1["steps"] - st0["steps"], 1),
                 "item_thread_occupancy": (st1["item_threads"] - st0["item_threads"]) / (384.0 * sat_items),
-                "decode_gpu_s": (st1["decode_us"] - st0["decode_us"]) * 1e-6, "wall_s": sat["wall_s"]}
+                "decode_gpu_s": (st1["decode_us"] - st0["decode_us"]) * 1e-6,
+                "step_gpu_s": (st1["step_us"] - st0["step_us"]) * 1e-6,
+                "host_launch_s": (st1["host_launch_us"] - st0["host_launch_us"]) * 1e-6,
+                "host_finish_s": (st1["host_finish_us"] - st0["host_finish_us"]) * 1e-6, "wall_s": sat["wall_s"]}
     points = []
     for frac in args.serve_loads:
         lam = frac * capacity

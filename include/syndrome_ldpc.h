@@ -345,10 +345,12 @@ int32_t syndrome_serve_poll(SyndromeServer* server, SyndromeServeResult* out, si
 int32_t syndrome_serve_fetch(SyndromeServer* server, uint64_t tb_id, uint8_t* tb_bits, size_t tb_len);
 /* Forgets tb_id and frees its accumulators (after success, or when giving up). */
 int32_t syndrome_serve_release(SyndromeServer* server, uint64_t tb_id);
-/* out11 = {steps, code blocks, transmissions, HARQ bytes in use, queued, steps in flight,
+/* out14 = {steps, code blocks, transmissions, HARQ bytes in use, queued, steps in flight,
  * transport blocks held, largest queue seen, decode work items, threads those items
- * occupy (of 384 per item), GPU microseconds spent in the decode launches}. */
-int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out11);
+ * occupy (of 384 per item), GPU microseconds in the decode launches, GPU microseconds
+ * from each step's first copy to its last, worker microseconds building steps,
+ * worker microseconds finishing steps}. */
+int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out14);
 
 /* Open-loop load test of a server (the serving benchmark; no counterpart in the
  * reference).  Transport blocks arrive as a Poisson process of offered_tb_per_s for

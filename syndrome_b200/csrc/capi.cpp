@@ -811,13 +811,15 @@ int32_t syndrome_serve_release(SyndromeServer* server, uint64_t tb_id) {
   });
 }
 
-int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out11) {
+int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out14) {
   return guard([&]() -> int32_t {
-    if (!server || !out11) return SYNDROME_NULL_POINTER;
+    if (!server || !out14) return SYNDROME_NULL_POINTER;
     const syn::ServeStats s = server->engine.stats();
-    const int64_t v[11] = {s.steps, s.code_blocks, s.transmissions, s.harq_bytes_used, s.pending, s.in_flight,
-                           s.tbs_held, s.max_pending, s.items, s.item_threads, (int64_t)(s.decode_ms * 1000.0)};
-    for (int i = 0; i < 11; ++i) out11[i] = v[i];
+    const int64_t v[14] = {s.steps, s.code_blocks, s.transmissions, s.harq_bytes_used, s.pending, s.in_flight,
+                           s.tbs_held, s.max_pending, s.items, s.item_threads, (int64_t)(s.decode_ms * 1000.0),
+                           (int64_t)(s.step_ms * 1000.0), (int64_t)(s.host_launch_ms * 1000.0),
+                           (int64_t)(s.host_finish_ms * 1000.0)};
+    for (int i = 0; i < 14; ++i) out14[i] = v[i];
     return SYNDROME_OK;
   });
 }

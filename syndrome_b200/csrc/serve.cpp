@@ -78,6 +78,7 @@ ServeEngine::~ServeEngine() {
     cudaFreeHost(s.h_bits);
     if (s.done) cudaEventDestroy(s.done);
     if (s.t0) cudaEventDestroy(s.t0);
+    if (s.ts) cudaEventDestroy(s.ts);
     if (s.t1) cudaEventDestroy(s.t1);
     if (s.stream) cudaStreamDestroy(s.stream);
   }
@@ -131,7 +132,7 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
   for (Slot& s : slots_) {
     if (!ok) break;
     ok = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) == cudaSuccess &&
-         cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreate(&s.done) == cudaSuccess && cudaEventCreate(&s.ts) == cudaSuccess &&
          cudaEventCreate(&s.t0) == cudaSuccess && cudaEventCreate(&s.t1) == cudaSuccess &&
          cudaMalloc(&s.d_llr, (size_t)M * 25344) == cudaSuccess &&
          cudaMalloc(&s.d_hard, sizeof(uint32_t) * (size_t)M * max_words_) == cudaSuccess &&
@@ -245,6 +246,7 @@ int ServeEngine::submit(uint64_t id, long long tb_size, float rate, int qm, long
 }
 
 bool ServeEngine::launch_step(Slot& s) {
+  const auto h0 = std::chrono::steady_clock::now();
   // --- admission (under the lock) and step layout
   s.txs.clear();
   s.bits_off.clear();
@@ -287,6 +289,7 @@ bool ServeEngine::launch_step(Slot& s) {
     }
   }
   if (s.txs.empty()) return false;
+  cudaEventRecord(s.ts, s.stream);
   // --- descriptors (Tb records are stable while busy)
   std::map<std::pair<int, int>, std::vector<int>> shapes;
   long long llr_off = 0, hard_off = 0, bits_off = 0, stage_off = 0;
@@ -412,15 +415,18 @@ bool ServeEngine::launch_step(Slot& s) {
   stats_.transmissions += n_tb;
   stats_.items += (long long)items.size();
   stats_.item_threads += threads;
+  stats_.host_launch_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
   return true;
 }
 
 void ServeEngine::finish_step(Slot& s) {
   const auto now = std::chrono::steady_clock::now();
-  float ms = 0.0f;
+  float ms = 0.0f, span = 0.0f;
   cudaEventElapsedTime(&ms, s.t0, s.t1);
+  cudaEventElapsedTime(&span, s.ts, s.done);
   std::lock_guard<std::mutex> lk(mu_);
   stats_.decode_ms += ms;
+  stats_.step_ms += span;
   for (size_t j = 0; j < s.txs.size(); ++j) {
     Tb& t = tbs_[s.txs[j].id];
     const int32_t* r = s.h_res + kResWords * j;
@@ -445,6 +451,7 @@ void ServeEngine::finish_step(Slot& s) {
   }
   s.txs.clear();
   s.busy = false;
+  stats_.host_finish_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - now).count();
   cv_done_.notify_all();
 }
 

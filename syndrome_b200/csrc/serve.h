@@ -48,6 +48,8 @@ struct ServeStats {
   long long tbs_held = 0, max_pending = 0;
   long long items = 0, item_threads = 0;  // work items launched and threads they occupy (of 384 each)
   double decode_ms = 0.0;                 // GPU time of the decode launches (CUDA events)
+  double step_ms = 0.0;                   // GPU time from a step's first copy to its last
+  double host_launch_ms = 0.0, host_finish_ms = 0.0;  // worker time building and finishing steps
 };
 
 class ServeEngine {
@@ -89,6 +91,7 @@ class ServeEngine {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;  // around the decode launch
+    cudaEvent_t ts = nullptr;                // step start
     bool busy = false;
     // device
     int8_t* d_llr = nullptr;

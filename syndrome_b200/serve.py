@@ -123,10 +123,10 @@ class Server:
         _lib.check(_lib.load().syndrome_serve_release(self._h, tb_id))
 
     def stats(self):
-        v = np.zeros(11, dtype=np.int64)
+        v = np.zeros(14, dtype=np.int64)
         _lib.check(_lib.load().syndrome_serve_stats(self._h, v.ctypes.data))
         keys = ("steps", "code_blocks", "transmissions", "harq_bytes_used", "pending", "in_flight", "tbs_held",
-                "max_pending", "items", "item_threads", "decode_us")
+                "max_pending", "items", "item_threads", "decode_us", "step_us", "host_launch_us", "host_finish_us")
         return dict(zip(keys, (int(x) for x in v)))
 
     def run_load(self, pool, offered_tb_per_s, duration_s, max_transmissions=4, seed=0, latencies=False):
