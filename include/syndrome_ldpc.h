@@ -309,7 +309,7 @@ typedef struct SyndromeServer SyndromeServer;
 typedef struct {
   uint32_t max_step_code_blocks; /* code blocks per GPU step, >= 160 (0 = 2048) */
   uint32_t steps_in_flight;      /* 1..4 (0 = 2) */
-  uint64_t harq_bytes;           /* device memory for HARQ accumulators (0 = 2 GiB) */
+  uint64_t harq_bytes;           /* device memory for HARQ accumulators (0 = 8 GiB) */
   uint64_t staging_bytes;        /* device staging for host-memory LLRs, per step (0 = 256 MiB) */
   int32_t iterations;            /* maximum LOMS iterations (early stop on a zero syndrome) */
   float offset_beta;             /* beta_q = round(offset_beta * scale) clamped to [0, 127] */

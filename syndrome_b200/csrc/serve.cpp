@@ -6,7 +6,8 @@
 // order while they fit its code-block budget and, for a transport block seen for the
 // first time, while its HARQ accumulators fit the HBM budget; a new block that does
 // not fit waits, and so do the new blocks behind it, while retransmissions of blocks
-// that already hold accumulators go ahead.  A step runs, on its stream:
+// that already hold accumulators (kept in their own queue) go first.  A step runs, on
+// its stream:
 //   1. serve_combine_kernel: HARQ soft combining into the device-resident
 //      accumulators and quantization to int8 decoder input,
 //   2. the persistent mixed-shape 5G NR decode (one work queue over every code block
@@ -238,8 +239,13 @@ int ServeEngine::submit(uint64_t id, long long tb_size, float rate, int qm, long
   Tb& t = it->second;
   if (llr_len < (long long)t.p.c * t.e) return fail(SYNDROME_BUFFER_TOO_SMALL, "llr shorter than C * E");
   t.busy = true;
-  pending_.push_back(Pending{id, rv, llr, on_device, std::chrono::steady_clock::now()});
-  stats_.max_pending = std::max<long long>(stats_.max_pending, (long long)pending_.size());
+  const Pending pd{id, rv, llr, on_device, std::chrono::steady_clock::now()};
+  if (t.harq_off >= 0)
+    pending_retx_.push_back(pd);
+  else
+    pending_new_.push_back(pd);
+  stats_.max_pending =
+      std::max<long long>(stats_.max_pending, (long long)(pending_retx_.size() + pending_new_.size()));
   lk.unlock();
   cv_work_.notify_one();
   return SYNDROME_OK;
@@ -255,38 +261,32 @@ bool ServeEngine::launch_step(Slot& s) {
   long long stage_used = 0;
   int n_cbs = 0;
   {
-    // Arrival order, except that a retransmission (its accumulators are already held)
-    // never waits behind a new transport block that is waiting for HBM: that block may
-    // be waiting for exactly those accumulators to be freed.  New blocks keep their
-    // order among themselves.
+    // Retransmissions first (their blocks hold accumulators, and a new block may be
+    // waiting for exactly those to be freed), then new blocks in arrival order while
+    // their accumulators fit the HBM budget.
     std::lock_guard<std::mutex> lk(mu_);
-    bool new_blocked = false;
-    for (auto it = pending_.begin(); it != pending_.end();) {
-      const Pending pd = *it;
-      Tb& t = tbs_[pd.id];
-      if (n_cbs > 0 && n_cbs + t.p.c > cfg_.max_step_cbs) break;
-      const long long need_stage = pd.on_device ? 0 : (long long)t.p.c * t.e * 4;
-      if (need_stage && stage_used + need_stage > cfg_.staging_bytes) break;
-      if (t.harq_off < 0) {
-        if (new_blocked) {
-          ++it;
-          continue;
+    auto admit = [&](std::deque<Pending>& q, bool need_harq) {
+      while (!q.empty()) {
+        const Pending pd = q.front();
+        Tb& t = tbs_[pd.id];
+        if (n_cbs > 0 && n_cbs + t.p.c > cfg_.max_step_cbs) return;
+        const long long need_stage = pd.on_device ? 0 : (long long)t.p.c * t.e * 4;
+        if (need_stage && stage_used + need_stage > cfg_.staging_bytes) return;
+        if (need_harq && t.harq_off < 0) {
+          t.harq_off = harq_alloc((long long)t.p.c * t.p.ncb * 4);
+          if (t.harq_off < 0) return;  // HBM budget full: wait for accumulators to free
+          t.tx_count = 0;
         }
-        t.harq_off = harq_alloc((long long)t.p.c * t.p.ncb * 4);
-        if (t.harq_off < 0) {  // HBM budget full: wait for accumulators to free
-          new_blocked = true;
-          ++it;
-          continue;
-        }
-        t.tx_count = 0;
+        stage_used += need_stage;
+        n_cbs += t.p.c;
+        s.txs.push_back(pd);
+        tbv.push_back(&t);
+        first_tx.push_back(t.tx_count == 0 ? 1 : 0);
+        q.pop_front();
       }
-      stage_used += need_stage;
-      n_cbs += t.p.c;
-      s.txs.push_back(pd);
-      tbv.push_back(&t);
-      first_tx.push_back(t.tx_count == 0 ? 1 : 0);
-      it = pending_.erase(it);
-    }
+    };
+    admit(pending_retx_, false);
+    admit(pending_new_, true);
   }
   if (s.txs.empty()) return false;
   cudaEventRecord(s.ts, s.stream);
@@ -481,16 +481,17 @@ void ServeEngine::worker() {
       if (stop_) break;
       if (!fatal_.empty()) {
         // fail every queued transmission
-        while (!pending_.empty()) {
-          ServeResult res;
-          res.id = pending_.front().id;
-          tbs_[res.id].busy = false;
-          pending_.pop_front();
-          done_.push_back(res);
-        }
+        for (std::deque<Pending>* q : {&pending_retx_, &pending_new_})
+          while (!q->empty()) {
+            ServeResult res;
+            res.id = q->front().id;
+            tbs_[res.id].busy = false;
+            q->pop_front();
+            done_.push_back(res);
+          }
         cv_done_.notify_all();
       }
-      if (order_.empty() && pending_.empty()) {
+      if (order_.empty() && pending_retx_.empty() && pending_new_.empty()) {
         cv_work_.wait_for(lk, std::chrono::milliseconds(5));
         continue;
       }
@@ -506,7 +507,7 @@ void ServeEngine::worker() {
       bool have;
       {
         std::lock_guard<std::mutex> lk(mu_);
-        have = !pending_.empty() && fatal_.empty();
+        have = (!pending_retx_.empty() || !pending_new_.empty()) && fatal_.empty();
       }
       if (have && launch_step(slots_[free_slot])) {
         slots_[free_slot].busy = true;
@@ -569,7 +570,7 @@ ServeStats ServeEngine::stats() {
   std::lock_guard<std::mutex> lk(mu_);
   ServeStats s = stats_;
   s.harq_bytes_used = harq_used_;
-  s.pending = (long long)pending_.size();
+  s.pending = (long long)(pending_retx_.size() + pending_new_.size());
   s.in_flight = inflight_;
   s.tbs_held = (long long)tbs_.size();
   return s;

@@ -25,7 +25,7 @@ namespace syn {
 struct ServeConfig {
   int max_step_cbs = 2048;               // code blocks per GPU step (at least one whole TB)
   int slots = 2;                         // steps in flight
-  long long harq_bytes = 2LL << 30;      // device memory for HARQ accumulators
+  long long harq_bytes = 8LL << 30;      // device memory for HARQ accumulators
   long long staging_bytes = 256LL << 20; // device staging of host-memory LLRs, per step
   int iterations = 8;
   float beta = 0.5f;
@@ -140,7 +140,8 @@ class ServeEngine {
   std::mutex mu_;
   std::condition_variable cv_work_, cv_done_;
   std::unordered_map<uint64_t, Tb> tbs_;
-  std::deque<Pending> pending_;
+  std::deque<Pending> pending_retx_;  // transmissions of blocks that hold accumulators
+  std::deque<Pending> pending_new_;   // first transmissions (need accumulators)
   std::deque<ServeResult> done_;
   ServeStats stats_;
   bool stop_ = false;
