@@ -308,7 +308,7 @@ int32_t syndrome_dlsch_encode(const SyndromeDlSchEncoder* encoder, const uint8_t
 typedef struct SyndromeServer SyndromeServer;
 typedef struct {
   uint32_t max_step_code_blocks; /* code blocks per GPU step, >= 160 (0 = 2048) */
-  uint32_t steps_in_flight;      /* 1..4 (0 = 2) */
+  uint32_t steps_in_flight;      /* 1..16 (0 = 6): steps run concurrently on free SMs */
   uint64_t harq_bytes;           /* device memory for HARQ accumulators (0 = 8 GiB) */
   uint64_t staging_bytes;        /* device staging for host-memory LLRs, per step (0 = 256 MiB) */
   int32_t iterations;            /* maximum LOMS iterations (early stop on a zero syndrome) */
@@ -378,7 +378,8 @@ typedef struct {
   double wall_s;
   double info_bits_ok;       /* payload bits of the blocks whose CRCs passed */
   double info_bits_decoded;  /* payload bits over all transmissions (decode work done) */
-  double p50_us, p99_us, mean_us, max_us;
+  double p50_us, p99_us, mean_us, max_us;  /* per transport block, arrival to last result */
+  double tx_p50_us, tx_p99_us;             /* per transmission, submit to result */
 } SyndromeLoadReport;
 int32_t syndrome_serve_run_load(SyndromeServer* server, const SyndromeLoadTb* pool, size_t pool_n,
                                 const SyndromeLoadSpec* spec, SyndromeLoadReport* report,

@@ -732,7 +732,7 @@ int32_t syndrome_serve_create(const SyndromeServeConfig* config, SyndromeServer*
     syn::ServeConfig c;
     if (config) {
       if (config->max_step_code_blocks) c.max_step_cbs = (int)std::min<uint32_t>(config->max_step_code_blocks, 65535);
-      if (config->steps_in_flight) c.slots = (int)std::min<uint32_t>(config->steps_in_flight, 4);
+      if (config->steps_in_flight) c.slots = (int)std::min<uint32_t>(config->steps_in_flight, 16);
       if (config->harq_bytes) c.harq_bytes = (long long)config->harq_bytes;
       if (config->staging_bytes) c.staging_bytes = (long long)config->staging_bytes;
       c.iterations = config->iterations;

@@ -96,7 +96,7 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
   cfg_ = cfg;
   if (cfg_.max_step_cbs < kMaxCbPerTb) cfg_.max_step_cbs = kMaxCbPerTb;
   if (cfg_.max_step_cbs > 65535) return fail("max_step_cbs above 65535");
-  cfg_.slots = std::max(1, std::min(cfg_.slots, 4));
+  cfg_.slots = std::max(1, std::min(cfg_.slots, 16));
   if (cfg_.harq_bytes <= 0 || cfg_.staging_bytes < 0) return fail("negative memory budget");
   if (cfg_.iterations < 0) return fail("iterations must be non-negative");
   if (cfg_.app_clamp < 255) return fail("app_clamp below 255 is not supported by the serving decoder");

@@ -24,7 +24,7 @@ namespace syn {
 
 struct ServeConfig {
   int max_step_cbs = 2048;               // code blocks per GPU step (at least one whole TB)
-  int slots = 2;                         // steps in flight
+  int slots = 6;                         // steps in flight (concurrent on free SMs)
   long long harq_bytes = 8LL << 30;      // device memory for HARQ accumulators
   long long staging_bytes = 256LL << 20; // device staging of host-memory LLRs, per step
   int iterations = 8;

@@ -33,6 +33,8 @@ int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const 
   std::vector<double> latency(n, -1.0);
   std::vector<char> ok(n, 0);
   std::vector<ServeResult> res(1024);
+  std::vector<double> tx_lat;
+  tx_lat.reserve(n * 2);
   size_t next = 0, finished = 0;
   long long transmissions = 0;
   double info_ok = 0.0, info_decoded = 0.0;
@@ -64,6 +66,7 @@ int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const 
     const int got = eng.poll(res.data(), (int)res.size(), (long long)std::min(wait_s * 1e6, 2000.0));
     for (int j = 0; j < got; ++j) {
       const size_t i = (size_t)res[j].id;
+      tx_lat.push_back(res[j].latency_us);
       if (res[j].crc_ok || tx[i] >= max_tx) {
         latency[i] = (now_s() - arrivals[i]) * 1e6;
         ok[i] = res[j].crc_ok ? 1 : 0;
@@ -98,6 +101,13 @@ int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const 
   rep->p99_us = pct(0.99);
   rep->mean_us = n ? mean / (double)n : 0.0;
   rep->max_us = sorted.empty() ? 0.0 : sorted.back();
+  std::sort(tx_lat.begin(), tx_lat.end());
+  auto tpct = [&](double q) {
+    if (tx_lat.empty()) return 0.0;
+    return tx_lat[std::min(tx_lat.size() - 1, (size_t)std::floor(q * (double)(tx_lat.size() - 1) + 0.5))];
+  };
+  rep->tx_p50_us = tpct(0.50);
+  rep->tx_p99_us = tpct(0.99);
   if (lat_out)
     for (size_t i = 0; i < std::min(lat_cap, n); ++i) lat_out[i] = latency[i];
   return SYNDROME_OK;

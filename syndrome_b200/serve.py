@@ -38,12 +38,13 @@ class _LoadReport(ctypes.Structure):
     _fields_ = [("tbs", ctypes.c_uint64), ("tbs_ok", ctypes.c_uint64), ("transmissions", ctypes.c_uint64),
                 ("wall_s", ctypes.c_double), ("info_bits_ok", ctypes.c_double),
                 ("info_bits_decoded", ctypes.c_double), ("p50_us", ctypes.c_double),
-                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double)]
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double),
+                ("tx_p50_us", ctypes.c_double), ("tx_p99_us", ctypes.c_double)]
 
 
 class Server:
     """A serving engine on the current CUDA device.  Zero-valued sizes take the
-    library defaults (2048 code blocks per step, 2 steps in flight, 8 GiB of HARQ
+    library defaults (2048 code blocks per step, 6 steps in flight, 8 GiB of HARQ
     accumulators, 256 MiB of staging for host-memory LLRs)."""
 
     def __init__(self, max_step_code_blocks=0, steps_in_flight=0, harq_bytes=0, staging_bytes=0, iterations=8,
