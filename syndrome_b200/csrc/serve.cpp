@@ -459,17 +459,20 @@ void ServeEngine::worker() {
   cudaSetDevice(device_);
   for (;;) {
     bool progressed = false;
-    // completed steps, in launch order
-    while (!order_.empty()) {
-      Slot& s = slots_[order_.front()];
+    // completed steps, whichever finished (a long step does not hold back short ones)
+    for (auto it = order_.begin(); it != order_.end();) {
+      Slot& s = slots_[*it];
       const cudaError_t q = cudaEventQuery(s.done);
-      if (q == cudaErrorNotReady) break;
+      if (q == cudaErrorNotReady) {
+        ++it;
+        continue;
+      }
       if (q != cudaSuccess) {
         std::lock_guard<std::mutex> lk(mu_);
         fatal_ = std::string("serving step failed: ") + cudaGetErrorString(q);
       }
       finish_step(s);
-      order_.pop_front();
+      it = order_.erase(it);
       {
         std::lock_guard<std::mutex> lk(mu_);
         inflight_ = (int)order_.size();

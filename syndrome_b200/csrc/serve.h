@@ -24,7 +24,7 @@ namespace syn {
 
 struct ServeConfig {
   int max_step_cbs = 2048;               // code blocks per GPU step (at least one whole TB)
-  int slots = 6;                         // steps in flight (concurrent on free SMs)
+  int slots = 8;                         // steps in flight (concurrent on free SMs)
   long long harq_bytes = 8LL << 30;      // device memory for HARQ accumulators
   long long staging_bytes = 256LL << 20; // device staging of host-memory LLRs, per step
   int iterations = 8;
@@ -135,7 +135,7 @@ class ServeEngine {
   std::unordered_map<long long, long long> used_;
   long long harq_used_ = 0;
   std::vector<Slot> slots_;
-  std::deque<int> order_;                    // busy slots in launch order (worker thread only)
+  std::deque<int> order_;                    // busy slots (worker thread only)
   int inflight_ = 0;                         // order_.size(), readable under mu_
   std::mutex mu_;
   std::condition_variable cv_work_, cv_done_;
