@@ -280,6 +280,7 @@ def serve_section(batch_gbps, dev, args):
                        "transmissions_per_tb": rep["transmissions"] / max(rep["tbs"], 1),
                        "p50_us": rep["p50_us"], "p99_us": rep["p99_us"], "mean_us": rep["mean_us"],
                        "tx_p50_us": rep["tx_p50_us"], "tx_p99_us": rep["tx_p99_us"],
+                       "tx_mean_queue_us": rep["tx_mean_queue_us"], "tx_mean_step_us": rep["tx_mean_step_us"],
                        "max_us": rep["max_us"], "wall_s": rep["wall_s"],
                        "decoded_gbps": rep["info_bits_decoded"] / rep["wall_s"] / 1e9,
                        "goodput_gbps": rep["info_bits_ok"] / rep["wall_s"] / 1e9})

@@ -380,6 +380,8 @@ typedef struct {
   double info_bits_decoded;  /* payload bits over all transmissions (decode work done) */
   double p50_us, p99_us, mean_us, max_us;  /* per transport block, arrival to last result */
   double tx_p50_us, tx_p99_us;             /* per transmission, submit to result */
+  double tx_mean_queue_us;                 /* mean wait from submit to the launch of its step */
+  double tx_mean_step_us;                  /* mean GPU time of the step that decoded it */
 } SyndromeLoadReport;
 int32_t syndrome_serve_run_load(SyndromeServer* server, const SyndromeLoadTb* pool, size_t pool_n,
                                 const SyndromeLoadSpec* spec, SyndromeLoadReport* report,

@@ -289,6 +289,7 @@ bool ServeEngine::launch_step(Slot& s) {
     admit(pending_new_, true);
   }
   if (s.txs.empty()) return false;
+  s.launched = std::chrono::steady_clock::now();
   cudaEventRecord(s.ts, s.stream);
   // --- descriptors (Tb records are stable while busy)
   std::map<std::pair<int, int>, std::vector<int>> shapes;
@@ -439,6 +440,8 @@ void ServeEngine::finish_step(Slot& s) {
     res.n_cb = t.p.c;
     for (int w = 0; w < 5; ++w) res.cb_crc[w] = (uint32_t)r[2 + w];
     res.latency_us = std::chrono::duration<double, std::micro>(now - s.txs[j].t0).count();
+    res.queue_us = std::chrono::duration<double, std::micro>(s.launched - s.txs[j].t0).count();
+    res.step_us = 1000.0 * span;
     const long long nw = (t.tb_size + 31) / 32;
     t.bits.assign(s.h_bits + s.bits_off[j], s.h_bits + s.bits_off[j] + nw);
     if (res.crc_ok) {  // DlSchDecoder flushes the HARQ buffers on success

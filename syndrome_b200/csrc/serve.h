@@ -41,6 +41,8 @@ struct ServeResult {
   int n_cb = 0;
   uint32_t cb_crc[5] = {0, 0, 0, 0, 0};
   double latency_us = 0.0;  // submit to completion
+  double queue_us = 0.0;    // submit to the launch of its step
+  double step_us = 0.0;     // GPU time of its step (first copy to last)
 };
 
 struct ServeStats {
@@ -117,6 +119,7 @@ class ServeEngine {
     std::vector<Pending> txs;
     std::vector<long long> bits_off;
     int n_cbs = 0;
+    std::chrono::steady_clock::time_point launched;
   };
 
   void worker();

@@ -35,6 +35,7 @@ int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const 
   std::vector<ServeResult> res(1024);
   std::vector<double> tx_lat;
   tx_lat.reserve(n * 2);
+  double sum_queue = 0.0, sum_step = 0.0;
   size_t next = 0, finished = 0;
   long long transmissions = 0;
   double info_ok = 0.0, info_decoded = 0.0;
@@ -67,6 +68,8 @@ int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const 
     for (int j = 0; j < got; ++j) {
       const size_t i = (size_t)res[j].id;
       tx_lat.push_back(res[j].latency_us);
+      sum_queue += res[j].queue_us;
+      sum_step += res[j].step_us;
       if (res[j].crc_ok || tx[i] >= max_tx) {
         latency[i] = (now_s() - arrivals[i]) * 1e6;
         ok[i] = res[j].crc_ok ? 1 : 0;
@@ -108,6 +111,8 @@ int run_load(ServeEngine& eng, const SyndromeLoadTb* pool, size_t pool_n, const 
   };
   rep->tx_p50_us = tpct(0.50);
   rep->tx_p99_us = tpct(0.99);
+  rep->tx_mean_queue_us = tx_lat.empty() ? 0.0 : sum_queue / (double)tx_lat.size();
+  rep->tx_mean_step_us = tx_lat.empty() ? 0.0 : sum_step / (double)tx_lat.size();
   if (lat_out)
     for (size_t i = 0; i < std::min(lat_cap, n); ++i) lat_out[i] = latency[i];
   return SYNDROME_OK;

@@ -39,7 +39,8 @@ class _LoadReport(ctypes.Structure):
                 ("wall_s", ctypes.c_double), ("info_bits_ok", ctypes.c_double),
                 ("info_bits_decoded", ctypes.c_double), ("p50_us", ctypes.c_double),
                 ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double),
-                ("tx_p50_us", ctypes.c_double), ("tx_p99_us", ctypes.c_double)]
+                ("tx_p50_us", ctypes.c_double), ("tx_p99_us", ctypes.c_double),
+                ("tx_mean_queue_us", ctypes.c_double), ("tx_mean_step_us", ctypes.c_double)]
 
 
 class Server:
