@@ -416,12 +416,13 @@ def main():
     peak, peak_kind = measured_peaks()
     hbm_bytes = B * (N_TX + WORDS * 4 + 4)
     achieved = hbm_bytes / (ms_per_step * 1e-3) / 1e9
-    traffic = None
+    traffic, instr_per_update = None, None
     prof = os.path.join(ROOT, "profiles", "decode_i8_bg1_z384_traffic.json")
     if os.path.exists(prof):
         with open(prof) as f:
             pj = json.load(f)
         traffic = pj["dram_bytes_per_codeword"] * B
+        instr_per_update = pj.get("thread_instructions_per_codeword_edge_update")
     edge_updates = float(mean_iters) * 316 * Z * B
     smem_peak = 128.0 * 148 * 1.965e9  # bytes/s: 128 B/clk/SM (one 32-lane LDS.32 per clock), 148 SMs, max clock
 
@@ -440,6 +441,13 @@ def main():
                      "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes_per_codeword": N_TX + WORDS * 4 + 4,
                      "note": "LOMS is issue/shared-memory bound, not HBM bound; see smem"},
+        "issue": None if instr_per_update is None else {
+            "note": "binding resource: SM instruction issue (integer ALU pipe); instructions per edge update "
+                    "from the committed ncu profile, edge updates per second measured here",
+            "thread_instructions_per_edge_update": instr_per_update,
+            "achieved_thread_instr_per_s": edge_updates / (ms_per_step * 1e-3) * instr_per_update,
+            "peak_thread_instr_per_s": 148 * 4 * 32 * 1.965e9,
+            "frac": edge_updates / (ms_per_step * 1e-3) * instr_per_update / (148 * 4 * 32 * 1.965e9)},
         "smem": {"edge_updates_per_s": edge_updates / (ms_per_step * 1e-3),
                  "algorithmic_bytes_per_update": 4,
                  "achieved_GBps": edge_updates * 4 / (ms_per_step * 1e-3) / 1e9,
