@@ -12,7 +12,7 @@
 //   posterior / Q      PB + v with PB = 0x8000 (|v| <= 3938 + 127, or the filler
 //                      proxy below); the lane's top bit is 1 iff v >= 0
 //   message table out  127 + R (R in [-127, 127]), zero-extended
-//   min-sum key        |Q| * 128 + tag(edge)
+//   min-sum key        |Q| * 256 + tag(edge)
 //
 // Per check row the compressed C->V state is one meta word, bytes
 // [min1'A, min2'A, min1'B, min2'B] (offset magnitudes), and ceil(deg / 8) code
@@ -170,6 +170,7 @@ __host__ __device__ __forceinline__ uint32_t ext_lanes(uint32_t xreg, int xi) {
 //   uint32_t ld_st(int w) / void st_st(int w, uint32_t)   state word w of this row group
 //   uint32_t xr(int i) const             extension channel register i
 
+// bq2 = 256 * beta_q in both lanes (beta_q * 0x01000100).
 template <int BG, int L, bool FILL, class C>
 __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
   constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L), NC = ncw(deg), W = state_off<BG>(L);
@@ -195,16 +196,17 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
       qu[e] = a - prmt(tlo, thi, code_sel(code[e >> 3], code_shift(e))) + 0x007F007Fu;  // PB + app - R_old
     }
     // PB + min(|Q|, 127) (0x10000 - Q32 is PB - Q in both lanes), then
-    // key = |Q| * 128 + tag (the 128 * PB terms cancel mod 2^32)
+    // key = |Q| * 256 + tag (the 256 * PB terms cancel mod 2^32)
     const uint32_t aq = vminu2(vmaxu2(qu[e], 0x00010000u - qu[e]), 0x807F807Fu);
-    const uint32_t key = aq * 128u + ((uint32_t)key_tag(e) * 0x10001u - 0x00400000u);
+    const uint32_t key = aq * 256u + ((uint32_t)key_tag(e) * 0x10001u - 0x00800000u);
     m2k = vminu2(m2k, vmaxu2(m1k, key));
     m1k = vminu2(m1k, key);
   });
-  // Row results: offset magnitudes, new meta word and message table.
-  const uint32_t m1 = (m1k >> 7) & 0x007F007Fu, m2 = (m2k >> 7) & 0x007F007Fu;
-  const uint32_t m1p = vmaxu2(m1, bq2) - bq2, m2p = vmaxu2(m2, bq2) - bq2;
-  const uint32_t nmeta = m2p * 256u + m1p;
+  // Row results.  In the key domain, max(key, 256 beta) - 256 beta has byte 1 of each
+  // lane = max(min - beta, 0), the offset magnitude; one byte permute gathers
+  // [min1'A, min2'A, min1'B, min2'B] into the new meta word.
+  const uint32_t m1x = vmaxu2(m1k, bq2) - bq2, m2x = vmaxu2(m2k, bq2) - bq2;
+  const uint32_t nmeta = prmt(m1x, m2x, 0x7351u);
   const uint32_t nlo = table_lo(nmeta), nhi = table_hi(nmeta);
   // Code words: the Q >= 0 bits (top bits of the lanes) of edges j and j + 4 spread to
   // whole bytes by one sign-replicating byte-permute, then masked into each edge's
@@ -226,12 +228,12 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
       }
     });
   });
-  // ... turned into R's sign (Q >= 0 xor an odd count of negative Q in the row) ...
-  const uint32_t par = sacc ^ (sacc >> 16);  // byte 0: lane A parity of Q >= 0, byte 1: lane B
-  const uint32_t sn = (par & 0x0101u) ^ ((deg & 1) ? 0x0101u : 0u);
-  const uint32_t smask = sn * 0x00AA00AAu;
+  // ... turned into R's sign (Q >= 0 xor an odd count of negative Q in the row):
+  // bytes [A, B, A, B] of par are each lane's parity of Q >= 0 as 0x00 / 0xFF ...
+  const uint32_t par = sacc ^ prmt(sacc, sacc, 0x1032u);
+  const uint32_t smask = ((deg & 1) ? ~par : par) & 0xAAAAAAAAu;
   // ... plus the argmin flag from the winning key's tag.
-  const uint32_t tA = m1k & 127u, tB = (m1k >> 16) & 127u;
+  const uint32_t tA = m1k & 255u, tB = prmt(m1k, 0u, 0x4442u);
   static_for<0, NC>([&](auto ki) {
     constexpr int k = decltype(ki)::value;
     nc[k] = (nc[k] ^ smask) | shl_sat(1u, tA - 32u * k) | shl_sat(256u, tB - 32u * k);

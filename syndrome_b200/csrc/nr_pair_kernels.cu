@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
   cx.Z4 = Z * 4;
   cx.a = &a;
   uint8_t* eh = eh_base + pq * NEXT * Z;
-  const uint32_t bq2 = (uint32_t)c.beta_q * 0x10001u;
+  const uint32_t bq2 = (uint32_t)c.beta_q * 0x01000100u;
   const int core_n = CORE * Z, K = T::KB * Z;
   const long long npairs = (c.batch + 1) / 2;
   const long long ngroups = (npairs + P - 1) / P;
@@ -380,7 +380,7 @@ __device__ __forceinline__ void pair_mixed_item(const MixArgs& m, const MixItem&
   cx.Z4 = Z * 4;
   cx.a = nullptr;
   const int eh_off = eh_base + pq * NEXT * Z;
-  const uint32_t bq2 = (uint32_t)m.beta_q * 0x10001u;
+  const uint32_t bq2 = (uint32_t)m.beta_q * 0x01000100u;
   const int core_n = CORE * Z, K = T::KB * Z;
   const int lane = tid & 31, warp = tid >> 5, nwarps = ns >> 5;
   const bool va = lane_ok && 2 * p < it.count, vbv = lane_ok && 2 * p + 1 < it.count;

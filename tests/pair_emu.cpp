@@ -62,7 +62,7 @@ int run(int Z, const int* shifts, int beta_q, int app_clamp, int prologue, int n
       xr[(size_t)z * NX + (xi >> 1)] |= (lanes[0] | (lanes[1] << 8)) << (16 * (xi & 1));
     }
   }
-  const uint32_t bq2 = (uint32_t)beta_q * 0x10001u;
+  const uint32_t bq2 = (uint32_t)beta_q * 0x01000100u;
   auto ctx = [&](int z) {
     return EmuCtx<BG>{ap.data(), st.data() + (size_t)z * NW, xr.data() + (size_t)z * NX, z, Z, shifts};
   };
