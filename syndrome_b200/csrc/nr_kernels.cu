@@ -218,14 +218,20 @@ __device__ __forceinline__ int iterate(const EDGES ed, const RunConsts rc, bool 
     });
     if (lane_ok && z == 0) s_flag[slot] = 0;
     __syncthreads();
-    constexpr int QL = quick_layer<BG>();
-    if (active && row_parity<BG, QL>(ed, rc.z, z, A, X, st, ns)) s_flag[slot] = 1;
+    if (active) {
+      bool odd = false;
+      static_for<0, T::MB>([&](auto li) {
+        constexpr int L = decltype(li)::value;
+        if constexpr (is_quick<BG>(L)) odd |= row_parity<BG, L>(ed, rc.z, z, A, X, st, ns);
+      });
+      if (odd) s_flag[slot] = 1;
+    }
     __syncthreads();
     if (active && s_flag[slot] == 0) {
       bool odd = false;
       static_for<0, T::MB>([&](auto li) {
         constexpr int L = decltype(li)::value;
-        if constexpr (L != QL) odd |= row_parity<BG, L>(ed, rc.z, z, A, X, st, ns);
+        if constexpr (!is_quick<BG>(L)) odd |= row_parity<BG, L>(ed, rc.z, z, A, X, st, ns);
       });
       if (odd) s_flag[slot] = 1;
     }

@@ -45,16 +45,31 @@ namespace nrp {
 using nr::deg_of;
 using nr::ext_pos;
 using nr::is_ext;
-using nr::quick_layer;
+using nr::is_quick;
 using nr::static_for;
 using nr::Tab;
 
-constexpr uint32_t kPB = 0x8000u;            // lane bias
+constexpr uint32_t kPB = 0x8000u;            // lane bias of computed values (Q, app)
 constexpr uint32_t kPB2 = 0x80008000u;
+// Stored posterior lanes carry kAB = PB + 127, the message table's bias, so that
+// Q = stored - message and stored' = Q + message need no constant.
+constexpr uint32_t kAB = kPB + 127u;
+constexpr uint32_t kAB2 = kAB * 0x10001u;
 constexpr int kCapV = 8192;                  // filler proxy ceiling (>= 7874)
-constexpr uint32_t kCap2 = (kPB + kCapV) * 0x10001u;
+constexpr uint32_t kCapS2 = (kAB + kCapV) * 0x10001u;  // filler proxy ceiling, stored form
 constexpr int kMinFillerClamp = 7874;        // 30 * 254 + 2 * 127: deficit bound plus Q clamp
 constexpr int kMaxReach = 3938;              // 128 + 30 * 127: largest reachable |posterior|
+
+// Multipliers read from the constant bank: the compiler cannot see their values, so
+// the multiply-adds below stay multiply-adds on the FMA pipe instead of becoming
+// shifts, adds or LEAs on the integer ALU pipe, which is the kernel's binding pipe.
+// [0] 1, [1] -1, [2] 256, [3] 0xFFFF, [4..6] 2^30, 2^28, 2^26, [7] 2^16,
+// [8..11] 2^16, 2^14, 2^12, 2^10.
+#define SYN_PAIR_K \
+  { 1u, 0xFFFFFFFFu, 256u, 0xFFFFu, 1u << 30, 1u << 28, 1u << 26, 1u << 16, 1u << 16, 1u << 14, 1u << 12, 1u << 10 }
+#ifdef __CUDACC__
+static __constant__ uint32_t kPairK[12] = SYN_PAIR_K;
+#endif
 
 // ------------------------------------------------------------------ SWAR ops --
 
@@ -147,14 +162,47 @@ __host__ __device__ constexpr int ext_regs() {
   return (Tab<BG>::MB - 4 + 1) / 2;
 }
 
-// Byte-permute selector of edge e from its code word (the shift as a multiply-high).
-__host__ __device__ __forceinline__ uint32_t code_sel(uint32_t code_word, int shift) {
-  const uint32_t w = shift ? mulhi(code_word, 1u << (32 - shift)) : code_word;
-  return (w & 0x0303u) | 0xC480u;
+// a * K[ki] + b and hi(a * K[ki]), with K the multiplier table above (IMADs on the device).
+__host__ __device__ __forceinline__ uint32_t mad_k(uint32_t a, int ki, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return a * kPairK[ki] + b;
+#else
+  constexpr uint32_t K[12] = SYN_PAIR_K;
+  return a * K[ki] + b;
+#endif
 }
-// Message table of a meta word: lanes 127 + R after prmt(lo, hi, selector).
-__host__ __device__ __forceinline__ uint32_t table_lo(uint32_t meta) { return (meta & 0xFFFFu) * 0xFFFFu + 0x7F7F7F7Fu; }
-__host__ __device__ __forceinline__ uint32_t table_hi(uint32_t meta) { return (meta >> 16) * 0xFFFFu + 0x7F7F7F7Fu; }
+__host__ __device__ __forceinline__ uint32_t mulhi_k(uint32_t a, int ki) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, kPairK[ki]);
+#else
+  constexpr uint32_t K[12] = SYN_PAIR_K;
+  return (uint32_t)(((uint64_t)a * K[ki]) >> 32);
+#endif
+}
+
+// Byte-permute selector of an edge from its code word: ((code >> shift) & 0x0303) | selc
+// with selc = 0xC480, the shift as a multiply-high and the mask-and-or as one LOP3
+// (written out: the compiler splits it in two otherwise).
+__host__ __device__ __forceinline__ uint32_t code_sel(uint32_t code_word, int shift, uint32_t selc) {
+  const uint32_t w = shift ? mulhi_k(code_word, shift < 16 ? 3 + (shift >> 1) : 8 + ((shift - 16) >> 1)) : code_word;
+#ifdef __CUDA_ARCH__
+  uint32_t d;
+  asm("lop3.b32 %0, %1, 0x0303, %2, 0xEA;" : "=r"(d) : "r"(w), "r"(selc));
+  return d;
+#else
+  return (w & 0x0303u) | selc;
+#endif
+}
+
+// Message tables of a meta word [m1'A, m2'A, m1'B, m2'B]: lo = lane A's bytes
+// [127 - m1', 127 - m2', 127 + m1', 127 + m2'], hi = lane B's; c7f = 0x7F7F7F7F.
+// With mB = meta >> 16: hi = mB * 0xFFFF + c7f and lo = (meta & 0xFFFF) * 0xFFFF + c7f
+// = meta * 0xFFFF + mB * 2^16 + c7f (mod 2^32), all multiply-adds.
+__host__ __device__ __forceinline__ void tables(uint32_t meta, uint32_t c7f, uint32_t& lo, uint32_t& hi) {
+  const uint32_t mB = mulhi_k(meta, 7);
+  hi = mad_k(mB, 3, c7f);
+  lo = mad_k(mB, 7, mad_k(meta, 3, c7f));
+}
 
 // Biased channel value lanes (PB + x) of extension layer index xi (= layer - 4).
 __host__ __device__ __forceinline__ uint32_t ext_lanes(uint32_t xreg, int xi) {
@@ -169,19 +217,24 @@ __host__ __device__ __forceinline__ uint32_t ext_lanes(uint32_t xreg, int xi) {
 //   uint32_t ld_ap(int) / void st_ap(int, uint32_t)
 //   uint32_t ld_st(int w) / void st_st(int w, uint32_t)   state word w of this row group
 //   uint32_t xr(int i) const             extension channel register i
+//   uint32_t selc() const, c7f() const   the constants 0xC480 and 0x7F7F7F7F (registers)
 
-// bq2 = 256 * beta_q in both lanes (beta_q * 0x01000100).
+// Offset beta_q in the key domain, both lanes (the pair_row argument).
+__host__ __device__ constexpr uint32_t pair_beta(int beta_q) { return (uint32_t)beta_q * 0x01000100u; }
+
 template <int BG, int L, bool FILL, class C>
 __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
   constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L), NC = ncw(deg), W = state_off<BG>(L);
   constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
+  const uint32_t selc = c.selc(), c7f = c.c7f();
   const uint32_t meta = c.ld_st(W);
   uint32_t code[NC];
   static_for<0, NC>([&](auto ki) {
     constexpr int k = decltype(ki)::value;
     code[k] = c.ld_st(W + 1 + k);
   });
-  const uint32_t tlo = table_lo(meta), thi = table_hi(meta);
+  uint32_t tlo, thi;
+  tables(meta, c7f, tlo, thi);
   uint32_t qu[deg];
   int vb[deg];
   uint32_t m1k = 0x7FFF7FFFu, m2k = 0x7FFF7FFFu;
@@ -192,13 +245,13 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
       vb[e] = 0;
     } else {
       vb[e] = c.template vb<lb + e>();
-      const uint32_t a = c.ld_ap(vb[e]);
-      qu[e] = a - prmt(tlo, thi, code_sel(code[e >> 3], code_shift(e))) + 0x007F007Fu;  // PB + app - R_old
+      // PB + app - R_old = stored - (127 + R_old)
+      qu[e] = mad_k(prmt(tlo, thi, code_sel(code[e >> 3], code_shift(e), selc)), 1, c.ld_ap(vb[e]));
     }
     // PB + min(|Q|, 127) (0x10000 - Q32 is PB - Q in both lanes), then
     // key = |Q| * 256 + tag (the 256 * PB terms cancel mod 2^32)
-    const uint32_t aq = vminu2(vmaxu2(qu[e], 0x00010000u - qu[e]), 0x807F807Fu);
-    const uint32_t key = aq * 256u + ((uint32_t)key_tag(e) * 0x10001u - 0x00800000u);
+    const uint32_t aq = vminu2(vmaxu2(qu[e], mad_k(qu[e], 1, 0x00010000u)), 0x807F807Fu);
+    const uint32_t key = mad_k(aq, 2, (uint32_t)key_tag(e) * 0x10001u - 0x00800000u);
     m2k = vminu2(m2k, vmaxu2(m1k, key));
     m1k = vminu2(m1k, key);
   });
@@ -207,7 +260,8 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
   // [min1'A, min2'A, min1'B, min2'B] into the new meta word.
   const uint32_t m1x = vmaxu2(m1k, bq2) - bq2, m2x = vmaxu2(m2k, bq2) - bq2;
   const uint32_t nmeta = prmt(m1x, m2x, 0x7351u);
-  const uint32_t nlo = table_lo(nmeta), nhi = table_hi(nmeta);
+  uint32_t nlo, nhi;
+  tables(nmeta, c7f, nlo, nhi);
   // Code words: the Q >= 0 bits (top bits of the lanes) of edges j and j + 4 spread to
   // whole bytes by one sign-replicating byte-permute, then masked into each edge's
   // sign slot ...
@@ -238,12 +292,12 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
     constexpr int k = decltype(ki)::value;
     nc[k] = (nc[k] ^ smask) | shl_sat(1u, tA - 32u * k) | shl_sat(256u, tB - 32u * k);
   });
-  // Posterior update: app = Q + R_new.
+  // Posterior update: stored = Q + 127 + R_new.
   static_for<0, deg>([&](auto ei) {
     constexpr int e = decltype(ei)::value;
     if constexpr (e != ep) {
-      uint32_t v = qu[e] + prmt(nlo, nhi, code_sel(nc[e >> 3], code_shift(e))) - 0x007F007Fu;
-      if constexpr (FILL) v = vminu2(v, kCap2);
+      uint32_t v = mad_k(prmt(nlo, nhi, code_sel(nc[e >> 3], code_shift(e), selc)), 0, qu[e]);
+      if constexpr (FILL) v = vminu2(v, kCapS2);
       c.st_ap(vb[e], v);
     }
   });
@@ -258,8 +312,9 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
 template <int BG, int L, int E, class C>
 __host__ __device__ __forceinline__ uint32_t pair_message(const C& c) {
   constexpr int W = state_off<BG>(L);
-  const uint32_t meta = c.ld_st(W);
-  return prmt(table_lo(meta), table_hi(meta), code_sel(c.ld_st(W + 1 + (E >> 3)), code_shift(E)));
+  uint32_t lo, hi;
+  tables(c.ld_st(W), 0x7F7F7F7Fu, lo, hi);
+  return prmt(lo, hi, code_sel(c.ld_st(W + 1 + (E >> 3)), code_shift(E), 0xC480u));
 }
 
 // Posterior lanes (PB + app) of the extension column of layer L >= 4.
@@ -281,11 +336,22 @@ __host__ __device__ __forceinline__ uint32_t pair_parity(const C& c) {
     if constexpr (e == ep) {
       x ^= pair_ext_app<BG, L>(c);
     } else {
-      x ^= c.ld_ap(c.template vb<lb + e>());
+      x ^= c.ld_ap(c.template vb<lb + e>()) - (kAB2 - kPB2);  // stored lanes to PB + app
     }
   });
   const uint32_t nn = ((x >> 15) & 1u) | ((x >> 30) & 2u);
   return nn ^ ((deg & 1) ? 3u : 0u);
+}
+
+// Parity of the quick-stage layers (same bits as pair_parity).
+template <int BG, class C>
+__host__ __device__ __forceinline__ uint32_t quick_parity(const C& c) {
+  uint32_t odd = 0u;
+  static_for<0, Tab<BG>::MB>([&](auto li) {
+    constexpr int L = decltype(li)::value;
+    if constexpr (is_quick<BG>(L)) odd |= pair_parity<BG, L>(c);
+  });
+  return odd;
 }
 
 }  // namespace nrp

@@ -57,7 +57,14 @@ struct DevCtx {
   int Z4;
   const PairArgs<BG>* a;
   uint32_t x[NX];
+  // Constants the row update takes from registers (a LOP3 or IMAD addend): set once
+  // and made opaque to the compiler, which would otherwise fold them into immediates
+  // and split the instruction in two.
+  uint32_t sc;   // 0xC480, the byte-permute selector's fixed bits
+  uint32_t k7f;  // 0x7F7F7F7F, the message tables' bias
 
+  __device__ __forceinline__ uint32_t selc() const { return sc; }
+  __device__ __forceinline__ uint32_t c7f() const { return k7f; }
   template <int GE>
   __device__ __forceinline__ int vb() const {
     // (z + shift) mod Z in bytes, as an unsigned min: below Z the second candidate wraps high.
@@ -81,10 +88,12 @@ struct DevCtx {
     }
   }
   __device__ __forceinline__ int stride() const { return NS > 0 ? NS : ns; }
+  // With ZT > 0 the CTA holds one pair whose posteriors start right after the two flag words.
+  __device__ __forceinline__ int apb() const { return ZT > 0 ? 16 : ap; }
   __device__ __forceinline__ uint32_t ld_ap(int b) const {
-    return *reinterpret_cast<const uint32_t*>(pair_smem + ap + b);
+    return *reinterpret_cast<const uint32_t*>(pair_smem + apb() + b);
   }
-  __device__ __forceinline__ void st_ap(int b, uint32_t v) { *reinterpret_cast<uint32_t*>(pair_smem + ap + b) = v; }
+  __device__ __forceinline__ void st_ap(int b, uint32_t v) { *reinterpret_cast<uint32_t*>(pair_smem + apb() + b) = v; }
   __device__ __forceinline__ uint32_t ld_st(int w) const {
     return *reinterpret_cast<const uint32_t*>(pair_smem + st + 4 * w * stride());
   }
@@ -103,19 +112,21 @@ __host__ __device__ inline int pair_smem_bytes(int pairs, int z, int threads) {
          al16(pairs * (T::MB - 4) * z);
 }
 
-__device__ __forceinline__ int lane_of(uint32_t w, int lane) { return (int)((w >> (16 * lane)) & 0xFFFFu) - (int)kPB; }
+// Signed value of one lane of a biased word: bias kPB (computed posteriors) or kAB (stored).
+__device__ __forceinline__ int lane_of(uint32_t w, int lane, uint32_t bias = kPB) {
+  return (int)((w >> (16 * lane)) & 0xFFFFu) - (int)bias;
+}
 
 // Cold paths as separate functions (own register allocation; the caller passes a copy
 // of its context so that the hot loop's registers stay where they are).
 
-// Parity of every check row except the quick layer's (bit 0 lane A odd, bit 1 lane B).
+// Parity of every check row outside the quick-stage layers (bit 0 lane A odd, bit 1 lane B).
 template <int BG, int ZT>
 __device__ __noinline__ uint32_t full_parity(const DevCtx<BG, ZT>* cx) {
-  constexpr int QL = quick_layer<BG>();
   uint32_t odd = 0u;
   static_for<0, Tab<BG>::MB>([&](auto li) {
     constexpr int L = decltype(li)::value;
-    if constexpr (L != QL) odd |= pair_parity<BG, L>(*cx);
+    if constexpr (!is_quick<BG>(L)) odd |= pair_parity<BG, L>(*cx);
   });
   return odd;
 }
@@ -153,7 +164,6 @@ template <int BG, int ZT, bool FILL>
 __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_constant__ PairArgs<BG> a) {
   using T = Tab<BG>;
   constexpr int NW = state_words<BG>(), CORE = T::KB + 4, NEXT = T::MB - 4;
-  constexpr int QL = quick_layer<BG>();
   unsigned char* smem = pair_smem;
   const NrCommon& c = a.c;
   const int Z = ZT > 0 ? ZT : c.z;
@@ -175,9 +185,12 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
   cx.ns = ns;
   cx.z4 = z * 4;
   cx.Z4 = Z * 4;
+  cx.sc = 0xC480u;
+  cx.k7f = 0x7F7F7F7Fu;
+  asm volatile("" : "+r"(cx.sc), "+r"(cx.k7f));
   cx.a = &a;
   uint8_t* eh = eh_base + pq * NEXT * Z;
-  const uint32_t bq2 = (uint32_t)c.beta_q * 0x01000100u;
+  const uint32_t bq2 = pair_beta(c.beta_q);
   const int core_n = CORE * Z, K = T::KB * Z;
   const long long npairs = (c.batch + 1) / 2;
   const long long ngroups = (npairs + P - 1) / P;
@@ -195,12 +208,12 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
       uint32_t* apw = reinterpret_cast<uint32_t*>(smem + cx.ap);
       for (int col = 0; col < CORE; ++col) {
         const int j = col * Z + z;
-        uint32_t l0 = kPB + (uint32_t)fetch(sa, j), l1 = kPB + (uint32_t)fetch(sb, j);
+        uint32_t l0 = kAB + (uint32_t)fetch(sa, j), l1 = kAB + (uint32_t)fetch(sb, j);
         if (c.prologue) {
           if (j < 2 * Z) {
-            l0 = l1 = kPB;
+            l0 = l1 = kAB;
           } else if (FILL && j >= c.k_prime && j < K) {
-            l0 = l1 = kPB + kCapV;
+            l0 = l1 = kAB + kCapV;
           }
         }
         apw[j] = (l0 & 0xFFFFu) | (l1 << 16);
@@ -250,7 +263,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
           const uint8_t* ehq = eh_base + q * NEXT * Z;
           if (c.app_out || c.hard_out) {
             for (int j = tid; j < core_n; j += ns) {
-              int v = lane_of(apq[j], X);
+              int v = lane_of(apq[j], X, kAB);
               if (FILL && j >= c.k_prime && j < K) v += c.app_clamp - kCapV;
               if (c.app_out) c.app_out[cwo * c.app_stride + j] = (int16_t)v;
               if (c.hard_out) c.hard_out[cwo * c.hard_stride + j] = v < 0 ? 1 : 0;
@@ -262,7 +275,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
             for (int w = warp; w < nwords; w += nwarps) {
               const int j = (w << 5) + lane;
               bool bit = false;
-              if (j < c.hard_bits) bit = j < core_n ? lane_of(apq[j], X) < 0 : ehq[j - core_n] != 0;
+              if (j < c.hard_bits) bit = j < core_n ? lane_of(apq[j], X, kAB) < 0 : ehq[j - core_n] != 0;
               const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
               if (lane == 0) dst[w] = m;
             }
@@ -276,13 +289,13 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
       static_for<0, T::MB>([&](auto li) {
         constexpr int L = decltype(li)::value;
         if (lane_ok) pair_row<BG, L, FILL>(cx, bq2);
-        __syncthreads();
+        if constexpr (nr::barrier_after<BG>(L)) __syncthreads();
       });
       // syndrome: the smallest layer first, the others only for lanes that pass it
       if (lane_ok && z == 0) s_fail[p] = 0;
       __syncthreads();
       if (act) {
-        const uint32_t odd = pair_parity<BG, QL>(cx) & act;
+        const uint32_t odd = quick_parity<BG>(cx) & act;
         if (odd) atomicOr(&s_fail[p], (int)odd);
       }
       __syncthreads();
@@ -348,7 +361,6 @@ template <int BG>
 __device__ __forceinline__ void pair_mixed_item(const MixArgs& m, const MixItem& it, int tab_off) {
   using T = Tab<BG>;
   constexpr int NW = state_words<BG>(), CORE = T::KB + 4, NEXT = T::MB - 4;
-  constexpr int QL = quick_layer<BG>();
   unsigned char* smem = pair_smem;
   const int Z = it.z, ns = (int)blockDim.x, tid = (int)threadIdx.x;
   const int P = (it.count + 1) / 2;
@@ -378,9 +390,12 @@ __device__ __forceinline__ void pair_mixed_item(const MixArgs& m, const MixItem&
   cx.ns = ns;
   cx.z4 = z * 4;
   cx.Z4 = Z * 4;
+  cx.sc = 0xC480u;
+  cx.k7f = 0x7F7F7F7Fu;
+  asm volatile("" : "+r"(cx.sc), "+r"(cx.k7f));
   cx.a = nullptr;
   const int eh_off = eh_base + pq * NEXT * Z;
-  const uint32_t bq2 = (uint32_t)m.beta_q * 0x01000100u;
+  const uint32_t bq2 = pair_beta(m.beta_q);
   const int core_n = CORE * Z, K = T::KB * Z;
   const int lane = tid & 31, warp = tid >> 5, nwarps = ns >> 5;
   const bool va = lane_ok && 2 * p < it.count, vbv = lane_ok && 2 * p + 1 < it.count;
@@ -395,9 +410,9 @@ __device__ __forceinline__ void pair_mixed_item(const MixArgs& m, const MixItem&
     uint32_t* apw = reinterpret_cast<uint32_t*>(smem + cx.ap);
     for (int col = 0; col < CORE; ++col) {
       const int j = col * Z + z;
-      uint32_t l0 = kPB + (uint32_t)fetch(sa, j), l1 = kPB + (uint32_t)fetch(sb, j);
-      if (j >= kpa && j < K) l0 = kPB + kCapV;
-      if (j >= kpb && j < K) l1 = kPB + kCapV;
+      uint32_t l0 = kAB + (uint32_t)fetch(sa, j), l1 = kAB + (uint32_t)fetch(sb, j);
+      if (j >= kpa && j < K) l0 = kAB + kCapV;
+      if (j >= kpb && j < K) l1 = kAB + kCapV;
       apw[j] = (l0 & 0xFFFFu) | (l1 << 16);
     }
     static_for<0, DevCtx<BG, -1>::NX>([&](auto ri) {
@@ -444,7 +459,7 @@ __device__ __forceinline__ void pair_mixed_item(const MixArgs& m, const MixItem&
         for (int w = warp; w < nwords; w += nwarps) {
           const int j = (w << 5) + lane;
           bool bit = false;
-          if (j < cw.hard_bits) bit = j < core_n ? lane_of(apq[j], X) < 0 : ehq[j - core_n] != 0;
+          if (j < cw.hard_bits) bit = j < core_n ? lane_of(apq[j], X, kAB) < 0 : ehq[j - core_n] != 0;
           const uint32_t mm = __ballot_sync(0xFFFFFFFFu, bit);
           if (lane == 0) dst[w] = mm;
         }
@@ -457,12 +472,12 @@ __device__ __forceinline__ void pair_mixed_item(const MixArgs& m, const MixItem&
     static_for<0, T::MB>([&](auto li) {
       constexpr int L = decltype(li)::value;
       if (lane_ok) pair_row<BG, L, true>(cx, bq2);
-      __syncthreads();
+      if constexpr (nr::barrier_after<BG>(L)) __syncthreads();
     });
     if (lane_ok && z == 0) s_fail[p] = 0;
     __syncthreads();
     if (act) {
-      const uint32_t odd = pair_parity<BG, QL>(cx) & act;
+      const uint32_t odd = quick_parity<BG>(cx) & act;
       if (odd) atomicOr(&s_fail[p], (int)odd);
     }
     __syncthreads();

@@ -33,6 +33,8 @@ struct EmuCtx {
   uint32_t ld_st(int w) const { return st[w]; }
   void st_st(int w, uint32_t v) { st[w] = v; }
   uint32_t xr(int i) const { return x[i]; }
+  uint32_t selc() const { return 0xC480u; }
+  uint32_t c7f() const { return 0x7F7F7F7Fu; }
 };
 
 template <int BG, bool FILL>
@@ -51,7 +53,7 @@ int run(int Z, const int* shifts, int beta_q, int app_clamp, int prologue, int n
       if (prologue && j < 2 * Z) v = 0;
       const bool filler = prologue && j >= kp && j < K;
       if (j < core)
-        lanes[l] = filler ? kPB + kCapV : kPB + v;
+        lanes[l] = filler ? kAB + kCapV : kAB + v;
       else
         lanes[l] = (uint32_t)(v + 128) & 0xFFu;
     }
@@ -62,7 +64,7 @@ int run(int Z, const int* shifts, int beta_q, int app_clamp, int prologue, int n
       xr[(size_t)z * NX + (xi >> 1)] |= (lanes[0] | (lanes[1] << 8)) << (16 * (xi & 1));
     }
   }
-  const uint32_t bq2 = (uint32_t)beta_q * 0x01000100u;
+  const uint32_t bq2 = pair_beta(beta_q);
   auto ctx = [&](int z) {
     return EmuCtx<BG>{ap.data(), st.data() + (size_t)z * NW, xr.data() + (size_t)z * NX, z, Z, shifts};
   };
@@ -71,7 +73,7 @@ int run(int Z, const int* shifts, int beta_q, int app_clamp, int prologue, int n
     int16_t* app = app_out + (size_t)lane * N;
     int8_t* er = edge_r_out + (size_t)lane * T::E * Z;
     for (int j = 0; j < core; ++j) {
-      int v = (int)((ap[j] >> (16 * lane)) & 0xFFFFu) - (int)kPB;
+      int v = (int)((ap[j] >> (16 * lane)) & 0xFFFFu) - (int)kAB;
       if (FILL && j >= kp && j < K) v += app_clamp - kCapV;
       app[j] = (int16_t)v;
     }
