@@ -237,7 +237,10 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
   tables(meta, c7f, tlo, thi);
   uint32_t qu[deg];
   int vb[deg];
-  uint32_t m1k = 0x7FFF7FFFu, m2k = 0x7FFF7FFFu;
+  // The two smallest keys (distinct: the tags differ), with the keys taken in pairs:
+  // sort the pair, then merge it into the running (min1, min2).  That is fewer
+  // operations than one key at a time and halves the dependency chain through min1.
+  uint32_t m1k = 0u, m2k = 0u, held = 0u;
   static_for<0, deg>([&](auto ei) {
     constexpr int e = decltype(ei)::value;
     if constexpr (e == ep) {
@@ -252,8 +255,20 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
     // key = |Q| * 256 + tag (the 256 * PB terms cancel mod 2^32)
     const uint32_t aq = vminu2(vmaxu2(qu[e], mad_k(qu[e], 1, 0x00010000u)), 0x807F807Fu);
     const uint32_t key = mad_k(aq, 2, (uint32_t)key_tag(e) * 0x10001u - 0x00800000u);
-    m2k = vminu2(m2k, vmaxu2(m1k, key));
-    m1k = vminu2(m1k, key);
+    if constexpr (e % 2 == 0 && e + 1 < deg) {
+      held = key;
+    } else if constexpr (e % 2 == 1) {
+      const uint32_t lo = vminu2(held, key), hi = vmaxu2(held, key);
+      if constexpr (e == 1) {
+        m1k = lo, m2k = hi;
+      } else {
+        m2k = vminu2(vminu2(m2k, hi), vmaxu2(m1k, lo));
+        m1k = vminu2(m1k, lo);
+      }
+    } else {  // odd degree: the last key alone
+      m2k = vminu2(m2k, vmaxu2(m1k, key));
+      m1k = vminu2(m1k, key);
+    }
   });
   // Row results.  In the key domain, max(key, 256 beta) - 256 beta has byte 1 of each
   // lane = max(min - beta, 0), the offset magnitude; one byte permute gathers
