@@ -145,6 +145,40 @@ int32_t syndrome_ldpc_encode(const SyndromeLdpcEncoder* encoder, const uint8_t* 
 int32_t syndrome_ldpc_encode_batch(const SyndromeLdpcEncoder* encoder, const uint8_t* info_bits,
                                    size_t info_stride, uint8_t* codewords, size_t codeword_stride,
                                    size_t count, int32_t threads);
+/* ------------------------------------ Wi-Fi shortening and puncturing ---- */
+/* src/wifi_rate_matching.rs:88 shortening_and_puncture_counts: n_shrt = k - payload_bits,
+ * n_punc = (n - n_shrt) - target_coded_bits.  INVALID_PARAM when n < k,
+ * payload_bits > k, target_coded_bits < payload_bits or target_coded_bits > n - n_shrt. */
+int32_t syndrome_wifi_shortening_counts(size_t k, size_t n, size_t payload_bits, size_t target_coded_bits,
+                                        size_t* out_n_shrt, size_t* out_n_punc);
+/* src/wifi_rate_matching.rs:163 encode_shortened: payload padded with zeros to K,
+ * encoded, then the payload and the first (N - K) - n_punc parity bits are sent
+ * (out_len == target_coded_bits, else BUFFER_TOO_SMALL). */
+int32_t syndrome_wifi_encode_shortened(const SyndromeLdpcEncoder* encoder, const uint8_t* payload,
+                                       size_t payload_bits, size_t target_coded_bits, uint8_t* out,
+                                       size_t out_len);
+/* src/wifi_rate_matching.rs:267 decode_shortened: codeword_llr (length N, else
+ * BUFFER_TOO_SMALL) is rebuilt from rx_llr (rx_len = target_coded_bits) -- payload,
+ * 1e6 for the shortened bits, the sent parity, 0 for the punctured bits -- and decoded
+ * in place as syndrome_ldpc_decode does (it ends as the posterior).  The payload is
+ * hard_output[0 .. payload_bits). */
+int32_t syndrome_wifi_decode_shortened(SyndromeLdpcDecoder* decoder, size_t payload_bits, const float* rx_llr,
+                                       size_t rx_len, float* codeword_llr, size_t codeword_len,
+                                       float* edge_r, size_t edge_r_len, float* layer_scratch,
+                                       size_t layer_scratch_len, uint8_t* hard_output, size_t hard_output_len,
+                                       size_t iterations, size_t* out_iterations_used);
+/* Batched form on the device: row b of d_rx (d_rx[b * rx_stride + t], t <
+ * target_coded_bits) is one received shortened / punctured codeword; the f32 kernel
+ * rebuilds the full codeword while loading it (no N-length staging buffer).  Outputs
+ * as syndrome_ldpc_decode_batch_f32; the payload is the first payload_bits hard
+ * decisions. */
+int32_t syndrome_wifi_decode_shortened_batch_f32(const SyndromeLdpcDecoder* decoder, const float* d_rx,
+                                                 size_t rx_stride, size_t payload_bits, size_t target_coded_bits,
+                                                 size_t batch, size_t iterations, uint32_t* d_hard_packed,
+                                                 size_t hard_bits, size_t hard_words_stride, int32_t* d_iters,
+                                                 float* d_app, size_t app_stride, float* d_edge_r,
+                                                 size_t edge_r_stride, uint8_t* d_hard, size_t hard_stride,
+                                                 void* d_workspace, size_t workspace_bytes, void* stream);
 /* src/quantize.rs:331 quantize_llr_i16. */
 void syndrome_quantize_llr_i16(const float* llr, int16_t* out, size_t n, float scale);
 /* src/quantize.rs:298 QuantParams::beta_q. */

@@ -14,6 +14,7 @@
 //   * int16 syndrome check      src/qc_ldpc.rs:1766-1787
 //   * 5G int8 prologue          src/qc_ldpc.rs:1486-1523
 //   * quantizer / beta_q        src/quantize.rs:148-155, 298-305, 331-343 (+float_ext.rs round)
+//   * Wi-Fi shortening          src/wifi_rate_matching.rs:88-132, 163-192, 267-302
 //   * encoder                   src/qc_ldpc.rs:2166-2727 (sparse core solve) and :1996-2125 (dense)
 //   * AWGN channel              src/channel_sim.rs:61-241
 //   * DL-SCH transport blocks   segmentation.rs:75-400, crc.rs:65-350, rate_matching.rs:72-700,
@@ -901,6 +902,53 @@ void orc_dlsch_flush(void* h) {
   OrcDlsch* d = static_cast<OrcDlsch*>(h);
   for (auto& a : d->acc) std::fill(a.begin(), a.end(), 0.0f);
   std::fill(d->tx.begin(), d->tx.end(), 0);
+}
+
+}  // extern "C"
+
+// ----------------------------------------------- Wi-Fi shortening / puncturing --
+// src/wifi_rate_matching.rs: shortening_and_puncture_counts :88-132, encode_shortened
+// :163-192, decode_shortened :267-302 (known-zero LLR 1e6 :58).
+extern "C" {
+
+// out2 = {n_shrt, n_punc}; returns 0, or -1 for the reference's InvalidParam cases.
+int orc_wifi_counts(long k, long n, long payload, long target, long* out2) {
+  if (n < k || payload > k || target < payload) return -1;
+  const long shrt = k - payload, max_coded = n - shrt;
+  if (target > max_coded) return -1;
+  out2[0] = shrt;
+  out2[1] = max_coded - target;
+  return 0;
+}
+
+int orc_wifi_encode_shortened(void* h, const uint8_t* payload, long payload_bits, long target, uint8_t* out) {
+  Params* p = static_cast<Params*>(h);
+  const long z = p->z, n = (long)p->nb * z, k = (long)(p->nb - p->mb) * z;
+  long c[2];
+  if (orc_wifi_counts(k, n, payload_bits, target, c) != 0) return -1;
+  std::vector<uint8_t> info((size_t)k, 0), cw((size_t)n, 0);
+  for (long i = 0; i < payload_bits; ++i) info[(size_t)i] = payload[i];
+  if (orc_encode(h, info.data(), cw.data()) != 0) return -1;
+  const long par = (n - k) - c[1];
+  for (long i = 0; i < payload_bits; ++i) out[i] = payload[i];
+  for (long i = 0; i < par; ++i) out[payload_bits + i] = cw[(size_t)(k + i)];
+  return 0;
+}
+
+// Rebuilds codeword_llr[N] from rx[target] and decodes it (f32 LOMS, in place).
+// Returns the iterations used, or -1 for invalid counts.
+long orc_wifi_decode_shortened(const void* h, float beta, long payload_bits, const float* rx, long target,
+                               float* codeword_llr, float* edge_r, uint8_t* hard, long iterations) {
+  const Params* p = static_cast<const Params*>(h);
+  const long z = p->z, n = (long)p->nb * z, k = n - (long)p->mb * z;
+  long c[2];
+  if (orc_wifi_counts(k, n, payload_bits, target, c) != 0) return -1;
+  const long par = (n - k) - c[1];
+  for (long i = 0; i < payload_bits; ++i) codeword_llr[i] = rx[i];
+  for (long i = payload_bits; i < k; ++i) codeword_llr[i] = 1000000.0f;
+  for (long i = 0; i < par; ++i) codeword_llr[k + i] = rx[payload_bits + i];
+  for (long i = k + par; i < n; ++i) codeword_llr[i] = 0.0f;
+  return orc_decode_f32(h, beta, codeword_llr, edge_r, hard, iterations, nullptr);
 }
 
 }  // extern "C"

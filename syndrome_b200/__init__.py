@@ -30,3 +30,4 @@ from .mixed import CODEWORD_DTYPE, LIFTING_SIZES, MixedBatch, code_dims, tile_ca
 __version__ = "0.1.0"
 from .dlsch import DlSchEncoder, SegmentationParams, compute_segmentation, crc24  # noqa: F401,E402
 from .serve import Server  # noqa: F401,E402
+from . import wifi_rate_matching  # noqa: F401,E402

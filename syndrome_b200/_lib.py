@@ -83,6 +83,11 @@ PROTOTYPES = {
     "syndrome_serve_release": (_i32, [_vp, ctypes.c_uint64]),
     "syndrome_serve_stats": (_i32, [_vp, _vp]),
     "syndrome_serve_run_load": (_i32, [_vp, _vp, _sz, _vp, _vp, _vp, _sz]),
+    "syndrome_wifi_shortening_counts": (_i32, [_sz, _sz, _sz, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
+    "syndrome_wifi_encode_shortened": (_i32, [_vp, _vp, _sz, _sz, _vp, _sz]),
+    "syndrome_wifi_decode_shortened": (_i32, [_vp, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _sz, _vp]),
+    "syndrome_wifi_decode_shortened_batch_f32": (_i32, [_vp, _vp, _sz, _sz, _sz, _sz, _sz, _vp, _sz, _sz, _vp, _vp,
+                                                        _sz, _vp, _sz, _vp, _sz, _vp, _sz, _vp]),
     "syndrome_last_error": (ctypes.c_char_p, []),
 }
 

@@ -471,12 +471,13 @@ static int32_t batch_common(const SyndromeLdpcDecoder* decoder, syn::Precision p
                             uint32_t* d_hard_packed, size_t hard_bits, size_t hard_words_stride,
                             int32_t* d_iters, void* d_app, size_t app_stride, void* d_edge_r,
                             size_t edge_r_stride, uint8_t* d_hard, size_t hard_stride,
-                            void* d_workspace, size_t workspace_bytes, void* stream) {
+                            void* d_workspace, size_t workspace_bytes, void* stream,
+                            const long long* shorten = nullptr) {
   if (!decoder || (!d_llr && batch)) return SYNDROME_NULL_POINTER;
   const syn::Graph& g = decoder->graph;
   const size_t n = (size_t)g.n();
   if (llr_offset > n) return fail(SYNDROME_INVALID_PARAM, "llr_offset exceeds N");
-  if (llr_stride < n - llr_offset) return fail(SYNDROME_INVALID_PARAM, "llr_stride smaller than N - llr_offset");
+  if (!shorten && llr_stride < n - llr_offset) return fail(SYNDROME_INVALID_PARAM, "llr_stride smaller than N - llr_offset");
   if (d_app && app_stride < n) return fail(SYNDROME_INVALID_PARAM, "app_stride smaller than N");
   if (d_hard && hard_stride < n) return fail(SYNDROME_INVALID_PARAM, "hard_stride smaller than N");
   if (d_edge_r && edge_r_stride < (size_t)g.edge_buffer())
@@ -508,6 +509,11 @@ static int32_t batch_common(const SyndromeLdpcDecoder* decoder, syn::Precision p
   r.workspace = d_workspace;
   r.workspace_bytes = workspace_bytes;
   r.kernel = decoder->kernel;
+  if (shorten) {
+    r.shorten = 1;
+    r.shorten_payload = shorten[0];
+    r.shorten_tx = shorten[1];
+  }
   std::string msg;
   cudaError_t e = decoder->dec.decode(p, r, static_cast<cudaStream_t>(stream), &msg);
   return from_cuda(e, msg);
@@ -590,6 +596,99 @@ int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const
                         nr_prologue, n_filler, iterations, 8.0f, 0, d_hard_packed, hard_bits,
                         hard_words_stride, d_iters, d_app, app_stride, d_edge_r, edge_r_stride, d_hard,
                         hard_stride, d_workspace, workspace_bytes, stream);
+  });
+}
+
+// ------------------------------------------- Wi-Fi shortening / puncturing ---
+// src/wifi_rate_matching.rs:88-132 (counts), :163-192 (encode), :267-302 (decode).
+
+static int32_t wifi_counts(size_t k, size_t n, size_t payload, size_t target, size_t* n_shrt, size_t* n_punc) {
+  if (n < k) return fail(SYNDROME_INVALID_PARAM, "codeword length N must be at least the information length K");
+  if (payload > k)
+    return fail(SYNDROME_INVALID_PARAM,
+                "payload_bits exceeds this codeword's K; multi-codeword segmentation is not implemented");
+  if (target < payload)
+    return fail(SYNDROME_INVALID_PARAM, "target_coded_bits must be at least payload_bits");
+  const size_t shrt = k - payload, max_coded = n - shrt;
+  if (target > max_coded) return fail(SYNDROME_INVALID_PARAM, "target_coded_bits exceeds N - n_shrt");
+  *n_shrt = shrt;
+  *n_punc = max_coded - target;
+  return SYNDROME_OK;
+}
+
+int32_t syndrome_wifi_shortening_counts(size_t k, size_t n, size_t payload_bits, size_t target_coded_bits,
+                                        size_t* out_n_shrt, size_t* out_n_punc) {
+  return guard([&]() -> int32_t {
+    if (!out_n_shrt || !out_n_punc) return SYNDROME_NULL_POINTER;
+    return wifi_counts(k, n, payload_bits, target_coded_bits, out_n_shrt, out_n_punc);
+  });
+}
+
+int32_t syndrome_wifi_encode_shortened(const SyndromeLdpcEncoder* encoder, const uint8_t* payload,
+                                       size_t payload_bits, size_t target_coded_bits, uint8_t* out,
+                                       size_t out_len) {
+  return guard([&]() -> int32_t {
+    if (!encoder || (!payload && payload_bits) || !out) return SYNDROME_NULL_POINTER;
+    const syn::Graph& g = encoder->enc.graph();
+    const size_t k = (size_t)g.k(), n = (size_t)g.n();
+    size_t shrt = 0, punc = 0;
+    int32_t st = wifi_counts(k, n, payload_bits, target_coded_bits, &shrt, &punc);
+    if (st != SYNDROME_OK) return st;
+    if (out_len != target_coded_bits) return fail(SYNDROME_BUFFER_TOO_SMALL, "out length must equal target_coded_bits");
+    std::vector<uint8_t> info(k, 0), cw(n);
+    std::copy(payload, payload + payload_bits, info.begin());
+    encoder->enc.encode(info.data(), cw.data());
+    const size_t par = (n - k) - punc;
+    std::copy(payload, payload + payload_bits, out);
+    std::copy(cw.begin() + k, cw.begin() + k + par, out + payload_bits);
+    return SYNDROME_OK;
+  });
+}
+
+int32_t syndrome_wifi_decode_shortened(SyndromeLdpcDecoder* decoder, size_t payload_bits, const float* rx_llr,
+                                       size_t rx_len, float* codeword_llr, size_t codeword_len,
+                                       float* edge_r, size_t edge_r_len, float* layer_scratch,
+                                       size_t layer_scratch_len, uint8_t* hard_output, size_t hard_output_len,
+                                       size_t iterations, size_t* out_iterations_used) {
+  return guard([&]() -> int32_t {
+    if (!decoder || (!rx_llr && rx_len) || !codeword_llr || !edge_r || !layer_scratch || !hard_output)
+      return SYNDROME_NULL_POINTER;
+    const syn::Graph& g = decoder->graph;
+    const size_t n = (size_t)g.n(), k = n - (size_t)g.m();
+    size_t shrt = 0, punc = 0;
+    int32_t st = wifi_counts(k, n, payload_bits, rx_len, &shrt, &punc);
+    if (st != SYNDROME_OK) return st;
+    if (codeword_len != n) return fail(SYNDROME_BUFFER_TOO_SMALL, "codeword_llr length must equal N");
+    const size_t par = (n - k) - punc;
+    std::copy(rx_llr, rx_llr + payload_bits, codeword_llr);
+    std::fill(codeword_llr + payload_bits, codeword_llr + k, 1000000.0f);
+    std::copy(rx_llr + payload_bits, rx_llr + payload_bits + par, codeword_llr + k);
+    std::fill(codeword_llr + k + par, codeword_llr + n, 0.0f);
+    st = validate_buffers(g, codeword_len, hard_output_len, edge_r_len, layer_scratch_len);
+    if (st != SYNDROME_OK) return st;
+    return host_decode(decoder, true, codeword_llr, edge_r, hard_output, iterations, 8.0f, 0, out_iterations_used);
+  });
+}
+
+int32_t syndrome_wifi_decode_shortened_batch_f32(const SyndromeLdpcDecoder* decoder, const float* d_rx,
+                                                 size_t rx_stride, size_t payload_bits, size_t target_coded_bits,
+                                                 size_t batch, size_t iterations, uint32_t* d_hard_packed,
+                                                 size_t hard_bits, size_t hard_words_stride, int32_t* d_iters,
+                                                 float* d_app, size_t app_stride, float* d_edge_r,
+                                                 size_t edge_r_stride, uint8_t* d_hard, size_t hard_stride,
+                                                 void* d_workspace, size_t workspace_bytes, void* stream) {
+  return guard([&]() -> int32_t {
+    if (!decoder) return SYNDROME_NULL_POINTER;
+    const syn::Graph& g = decoder->graph;
+    const size_t n = (size_t)g.n(), k = n - (size_t)g.m();
+    size_t shrt = 0, punc = 0;
+    int32_t st = wifi_counts(k, n, payload_bits, target_coded_bits, &shrt, &punc);
+    if (st != SYNDROME_OK) return st;
+    if (rx_stride < target_coded_bits) return fail(SYNDROME_INVALID_PARAM, "rx_stride smaller than target_coded_bits");
+    const long long sh[2] = {(long long)payload_bits, (long long)target_coded_bits};
+    return batch_common(decoder, syn::Precision::kF32, d_rx, rx_stride, 0, batch, 0, 0, iterations, 8.0f, 0,
+                        d_hard_packed, hard_bits, hard_words_stride, d_iters, d_app, app_stride, d_edge_r,
+                        edge_r_stride, d_hard, hard_stride, d_workspace, workspace_bytes, stream, sh);
   });
 }
 

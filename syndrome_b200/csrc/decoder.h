@@ -29,6 +29,15 @@ struct BatchRequest {
   int iterations = 0;
   int prologue_5g = 0;
   long long n_filler = 0;
+  // f32 path, Wi-Fi shortening and puncturing (src/wifi_rate_matching.rs:267-302): with
+  // shorten set, row b holds the shorten_tx transmitted LLRs of codeword b, the
+  // shorten_payload real information bits then the parity bits that were sent; the
+  // decode starts from variables [0, P) = the payload, [P, K) = 1e6 (shortened,
+  // known zero), [K, K + T - P) = the sent parity and the rest = 0 (punctured).
+  // llr_offset must be 0 and prologue_5g off.
+  int shorten = 0;
+  long long shorten_payload = 0;
+  long long shorten_tx = 0;
   // int8 path numerics (src/quantize.rs): beta_q = round(beta * scale) clamped, app clamp.
   int beta_q = 0;
   int app_clamp = 32767;

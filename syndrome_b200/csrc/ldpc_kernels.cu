@@ -54,6 +54,9 @@ struct KArgs {
   float beta;
   int prologue;
   long long k_prime;      // filler positions are [k_prime, k)
+  int shorten;            // f32: Wi-Fi shortened / punctured rows (BatchRequest::shorten)
+  long long sh_pay;       // payload bits P
+  long long sh_par_end;   // K + transmitted parity bits
   void* r_out;            // C->V messages of codeword b at r_out + b * r_out_stride
   long long r_out_stride;
   void* r_ws;             // else per (CTA, slot) scratch
@@ -331,6 +334,17 @@ __global__ void __launch_bounds__(kMaxThreads) loms_f32_kernel(const KArgs a) {
           else if (j >= a.k_prime && j < a.k)
             v = 1000000.0f;
         }
+        if (a.shorten) {
+          // the row holds the sent bits only: payload, then the parity that was not punctured
+          if (j < a.sh_pay)
+            v = src[j];
+          else if (j < a.k)
+            v = 1000000.0f;  // shortened: known zero (LLR_KNOWN_ZERO, wifi_rate_matching.rs:58)
+          else if (j < a.sh_par_end)
+            v = src[j - (a.k - a.sh_pay)];
+          else
+            v = 0.0f;  // punctured: erasure
+        }
         dst[j] = v;
       }
     }
@@ -507,6 +521,14 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
                           req.hard_words_stride < (req.hard_bits + 31) / 32))
     return bad("hard_bits / hard_words_stride out of range");
   if (req.app_clamp < 0 && p == Precision::kInt8) return bad("app_clamp must be non-negative");
+  if (req.shorten) {
+    if (p != Precision::kF32) return bad("shortened / punctured decodes are f32");
+    if (req.llr_offset != 0 || req.prologue_5g) return bad("a shortened decode takes no llr_offset or 5G prologue");
+    if (req.shorten_payload < 0 || req.shorten_payload > g_.k() || req.shorten_tx < req.shorten_payload ||
+        req.shorten_tx > g_.n() - (g_.k() - req.shorten_payload))
+      return bad("payload / transmitted bit counts out of range");
+    if (req.llr_stride < req.shorten_tx) return bad("llr_stride smaller than the transmitted bits");
+  }
   const bool nr_ok = p == Precision::kInt8 && nr_bg_ >= 0 && !req.llr_i16 && req.app_clamp >= 255;
   if ((req.kernel == 2 || req.kernel == 3) && !nr_ok) return bad("the 5G NR kernel does not apply to this request");
   if (nr_ok && req.kernel != 1) {
@@ -566,6 +588,9 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
   a.beta = req.beta;
   a.prologue = req.prologue_5g;
   a.k_prime = req.n_filler > g_.k() ? 0 : g_.k() - req.n_filler;
+  a.shorten = req.shorten;
+  a.sh_pay = req.shorten_payload;
+  a.sh_par_end = g_.k() + (req.shorten_tx - req.shorten_payload);
   a.r_out = req.edge_r;
   a.r_out_stride = req.edge_r_stride;
   a.r_ws = req.workspace;

@@ -250,3 +250,39 @@ class DlSchDecoder:
 
     def flush(self):
         lib().orc_dlsch_flush(self.h)
+
+
+# ---- Wi-Fi shortening / puncturing (src/wifi_rate_matching.rs) ----
+def wifi_counts(k, n, payload, target):
+    out = np.zeros(2, dtype=np.int64)
+    L = lib()
+    L.orc_wifi_counts.argtypes = [ctypes.c_long] * 4 + [ctypes.c_void_p]
+    rc = L.orc_wifi_counts(k, n, payload, target, out.ctypes.data)
+    return None if rc != 0 else (int(out[0]), int(out[1]))
+
+
+def wifi_encode_shortened(code, payload, target):
+    payload = np.ascontiguousarray(payload, dtype=np.uint8)
+    out = np.zeros(target, dtype=np.uint8)
+    L = lib()
+    L.orc_wifi_encode_shortened.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_long,
+                                            ctypes.c_void_p]
+    rc = L.orc_wifi_encode_shortened(code.h, payload.ctypes.data, payload.size, target, out.ctypes.data)
+    assert rc == 0
+    return out
+
+
+def wifi_decode_shortened(code, beta, payload_bits, rx, iterations):
+    rx = np.ascontiguousarray(rx, dtype=np.float32)
+    cw = np.zeros(code.n, dtype=np.float32)
+    edge_r = np.zeros(code.edges * code.z, dtype=np.float32)
+    hard = np.zeros(code.n, dtype=np.uint8)
+    L = lib()
+    L.orc_wifi_decode_shortened.restype = ctypes.c_long
+    L.orc_wifi_decode_shortened.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_long, ctypes.c_void_p,
+                                            ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_long]
+    used = L.orc_wifi_decode_shortened(code.h, beta, payload_bits, rx.ctypes.data, rx.size, cw.ctypes.data,
+                                       edge_r.ctypes.data, hard.ctypes.data, iterations)
+    assert used >= 0
+    return dict(iters=int(used), llr=cw, edge_r=edge_r, hard=hard)
