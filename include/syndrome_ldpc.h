@@ -193,6 +193,36 @@ void syndrome_awgn_quantized_batch(const uint8_t* bits, size_t n, size_t bits_st
                                    const uint64_t* seeds, float scale, int8_t* out,
                                    size_t out_stride, size_t count, int32_t threads);
 
+/* ------------------------------------------------------ frame pipeline ---- */
+/* src/ldpc_pipeline.rs:288-598 LdpcPipeline.  A pool of N-length f32 frames in pinned
+ * host memory: acquire a frame (its index; -1 when every frame is in use), fill its
+ * LLRs, submit it; host worker threads (n_workers, clamped to 1..8; 0 = one per core
+ * as LdpcPipeline::new, clamped the same way) decode submitted frames in batches on
+ * their own CUDA streams (decode_layered_offset_min_sum: the frame's LLRs become the
+ * posterior, hard decisions and iterations used are filled in); try_recv returns
+ * decoded frames in completion order (-1 when none is ready), release returns a
+ * frame to the pool.  The pool holds 256 frames (the reference's 16 is too few to
+ * keep a GPU busy).  The decoder must outlive the pipeline. */
+typedef struct SyndromeLdpcPipeline SyndromeLdpcPipeline;
+int32_t syndrome_ldpc_pipeline_create(const SyndromeLdpcDecoder* decoder, size_t iterations, size_t n_workers,
+                                      SyndromeLdpcPipeline** out_pipeline);
+void syndrome_ldpc_pipeline_destroy(SyndromeLdpcPipeline* pipeline);
+size_t syndrome_ldpc_pipeline_worker_count(const SyndromeLdpcPipeline* pipeline);
+size_t syndrome_ldpc_pipeline_pool_size(const SyndromeLdpcPipeline* pipeline);
+int64_t syndrome_ldpc_pipeline_acquire(SyndromeLdpcPipeline* pipeline);
+/* INVALID_PARAM unless the frame was acquired and not yet submitted. */
+int32_t syndrome_ldpc_pipeline_submit(SyndromeLdpcPipeline* pipeline, int64_t frame);
+int64_t syndrome_ldpc_pipeline_try_recv(SyndromeLdpcPipeline* pipeline);
+/* INVALID_PARAM unless the frame was received (or acquired and not submitted). */
+int32_t syndrome_ldpc_pipeline_release(SyndromeLdpcPipeline* pipeline, int64_t frame);
+/* LdpcFrame accessors: N f32 LLRs (the posterior after decoding), N hard decisions,
+ * iterations used, the caller's tag.  NULL / 0 for an invalid frame index. */
+float* syndrome_ldpc_pipeline_frame_llr(SyndromeLdpcPipeline* pipeline, int64_t frame);
+const uint8_t* syndrome_ldpc_pipeline_frame_hard(const SyndromeLdpcPipeline* pipeline, int64_t frame);
+size_t syndrome_ldpc_pipeline_frame_iterations(const SyndromeLdpcPipeline* pipeline, int64_t frame);
+void syndrome_ldpc_pipeline_frame_set_tag(SyndromeLdpcPipeline* pipeline, int64_t frame, size_t tag);
+size_t syndrome_ldpc_pipeline_frame_tag(const SyndromeLdpcPipeline* pipeline, int64_t frame);
+
 /* ================================================= 3. batched device API == */
 
 /* Device scratch bytes that syndrome_ldpc_decode_batch_* needs for `batch`
@@ -326,6 +356,36 @@ size_t syndrome_dlsch_encoder_num_code_blocks(const SyndromeDlSchEncoder* encode
  * out_len be at least output_bits (BUFFER_TOO_SMALL); rv > 3 is INVALID_PARAM. */
 int32_t syndrome_dlsch_encode(const SyndromeDlSchEncoder* encoder, const uint8_t* tb, size_t tb_len,
                               size_t rv, uint8_t* out, size_t out_len);
+/* src/transport_block.rs:405-1060 DlSchDecoder with the f32 code-block decode: HARQ
+ * f32 soft combining into device accumulators, the 5G prologue, all C code blocks
+ * decoded in one batched f32 launch (decode_layered_offset_min_sum), CB CRC-24B, TB
+ * CRC-24A, HARQ flush on success.  create: INVALID_PARAM for tb_size 0, Qm or G 0 or
+ * G % Qm != 0, or a TB size segmentation rejects (transport_block.rs:612-627). */
+typedef struct SyndromeDlSchDecoder SyndromeDlSchDecoder;
+typedef struct {
+  int32_t crc_ok;          /* TB CRC-24A and every CB CRC-24B passed */
+  int32_t max_iters_used;  /* largest iteration count over the code blocks */
+  int32_t harq_tx_count;   /* transmissions combined, this one included */
+  int32_t num_code_blocks;
+} SyndromeDecodeReport;
+int32_t syndrome_dlsch_decoder_create(size_t tb_size, float target_rate, size_t qm, size_t g, size_t iterations,
+                                      float offset_beta, SyndromeDlSchDecoder** out_decoder);
+void syndrome_dlsch_decoder_destroy(SyndromeDlSchDecoder* decoder);
+size_t syndrome_dlsch_decoder_num_code_blocks(const SyndromeDlSchDecoder* decoder);
+size_t syndrome_dlsch_decoder_output_bits(const SyndromeDlSchDecoder* decoder);
+/* :729 with_pipeline.  Accepted for API parity (INVALID_PARAM for 0): every decode
+ * already runs its code blocks concurrently in one batched GPU launch; the count is
+ * what worker_count reports (0 before any with_pipeline call). */
+int32_t syndrome_dlsch_decoder_with_pipeline(SyndromeDlSchDecoder* decoder, size_t n_workers);
+size_t syndrome_dlsch_decoder_worker_count(const SyndromeDlSchDecoder* decoder);
+/* :829 decode.  rx_llr holds C * E f32 LLRs (else BUFFER_TOO_SMALL), tb_len >= tb_size
+ * (else BUFFER_TOO_SMALL), rv 0..3.  tb_out is written only when crc_ok.  cb_crc
+ * (nullable, cb_crc_len >= C) receives each code block's CRC-24B result. */
+int32_t syndrome_dlsch_decode(SyndromeDlSchDecoder* decoder, const float* rx_llr, size_t rx_len, size_t rv,
+                              uint8_t* tb_out, size_t tb_len, SyndromeDecodeReport* report, uint8_t* cb_crc,
+                              size_t cb_crc_len);
+/* :1055 flush_harq. */
+void syndrome_dlsch_decoder_flush_harq(SyndromeDlSchDecoder* decoder);
 
 /* ============================================ 5. transport-block serving ===== */
 /* A device-resident serving engine for DL-SCH transmissions.  No single counterpart

@@ -750,6 +750,8 @@ struct OrcDlsch {
   void* params;
   std::vector<std::vector<float>> acc;
   std::vector<int> tx;
+  int f32 = 0;        // the reference's own f32 code-block decode (orc_dlsch_set_f32)
+  float beta = 0.0f;
 };
 
 extern "C" {
@@ -860,6 +862,13 @@ int orc_dlsch_decode(void* h, const float* rx, int rv, uint8_t* tb_out, int* rep
     d->tx[ci] += 1;
     std::fill(llr.begin(), llr.end(), 0.0f);
     std::copy(acc.begin(), acc.end(), llr.begin() + 2 * z);
+    if (d->f32) {  // prepare_cb_llr + decode_layered_offset_min_sum (transport_block.rs:473-496, 555)
+      orc_init_5g_f32(d->params, llr.data(), s.nf);
+      std::vector<float> er((size_t)(static_cast<Params*>(d->params)->cols.size() * z));
+      const long it = orc_decode_f32(d->params, d->beta, llr.data(), er.data(), hard.data(), d->iterations, nullptr);
+      if (iters_out) iters_out[ci] = (int)it;
+      max_iters = std::max(max_iters, (int)it);
+    } else {
     orc_quantize_i16(llr.data(), app.data(), n, d->scale);
     if (llr_out)
       for (long j = 0; j < s.n; ++j) llr_out[(long)ci * s.n + j] = (int8_t)app[2 * z + j];
@@ -869,6 +878,7 @@ int orc_dlsch_decode(void* h, const float* rx, int rv, uint8_t* tb_out, int* rep
                                   d->iterations);
     if (iters_out) iters_out[ci] = (int)it;
     max_iters = std::max(max_iters, (int)it);
+    }
     bool ok = true;
     if (s.has_crc) {  // crc.rs check: payload CRC against the trailing 24 bits
       uint32_t rec = 0;
@@ -896,6 +906,14 @@ int orc_dlsch_decode(void* h, const float* rx, int rv, uint8_t* tb_out, int* rep
   report4[2] = harq_tx;
   report4[3] = s.c;
   return 0;
+}
+
+// Switches the decoder to the f32 code-block decode with offset beta (the reference's
+// DlSchDecoder, transport_block.rs:829-1053); llr_out is not written then.
+void orc_dlsch_set_f32(void* h, float beta) {
+  OrcDlsch* d = static_cast<OrcDlsch*>(h);
+  d->f32 = 1;
+  d->beta = beta;
 }
 
 void orc_dlsch_flush(void* h) {

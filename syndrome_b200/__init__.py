@@ -28,6 +28,7 @@ from .qc_ldpc import (  # noqa: F401
 from .mixed import CODEWORD_DTYPE, LIFTING_SIZES, MixedBatch, code_dims, tile_capacity  # noqa: F401,E402
 
 __version__ = "0.1.0"
-from .dlsch import DlSchEncoder, SegmentationParams, compute_segmentation, crc24  # noqa: F401,E402
+from .dlsch import DecodeReport, DlSchDecoder, DlSchEncoder, SegmentationParams, compute_segmentation, crc24  # noqa: F401,E402
 from .serve import Server  # noqa: F401,E402
 from . import wifi_rate_matching  # noqa: F401,E402
+from .ldpc_pipeline import LdpcFrame, LdpcPipeline  # noqa: F401,E402

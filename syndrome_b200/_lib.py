@@ -88,6 +88,27 @@ PROTOTYPES = {
     "syndrome_wifi_decode_shortened": (_i32, [_vp, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _sz, _vp]),
     "syndrome_wifi_decode_shortened_batch_f32": (_i32, [_vp, _vp, _sz, _sz, _sz, _sz, _sz, _vp, _sz, _sz, _vp, _vp,
                                                         _sz, _vp, _sz, _vp, _sz, _vp, _sz, _vp]),
+    "syndrome_dlsch_decoder_create": (_i32, [_sz, _f32, _sz, _sz, _sz, _f32, ctypes.POINTER(_vp)]),
+    "syndrome_dlsch_decoder_destroy": (None, [_vp]),
+    "syndrome_dlsch_decoder_num_code_blocks": (_sz, [_vp]),
+    "syndrome_dlsch_decoder_output_bits": (_sz, [_vp]),
+    "syndrome_dlsch_decoder_with_pipeline": (_i32, [_vp, _sz]),
+    "syndrome_dlsch_decoder_worker_count": (_sz, [_vp]),
+    "syndrome_dlsch_decode": (_i32, [_vp, _vp, _sz, _sz, _vp, _sz, _vp, _vp, _sz]),
+    "syndrome_dlsch_decoder_flush_harq": (None, [_vp]),
+    "syndrome_ldpc_pipeline_create": (_i32, [_vp, _sz, _sz, ctypes.POINTER(_vp)]),
+    "syndrome_ldpc_pipeline_destroy": (None, [_vp]),
+    "syndrome_ldpc_pipeline_worker_count": (_sz, [_vp]),
+    "syndrome_ldpc_pipeline_pool_size": (_sz, [_vp]),
+    "syndrome_ldpc_pipeline_acquire": (ctypes.c_int64, [_vp]),
+    "syndrome_ldpc_pipeline_submit": (_i32, [_vp, ctypes.c_int64]),
+    "syndrome_ldpc_pipeline_try_recv": (ctypes.c_int64, [_vp]),
+    "syndrome_ldpc_pipeline_release": (_i32, [_vp, ctypes.c_int64]),
+    "syndrome_ldpc_pipeline_frame_llr": (_vp, [_vp, ctypes.c_int64]),
+    "syndrome_ldpc_pipeline_frame_hard": (_vp, [_vp, ctypes.c_int64]),
+    "syndrome_ldpc_pipeline_frame_iterations": (_sz, [_vp, ctypes.c_int64]),
+    "syndrome_ldpc_pipeline_frame_set_tag": (None, [_vp, ctypes.c_int64, _sz]),
+    "syndrome_ldpc_pipeline_frame_tag": (_sz, [_vp, ctypes.c_int64]),
     "syndrome_last_error": (ctypes.c_char_p, []),
 }
 

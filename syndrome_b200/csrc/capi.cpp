@@ -12,12 +12,14 @@
 #include <exception>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/syndrome_ldpc.h"
 #include "channel.h"
 #include "decoder.h"
 #include "encoder.h"
+#include "frames.h"
 #include "graph.h"
 #include "mixed.h"
 #include "serve.h"
@@ -820,6 +822,135 @@ int32_t syndrome_dlsch_encode(const SyndromeDlSchEncoder* e, const uint8_t* tb, 
     e->enc.encode(tb, (int)rv, out);
     return SYNDROME_OK;
   });
+}
+
+// ------------------------------------------------ DL-SCH decoder (f32) -----
+
+struct SyndromeDlSchDecoder {
+  syn::DlSchF32 d;
+  size_t workers = 0;
+};
+
+int32_t syndrome_dlsch_decoder_create(size_t tb_size, float target_rate, size_t qm, size_t g, size_t iterations,
+                                      float offset_beta, SyndromeDlSchDecoder** out) {
+  return guard([&]() -> int32_t {
+    if (!out) return SYNDROME_NULL_POINTER;
+    *out = nullptr;
+    if (tb_size > (size_t)syn::kMaxTbBits * 2 || qm > 64 || g > ((size_t)1 << 40) || iterations > (size_t)INT_MAX)
+      return fail(SYNDROME_INVALID_PARAM, "size out of range");
+    auto* d = new SyndromeDlSchDecoder();
+    std::string err;
+    if (!d->d.init((long long)tb_size, target_rate, (int)qm, (long long)g, (int)iterations, offset_beta, &err)) {
+      delete d;
+      cudaGetLastError();
+      return fail(err.rfind("CUDA ", 0) == 0 ? SYNDROME_CUDA_ERROR : SYNDROME_INVALID_PARAM, err);
+    }
+    *out = d;
+    return SYNDROME_OK;
+  });
+}
+
+void syndrome_dlsch_decoder_destroy(SyndromeDlSchDecoder* d) { delete d; }
+size_t syndrome_dlsch_decoder_num_code_blocks(const SyndromeDlSchDecoder* d) { return d ? (size_t)d->d.params().c : 0; }
+size_t syndrome_dlsch_decoder_output_bits(const SyndromeDlSchDecoder* d) { return d ? (size_t)d->d.output_bits() : 0; }
+
+int32_t syndrome_dlsch_decoder_with_pipeline(SyndromeDlSchDecoder* d, size_t n_workers) {
+  return guard([&]() -> int32_t {
+    if (!d) return SYNDROME_NULL_POINTER;
+    if (n_workers == 0) return fail(SYNDROME_INVALID_PARAM, "n_workers must be > 0");
+    d->workers = std::min<size_t>(n_workers, 8);
+    return SYNDROME_OK;
+  });
+}
+
+size_t syndrome_dlsch_decoder_worker_count(const SyndromeDlSchDecoder* d) { return d ? d->workers : 0; }
+
+int32_t syndrome_dlsch_decode(SyndromeDlSchDecoder* d, const float* rx, size_t rx_len, size_t rv, uint8_t* tb_out,
+                              size_t tb_len, SyndromeDecodeReport* report, uint8_t* cb_crc, size_t cb_crc_len) {
+  return guard([&]() -> int32_t {
+    if (!d || (!rx && rx_len) || !tb_out || !report) return SYNDROME_NULL_POINTER;
+    const int c = d->d.params().c;
+    if (cb_crc && cb_crc_len < (size_t)c) return fail(SYNDROME_BUFFER_TOO_SMALL, "cb_crc shorter than C");
+    if (rv > 3) return fail(SYNDROME_INVALID_PARAM, "rv must be 0..3");
+    std::vector<uint8_t> cbs((size_t)c);
+    int rep[3] = {0, 0, 0};
+    std::string err;
+    const int st = d->d.decode(rx, (long long)std::min<size_t>(rx_len, (size_t)LLONG_MAX), (int)rv, tb_out,
+                               (long long)std::min<size_t>(tb_len, (size_t)LLONG_MAX), rep, cbs.data(), &err);
+    if (st != SYNDROME_OK) return fail(st, err);
+    report->crc_ok = rep[0];
+    report->max_iters_used = rep[1];
+    report->harq_tx_count = rep[2];
+    report->num_code_blocks = c;
+    if (cb_crc) std::copy(cbs.begin(), cbs.end(), cb_crc);
+    return SYNDROME_OK;
+  });
+}
+
+void syndrome_dlsch_decoder_flush_harq(SyndromeDlSchDecoder* d) {
+  if (d) d->d.flush();
+}
+
+// ------------------------------------------------------- frame pipeline -----
+
+struct SyndromeLdpcPipeline {
+  syn::FramePipe p;
+};
+
+int32_t syndrome_ldpc_pipeline_create(const SyndromeLdpcDecoder* decoder, size_t iterations, size_t n_workers,
+                                      SyndromeLdpcPipeline** out) {
+  return guard([&]() -> int32_t {
+    if (!decoder || !out) return SYNDROME_NULL_POINTER;
+    *out = nullptr;
+    if (iterations > (size_t)INT_MAX) return fail(SYNDROME_INVALID_PARAM, "iterations out of range");
+    int w = (int)std::min<size_t>(n_workers, 8);
+    if (w == 0) w = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    auto* p = new SyndromeLdpcPipeline();
+    std::string err;
+    if (!p->p.init(decoder->graph, &decoder->dec, (int)iterations, w, &err)) {
+      delete p;
+      cudaGetLastError();
+      return fail(SYNDROME_CUDA_ERROR, err);
+    }
+    *out = p;
+    return SYNDROME_OK;
+  });
+}
+
+void syndrome_ldpc_pipeline_destroy(SyndromeLdpcPipeline* p) { delete p; }
+size_t syndrome_ldpc_pipeline_worker_count(const SyndromeLdpcPipeline* p) { return p ? (size_t)p->p.workers() : 0; }
+size_t syndrome_ldpc_pipeline_pool_size(const SyndromeLdpcPipeline*) { return (size_t)syn::FramePipe::kPool; }
+int64_t syndrome_ldpc_pipeline_acquire(SyndromeLdpcPipeline* p) { return p ? p->p.acquire() : -1; }
+int64_t syndrome_ldpc_pipeline_try_recv(SyndromeLdpcPipeline* p) { return p ? p->p.try_recv() : -1; }
+
+int32_t syndrome_ldpc_pipeline_submit(SyndromeLdpcPipeline* p, int64_t f) {
+  if (!p) return SYNDROME_NULL_POINTER;
+  if (f < 0 || f >= syn::FramePipe::kPool || !p->p.submit((int)f))
+    return fail(SYNDROME_INVALID_PARAM, "not an acquired frame");
+  return SYNDROME_OK;
+}
+
+int32_t syndrome_ldpc_pipeline_release(SyndromeLdpcPipeline* p, int64_t f) {
+  if (!p) return SYNDROME_NULL_POINTER;
+  if (f < 0 || f >= syn::FramePipe::kPool || !p->p.release((int)f))
+    return fail(SYNDROME_INVALID_PARAM, "not a received or acquired frame");
+  return SYNDROME_OK;
+}
+
+float* syndrome_ldpc_pipeline_frame_llr(SyndromeLdpcPipeline* p, int64_t f) {
+  return p && p->p.valid((int)f) && f == (int)f ? p->p.llr((int)f) : nullptr;
+}
+const uint8_t* syndrome_ldpc_pipeline_frame_hard(const SyndromeLdpcPipeline* p, int64_t f) {
+  return p && p->p.valid((int)f) && f == (int)f ? p->p.hard((int)f) : nullptr;
+}
+size_t syndrome_ldpc_pipeline_frame_iterations(const SyndromeLdpcPipeline* p, int64_t f) {
+  return p && p->p.valid((int)f) && f == (int)f ? (size_t)p->p.iterations_used((int)f) : 0;
+}
+void syndrome_ldpc_pipeline_frame_set_tag(SyndromeLdpcPipeline* p, int64_t f, size_t tag) {
+  if (p && p->p.valid((int)f) && f == (int)f) p->p.tag((int)f) = tag;
+}
+size_t syndrome_ldpc_pipeline_frame_tag(const SyndromeLdpcPipeline* p, int64_t f) {
+  return p && p->p.valid((int)f) && f == (int)f ? const_cast<syn::FramePipe&>(p->p).tag((int)f) : 0;
 }
 
 // ----------------------------------------------------------------- serving ---

@@ -91,7 +91,7 @@ __global__ void serve_combine_kernel(const ServeCb* __restrict__ cbs, float scal
   if (p >= cb.ncb) return;
   if (p >= cb.fs && p < cb.fe) {  // filler positions: never transmitted, decoder pins them
     if (cb.first) cb.acc[p] = 0.0f;
-    cb.llr[p] = 0;
+    if (cb.llr) cb.llr[p] = 0;
     return;
   }
   const int c = p < cb.fs ? p : p - (cb.fe - cb.fs);
@@ -117,6 +117,7 @@ __global__ void serve_combine_kernel(const ServeCb* __restrict__ cbs, float scal
     for (int i = 0; i < n; ++i) a = __fadd_rn(a, cb.e[q[i]]);
   }
   cb.acc[p] = a;
+  if (!cb.llr) return;  // f32 decode: the accumulator is the decoder input
   const float v = __fmul_rn(a, scale);
   int qv = 0;
   if (!isnan(v)) qv = (int)fminf(fmaxf(roundf(v), -127.0f), 127.0f);

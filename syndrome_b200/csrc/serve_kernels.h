@@ -11,7 +11,7 @@ namespace syn {
 struct ServeCb {
   float* acc;            // HARQ accumulator, ncb floats (circular buffer, variables 2Z..N)
   const float* e;        // received LLRs of this code block (e_len floats, interleaved order)
-  int8_t* llr;           // decoder input: ncb int8 values (variables 2Z..N)
+  int8_t* llr;           // decoder input: ncb int8 values (variables 2Z..N); null = f32 (acc only)
   const uint32_t* hard;  // decoder output: K' hard decisions, LSB-first words
   int ncb, fs, fe, m, c0;  // rate-matching walk (see tb.h RmWalk)
   int e_len, qm;

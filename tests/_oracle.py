@@ -223,9 +223,12 @@ class DlSchDecoder:
     """transport_block.rs DlSchDecoder with the int8 code-block decode (HARQ f32 sum,
     quantize_llr_i16, decode_5g_i8)."""
 
-    def __init__(self, tb_size, rate, qm, g, iterations=8, beta_q=4, scale=8.0, app_clamp=32767):
+    def __init__(self, tb_size, rate, qm, g, iterations=8, beta_q=4, scale=8.0, app_clamp=32767, f32_beta=None):
         self.h = lib().orc_dlsch_decoder_new(tb_size, rate, qm, g, iterations, beta_q, scale, app_clamp)
         assert self.h
+        if f32_beta is not None:  # the reference's own f32 code-block decode
+            lib().orc_dlsch_set_f32.argtypes = [ctypes.c_void_p, ctypes.c_float]
+            lib().orc_dlsch_set_f32(self.h, f32_beta)
         self.tb_size = tb_size
         self.seg = segmentation(tb_size, rate)
 
