@@ -179,6 +179,14 @@ int32_t syndrome_wifi_decode_shortened_batch_f32(const SyndromeLdpcDecoder* deco
                                                  float* d_app, size_t app_stride, float* d_edge_r,
                                                  size_t edge_r_stride, uint8_t* d_hard, size_t hard_stride,
                                                  void* d_workspace, size_t workspace_bytes, void* stream);
+/* The same batch encoded on the GPU (src/qc_ldpc.rs:2592-2727 codewords, which are
+ * unique): d_info [count][info_stride] and d_codewords [count][codeword_stride] are
+ * device arrays, one bit per byte; enqueued on `stream` (cudaStream_t, NULL = legacy
+ * default stream).  The encoder's tables are copied to the current device on the
+ * first call; later calls must use the same device (else CUDA_ERROR). */
+int32_t syndrome_ldpc_encode_batch_device(const SyndromeLdpcEncoder* encoder, const uint8_t* d_info,
+                                          size_t info_stride, uint8_t* d_codewords, size_t codeword_stride,
+                                          size_t count, void* stream);
 /* src/quantize.rs:331 quantize_llr_i16. */
 void syndrome_quantize_llr_i16(const float* llr, int16_t* out, size_t n, float scale);
 /* src/quantize.rs:298 QuantParams::beta_q. */

@@ -424,6 +424,22 @@ int32_t syndrome_ldpc_encode(const SyndromeLdpcEncoder* encoder, const uint8_t* 
   });
 }
 
+int32_t syndrome_ldpc_encode_batch_device(const SyndromeLdpcEncoder* encoder, const uint8_t* d_info,
+                                          size_t info_stride, uint8_t* d_codewords, size_t codeword_stride,
+                                          size_t count, void* stream) {
+  return guard([&]() -> int32_t {
+    if (!encoder || ((!d_info || !d_codewords) && count)) return SYNDROME_NULL_POINTER;
+    const syn::Graph& g = encoder->enc.graph();
+    if (info_stride < (size_t)g.k() || codeword_stride < (size_t)g.n())
+      return fail(SYNDROME_BUFFER_TOO_SMALL, "row stride smaller than K or N");
+    if (count > (size_t)LLONG_MAX / 2) return fail(SYNDROME_INVALID_PARAM, "count out of range");
+    const cudaError_t e = encoder->enc.encode_batch_device(d_info, (long long)info_stride, d_codewords,
+                                                           (long long)codeword_stride, (long long)count,
+                                                           static_cast<cudaStream_t>(stream));
+    return from_cuda(e, "device encode");
+  });
+}
+
 int32_t syndrome_ldpc_encode_batch(const SyndromeLdpcEncoder* encoder, const uint8_t* info_bits,
                                    size_t info_stride, uint8_t* codewords, size_t codeword_stride,
                                    size_t count, int32_t threads) {

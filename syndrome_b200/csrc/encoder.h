@@ -15,7 +15,11 @@
 // one pass over the extension layers.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 #include "graph.h"
@@ -35,12 +39,28 @@ class Encoder {
   void encode_batch(const uint8_t* info, long long info_stride, uint8_t* codewords,
                     long long cw_stride, long long count, int threads) const;
 
+  // The same codewords computed on the GPU (encoder_kernels.cu): info and codewords are
+  // device arrays (one bit per byte), enqueued on `stream`.  The device copy of the
+  // tables is made on the first call, on the current device.
+  cudaError_t encode_batch_device(const uint8_t* d_info, long long info_stride, uint8_t* d_codewords,
+                                  long long cw_stride, long long count, cudaStream_t stream) const;
+
  private:
   Graph g_;
   int core_blocks_ = 0;                 // parity blocks solved jointly
   int core_bits_ = 0;                   // core_blocks_ * z
   int words_ = 0;                       // 64-bit words per inverse row
   std::vector<uint64_t> inv_;           // core_bits_ x words_ bit matrix (row-major)
+  // Device tables (encoder_kernels.cu), made on first use and shared by copies.
+  struct Dev {
+    std::mutex mu;
+    int device = -1;
+    uint32_t* inv_t = nullptr;  // [words32][core_bits] transposed inverse
+    int32_t* loff = nullptr;    // [mb + 1]
+    uint32_t* edge = nullptr;   // [E] col << 16 | shift
+    ~Dev();
+  };
+  std::shared_ptr<Dev> dev_ = std::make_shared<Dev>();
 };
 
 }  // namespace syn

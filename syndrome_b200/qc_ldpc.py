@@ -349,6 +349,26 @@ class QcLdpcEncoder:
         return cw
 
 
+    def encode_batch_device(self, info_bits, stream=None):
+        """info_bits: uint8 CUDA tensor [count, K] (one bit per byte) -> uint8 CUDA
+        tensor [count, N] of codewords, encoded on the GPU (same codewords as
+        encode_batch)."""
+        import torch
+
+        if not (isinstance(info_bits, torch.Tensor) and info_bits.is_cuda and info_bits.dim() == 2
+                and info_bits.dtype == torch.uint8 and info_bits.stride(1) == 1):
+            raise TypeError("info_bits must be a 2-D uint8 CUDA tensor with contiguous rows")
+        count = info_bits.shape[0]
+        cw = torch.empty((count, self.codeword_bit_count()), dtype=torch.uint8, device=info_bits.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(info_bits.device)
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        stride = info_bits.stride(0) if count > 1 else info_bits.shape[1]
+        _lib.check(_lib.load().syndrome_ldpc_encode_batch_device(self._h, info_bits.data_ptr(), stride,
+                                                                 cw.data_ptr(), cw.shape[1], count, sp))
+        return cw
+
+
 def wifi_ldpc_encoder(z, rate_num, rate_den):
     """src/wifi_ldpc_tables.rs:490."""
     h = ctypes.c_void_p()
