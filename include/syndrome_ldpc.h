@@ -453,6 +453,11 @@ int32_t syndrome_serve_release(SyndromeServer* server, uint64_t tb_id);
  * from each step's first copy to its last, worker microseconds building steps,
  * worker microseconds finishing steps}. */
 int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out14);
+/* Work-item sizes per shape: n triples (base_graph, z, codewords per item; 0 = as many
+ * as one CTA holds), as chosen by the autotuner (syndrome_b200/autotune.py).  Takes
+ * effect from the next step; results do not depend on it.  INVALID_PARAM for a base
+ * graph other than 0/1 or z outside 1..384. */
+int32_t syndrome_serve_set_tiles(SyndromeServer* server, const int32_t* triples, size_t n);
 
 /* Open-loop load test of a server (the serving benchmark; no counterpart in the
  * reference).  Transport blocks arrive as a Poisson process of offered_tb_per_s for

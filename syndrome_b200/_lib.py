@@ -110,6 +110,7 @@ PROTOTYPES = {
     "syndrome_ldpc_pipeline_frame_set_tag": (None, [_vp, ctypes.c_int64, _sz]),
     "syndrome_ldpc_pipeline_frame_tag": (_sz, [_vp, ctypes.c_int64]),
     "syndrome_ldpc_encode_batch_device": (_i32, [_vp, _vp, _sz, _vp, _sz, _sz, _vp]),
+    "syndrome_serve_set_tiles": (_i32, [_vp, _vp, _sz]),
     "syndrome_last_error": (ctypes.c_char_p, []),
 }
 

@@ -1057,6 +1057,18 @@ int32_t syndrome_serve_release(SyndromeServer* server, uint64_t tb_id) {
   });
 }
 
+int32_t syndrome_serve_set_tiles(SyndromeServer* server, const int32_t* triples, size_t n) {
+  return guard([&]() -> int32_t {
+    if (!server || (!triples && n)) return SYNDROME_NULL_POINTER;
+    for (size_t i = 0; i < n; ++i) {
+      const int bg = triples[3 * i], z = triples[3 * i + 1];
+      if ((bg != 0 && bg != 1) || z < 1 || z > 384) return fail(SYNDROME_INVALID_PARAM, "base graph or z out of range");
+    }
+    for (size_t i = 0; i < n; ++i) server->engine.set_tile(triples[3 * i], triples[3 * i + 1], triples[3 * i + 2]);
+    return SYNDROME_OK;
+  });
+}
+
 int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out14) {
   return guard([&]() -> int32_t {
     if (!server || !out14) return SYNDROME_NULL_POINTER;

@@ -353,7 +353,9 @@ bool ServeEngine::launch_step(Slot& s) {
   ordered.reserve(n_cbs);
   for (auto& kv : shapes) {
     const int bg = kv.first.first, z = kv.first.second;
-    const int cap = paired_ ? pair_mixed_capacity(bg, z) : mixed_slot_capacity(bg, z);
+    int cap = paired_ ? pair_mixed_capacity(bg, z) : mixed_slot_capacity(bg, z);
+    const int hint = (bg == 0 || bg == 1) && z >= 1 && z <= 384 ? tiles_[bg][z].load(std::memory_order_relaxed) : 0;
+    if (hint > 0) cap = std::min(cap, hint);  // tuned item size (autotune.py)
     const std::vector<int>& idx = kv.second;
     for (size_t a = 0; a < idx.size(); a += cap) {
       MixItem m{};
@@ -570,6 +572,10 @@ int ServeEngine::release(uint64_t id, std::string* err) {
   if (it->second.harq_off >= 0) harq_free(it->second.harq_off);
   tbs_.erase(it);
   return SYNDROME_OK;
+}
+
+void ServeEngine::set_tile(int bg, int z, int tile) {
+  if ((bg == 0 || bg == 1) && z >= 1 && z <= 384) tiles_[bg][z].store(std::max(tile, 0), std::memory_order_relaxed);
 }
 
 ServeStats ServeEngine::stats() {

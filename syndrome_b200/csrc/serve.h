@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdint>
@@ -70,6 +71,9 @@ class ServeEngine {
   // Drops the state of id (HARQ accumulators included).  Not while a transmission is in flight.
   int release(uint64_t id, std::string* err);
   ServeStats stats();
+  // Codewords per work item for one shape (0 = as many as a CTA holds); takes effect
+  // from the next step.
+  void set_tile(int bg, int z, int tile);
 
  private:
   struct Tb {
@@ -150,6 +154,7 @@ class ServeEngine {
   bool stop_ = false;
   std::thread thread_;
   std::string fatal_;
+  std::atomic<int> tiles_[2][385] = {};
 };
 
 // Open-loop Poisson load against an engine (serve_load.cpp, syndrome_serve_run_load).

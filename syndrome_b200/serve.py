@@ -57,6 +57,12 @@ class Server:
         self._h = h.value
         self._keep = {}
 
+    def set_tiles(self, tiles):
+        """Work-item sizes per shape, {(bg, z): codewords} (autotune.tune_tiles)."""
+        arr = np.ascontiguousarray(np.asarray([(bg, z, t) for (bg, z), t in tiles.items()], dtype=np.int32)
+                                   .reshape(-1, 3))
+        _lib.check(_lib.load().syndrome_serve_set_tiles(self._h, arr.ctypes.data if len(arr) else None, len(arr)))
+
     def close(self):
         h, self._h = getattr(self, "_h", None), None
         if h:
