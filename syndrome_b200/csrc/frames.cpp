@@ -84,6 +84,7 @@ int DlSchF32::decode(const float* rx, long long rx_len, int rv, uint8_t* tb_out,
     cb.e = d_rx_ + (long long)ci * e_;
     cb.llr = nullptr;  // f32: the accumulators are the decoder input
     cb.hard = d_hard_ + (long long)ci * words_;
+    cb.hard_words = words_;
     cb.ncb = w.ncb;
     cb.fs = w.fs;
     cb.fe = w.fe;

@@ -312,6 +312,8 @@ bool ServeEngine::launch_step(Slot& s) {
     tb.has_cb_crc = p.has_cb_crc ? 1 : 0;
     tb.tb_size = t.tb_size;
     tb.x_payload = crc24_xpow_host(p.payload, kCrc24A);
+    tb.x_last = crc24_xpow_host(std::max<long long>(0, std::min<long long>(p.payload, p.b - (long long)(p.c - 1) * p.payload)),
+                                kCrc24A);
     tb.tb_bits = s.d_bits + bits_off;
     tb.result = s.d_res + kResWords * j;
     s.bits_off.push_back(bits_off);
@@ -323,6 +325,7 @@ bool ServeEngine::launch_step(Slot& s) {
       cb.e = e_src + (long long)ci * t.e;
       cb.llr = s.d_llr + llr_off;
       cb.hard = s.d_hard + hard_off;
+      cb.hard_words = words;
       cb.ncb = w.ncb;
       cb.fs = w.fs;
       cb.fe = w.fe;

@@ -6,14 +6,17 @@
 //     (selection k with (c0 + k) mod M = compressed(p), every M selections) and adds
 //     them in received order, exactly the order of the reference's scatter loop, so the
 //     f32 sums are bit-identical.  No atomics: each position has one owner.
-// serve_cb_crc_kernel   one warp per code block: the CRC-24B check over its K' decoded
-//     bits and the CRC-24A register of the bits it carries for the TB CRC.  Lanes take
-//     contiguous word chunks (byte-table CRC, tables in shared memory) and the chunk
-//     registers are joined with CRC(A|B) = CRC(A) * x^|B| + CRC(B) (mod P).
+// serve_cb_crc_kernel   one thread per code block: the CRC-24B check over its K' decoded
+//     bits and the CRC-24A register of the bits it carries for the TB CRC, 32 bits per
+//     step with slice-by-4 tables in shared memory (register' = sum over the four
+//     bytes b_k of ((R << 8) ^ word) of T_k[b_k], T_k[v] = v * x^(8k + 24) mod P).
 // serve_tb_finish_kernel one CTA per transport block: the TB CRC-24A from the blocks'
-//     registers (crc.rs check: the register over payload + received CRC is zero iff
-//     they match), the report (crc_ok, max iterations, per-block CRC) and the
-//     desegmented TB bits (transport_block.rs:1014-1050).
+//     registers, CRC(A|B) = CRC(A) * x^|B| + CRC(B) (mod P), the multiplication by the
+//     fixed x^payload done with three 256-entry tables built by the CTA (crc.rs check:
+//     the register over payload + received CRC is zero iff they match); the report
+//     (crc_ok, max iterations, per-block CRC); the desegmented TB bits
+//     (transport_block.rs:1014-1050), one thread per output word, each a funnel shift of
+//     the packed bits of at most two code blocks.
 #include "serve_kernels.h"
 
 #include <algorithm>
@@ -44,45 +47,32 @@ __host__ __device__ inline uint32_t crc_xpow(long long n, uint32_t poly) {
   return result;
 }
 
-__device__ inline uint32_t crc_byte(uint32_t reg, uint32_t byte, const uint32_t* table) {
-  return ((reg << 8) & 0xFFFFFFu) ^ table[((reg >> 16) ^ byte) & 0xFFu];
-}
-
 __device__ inline uint32_t crc_bit(uint32_t reg, uint32_t bit, uint32_t poly) {
   const uint32_t fb = ((reg >> 23) ^ bit) & 1u;
   reg = (reg << 1) & 0xFFFFFFu;
   return fb ? reg ^ poly : reg;
 }
 
-// CRC register of bits [0, nbits) of LSB-first packed words, computed by one warp.
-__device__ uint32_t warp_crc(const uint32_t* __restrict__ words, int nbits, const uint32_t* table, uint32_t poly,
-                             int lane) {
+// CRC register of bits [0, nbits) of LSB-first packed words (stream bit i is bit i % 32
+// of word i / 32), one thread, t = the four slice tables of the polynomial.
+__device__ uint32_t thread_crc(const uint32_t* words, int nbits, const uint32_t (*t)[256],
+                               uint32_t poly) {
   const int full = nbits >> 5, rem = nbits & 31;
-  const int chunk = (full + 31) >> 5;
-  const int lo = lane * chunk, hi = min(lo + chunk, full);
   uint32_t reg = 0;
-  for (int w = lo; w < hi; ++w) {
-    const uint32_t r = __brev(words[w]);  // bit 0 (first in order) becomes the MSB
-    reg = crc_byte(reg, r >> 24, table);
-    reg = crc_byte(reg, (r >> 16) & 0xFFu, table);
-    reg = crc_byte(reg, (r >> 8) & 0xFFu, table);
-    reg = crc_byte(reg, r & 0xFFu, table);
-  }
-  const uint32_t xchunk = chunk > 0 ? crc_xpow(32LL * chunk, poly) : 1u;
-  uint32_t total = 0;
-  for (int l = 0; l < 32; ++l) {
-    const uint32_t cl = __shfl_sync(0xFFFFFFFFu, reg, l);
-    const int nw = max(0, min(chunk, full - l * chunk));
-    if (nw == chunk && nw > 0)
-      total = crc_mulmod(total, xchunk, poly) ^ cl;
-    else if (nw > 0)
-      total = crc_mulmod(total, crc_xpow(32LL * nw, poly), poly) ^ cl;
+  for (int w = 0; w < full; ++w) {
+    const uint32_t x = (reg << 8) ^ __brev(words[w]);  // first stream bit in the MSB
+    reg = t[3][x >> 24] ^ t[2][(x >> 16) & 0xFFu] ^ t[1][(x >> 8) & 0xFFu] ^ t[0][x & 0xFFu];
   }
   if (rem) {
     const uint32_t w = words[full];
-    for (int i = 0; i < rem; ++i) total = crc_bit(total, (w >> i) & 1u, poly);
+    for (int i = 0; i < rem; ++i) reg = crc_bit(reg, (w >> i) & 1u, poly);
   }
-  return total;
+  return reg;
+}
+
+// x * y mod P for a fixed y, from the tables m[k][v] = (v << 8k) * y mod P.
+__device__ __forceinline__ uint32_t mul_fixed(uint32_t x, const uint32_t (*m)[256]) {
+  return m[0][x & 0xFFu] ^ m[1][(x >> 8) & 0xFFu] ^ m[2][(x >> 16) & 0xFFu];
 }
 
 __global__ void serve_combine_kernel(const ServeCb* __restrict__ cbs, float scale) {
@@ -124,41 +114,50 @@ __global__ void serve_combine_kernel(const ServeCb* __restrict__ cbs, float scal
   cb.llr[p] = (int8_t)qv;
 }
 
+constexpr int kCrcWarps = 4;
+constexpr int kCrcMaxWords = (8448 + 31) / 32;  // K' of the largest code block
+
 __global__ void serve_cb_crc_kernel(const ServeCb* __restrict__ cbs, int n_cbs, ServeCbCrc* __restrict__ out) {
-  __shared__ uint32_t tab[2][256];
-  for (int i = threadIdx.x; i < 512; i += blockDim.x) {
-    const uint32_t poly = i < 256 ? kPolyA : kPolyB;
+  __shared__ uint32_t tab[2][4][256];
+  __shared__ uint32_t bits[kCrcWarps][kCrcMaxWords];
+  for (int i = threadIdx.x; i < 2048; i += blockDim.x) {
+    const uint32_t poly = i < 1024 ? kPolyA : kPolyB;
+    const int k = (i >> 8) & 3;
     uint32_t reg = (uint32_t)(i & 255) << 16;
-    for (int b = 0; b < 8; ++b) reg = (reg & 0x800000u) ? ((reg << 1) ^ poly) & 0xFFFFFFu : (reg << 1) & 0xFFFFFFu;
-    tab[i >> 8][i & 255] = reg;
+    for (int b = 0; b < 8 * (k + 1); ++b) reg = (reg & 0x800000u) ? ((reg << 1) ^ poly) & 0xFFFFFFu : (reg << 1) & 0xFFFFFFu;
+    tab[i >> 10][k][i & 255] = reg;
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  // one warp per code block: its packed bits to shared memory (coalesced), then lane 0
+  // the CRC-24A register and lane 1 the CRC-24B check, side by side
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int i = blockIdx.x * kCrcWarps + wi;
   if (i >= n_cbs) return;
   const ServeCb cb = cbs[i];
-  const uint32_t ra = warp_crc(cb.hard, cb.crc_len, tab[0], kPolyA, lane);
-  int ok = 1;
-  if (cb.k_prime > 0) ok = warp_crc(cb.hard, cb.k_prime, tab[1], kPolyB, lane) == 0u;
-  if (lane == 0) {
-    out[i].crc_a = ra;
-    out[i].ok_b = ok;
-  }
+  const int nw = min(cb.hard_words, kCrcMaxWords);
+  for (int w = lane; w < nw; w += 32) bits[wi][w] = cb.hard[w];
+  __syncwarp();
+  if (lane == 0) out[i].crc_a = thread_crc(bits[wi], min(cb.crc_len, 32 * nw), tab[0], kPolyA);
+  if (lane == 1) out[i].ok_b = cb.k_prime > 0 ? thread_crc(bits[wi], min(cb.k_prime, 32 * nw), tab[1], kPolyB) == 0u : 1;
 }
 
 __global__ void serve_tb_finish_kernel(const ServeTb* __restrict__ tbs, const ServeCb* __restrict__ cbs,
                                        const ServeCbCrc* __restrict__ crc, const int32_t* __restrict__ iters) {
+  __shared__ uint32_t my[3][256];  // (v << 8k) * x^payload mod P_A
   const ServeTb tb = tbs[blockIdx.x];
+  for (int i = threadIdx.x; i < 768; i += blockDim.x)
+    my[i >> 8][i & 255] = crc_mulmod((uint32_t)(i & 255) << (8 * (i >> 8)), tb.x_payload, kPolyA);
+  __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t total = 0;
     int all_cb = 1, max_it = 0;
     for (int i = 0; i < tb.n_cb; ++i) {
       const int c = tb.first_cb + i;
       const int len = cbs[c].crc_len;
-      if (len > 0) {
-        const uint32_t xl = len == tb.payload ? tb.x_payload : crc_xpow(len, kPolyA);
-        total = crc_mulmod(total, xl, kPolyA) ^ crc[c].crc_a;
-      }
+      if (len == tb.payload)
+        total = mul_fixed(total, my) ^ crc[c].crc_a;
+      else if (len > 0)
+        total = crc_mulmod(total, i == tb.n_cb - 1 ? tb.x_last : crc_xpow(len, kPolyA), kPolyA) ^ crc[c].crc_a;
       all_cb &= crc[c].ok_b;
       max_it = max(max_it, iters[c]);
     }
@@ -170,18 +169,27 @@ __global__ void serve_tb_finish_kernel(const ServeTb* __restrict__ tbs, const Se
     for (int t = 0; t < 32 && 32 * w + t < tb.n_cb; ++t) bits |= (uint32_t)crc[tb.first_cb + 32 * w + t].ok_b << t;
     tb.result[2 + w] = (int32_t)bits;
   }
-  // desegmentation: TB bit i is bit i % payload of code block i / payload
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const long long nwords = (tb.tb_size + 31) >> 5;
-  for (long long w = warp; w < nwords; w += nwarps) {
-    const long long i = (w << 5) + lane;
-    bool bit = false;
-    if (i < tb.tb_size) {
-      const long long c = i / tb.payload, j = i - c * tb.payload;
-      bit = (cbs[tb.first_cb + c].hard[j >> 5] >> (j & 31)) & 1u;
+  // desegmentation: TB bit i is bit i % payload of code block i / payload; a word spans
+  // at most two code blocks (with more than one block, payload > 32)
+  auto bits_at = [&](int c, int j) -> uint32_t {  // 32 bits of block c from bit j on (0 past its words)
+    const ServeCb& cb = cbs[tb.first_cb + c];
+    const int w = j >> 5;
+    const uint32_t lo = w < cb.hard_words ? cb.hard[w] : 0u, hi = w + 1 < cb.hard_words ? cb.hard[w + 1] : 0u;
+    return __funnelshift_r(lo, hi, (unsigned)(j & 31));
+  };
+  const int nwords = (int)((tb.tb_size + 31) >> 5);
+  for (int w = threadIdx.x; w < nwords; w += blockDim.x) {
+    const int i0 = 32 * w;
+    const int c = i0 / tb.payload, j = i0 - c * tb.payload;
+    uint32_t v = bits_at(c, j);
+    const int avail = tb.payload - j;
+    if (avail < 32) {
+      v &= (1u << avail) - 1u;
+      if (c + 1 < tb.n_cb) v |= bits_at(c + 1, 0) << avail;
     }
-    const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
-    if (lane == 0) tb.tb_bits[w] = m;
+    const long long left = tb.tb_size - i0;
+    if (left < 32) v &= (1u << left) - 1u;
+    tb.tb_bits[w] = v;
   }
 }
 
@@ -198,7 +206,7 @@ cudaError_t serve_combine_launch(const ServeCb* d_cbs, int n_cbs, int max_ncb, f
 
 cudaError_t serve_cb_crc_launch(const ServeCb* d_cbs, int n_cbs, ServeCbCrc* d_out, cudaStream_t stream) {
   if (n_cbs <= 0) return cudaSuccess;
-  serve_cb_crc_kernel<<<(n_cbs + 3) / 4, 128, 0, stream>>>(d_cbs, n_cbs, d_out);
+  serve_cb_crc_kernel<<<(n_cbs + kCrcWarps - 1) / kCrcWarps, 32 * kCrcWarps, 0, stream>>>(d_cbs, n_cbs, d_out);
   return cudaGetLastError();
 }
 

@@ -19,6 +19,7 @@ struct ServeCb {
   int k_prime;           // bits covered by the code-block CRC-24B (CRC included)
   int crc_len;           // leading bits of this block inside the TB CRC-24A range
   int tb;                // index of the block's transport block in the step
+  int hard_words;        // words of `hard` (K' bits)
 };
 
 // One transport block (one transmission) in a serving step.
@@ -28,6 +29,7 @@ struct ServeTb {
   int has_cb_crc;
   long long tb_size;     // A
   uint32_t x_payload;    // x^payload mod P_A
+  uint32_t x_last;       // x^(CRC-24A bits of the last code block) mod P_A
   uint32_t* tb_bits;     // output: tb_size bits, LSB-first words
   int32_t* result;       // [0] crc_ok, [1] max iterations, [2 + i/32] bit i%32 = code block i CRC ok
 };
