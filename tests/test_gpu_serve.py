@@ -173,3 +173,15 @@ def test_serve_open_loop_load():
     assert (lat > 0).all() and 0 < rep["p50_us"] <= rep["p99_us"] <= rep["max_us"]
     assert s.stats()["tbs_held"] == 0 and s.stats()["harq_bytes_used"] == 0
     s.close()
+
+
+def test_serve_large_transport_blocks_match_oracle():
+    """Transport blocks of 36 and 152 code blocks (the largest TB size): the
+    desegmented payload and the TB CRC folded over every block must match the oracle
+    and the transmitted bits."""
+    cases = [(300000, 0.75, 2, 400002, 4.0), (1277992, 0.9, 6, 1419996, 5.0), (300000, 0.75, 2, 400002, 1.2)]
+    server = S.Server(iterations=8)
+    data, reports, payloads = run_sequences(server, cases, seed0=700)
+    assert any(v[-1]["crc_ok"] for v in reports.values())
+    check_against_oracle(data, reports, payloads)
+    server.close()
