@@ -62,7 +62,7 @@ def parse_args():
     p.add_argument("--serve-pool", type=int, default=48)
     p.add_argument("--serve-seconds", type=float, default=1.0)
     p.add_argument("--serve-step-cbs", type=int, default=1024)
-    p.add_argument("--serve-loads", type=float, nargs="+", default=[0.25, 0.5, 0.75],
+    p.add_argument("--serve-loads", type=float, nargs="+", default=[0.1, 0.25, 0.5, 0.75],
                    help="offered loads as fractions of the measured serving capacity")
     return p.parse_args()
 

@@ -410,7 +410,7 @@ void syndrome_dlsch_decoder_flush_harq(SyndromeDlSchDecoder* decoder);
 typedef struct SyndromeServer SyndromeServer;
 typedef struct {
   uint32_t max_step_code_blocks; /* code blocks per GPU step, >= 160 (0 = 2048) */
-  uint32_t steps_in_flight;      /* 1..16 (0 = 8): steps run concurrently on free SMs */
+  uint32_t steps_in_flight;      /* 1..16 (0 = 6): steps run concurrently on free SMs */
   uint64_t harq_bytes;           /* device memory for HARQ accumulators (0 = 8 GiB) */
   uint64_t staging_bytes;        /* device staging for host-memory LLRs, per step (0 = 256 MiB) */
   int32_t iterations;            /* maximum LOMS iterations (early stop on a zero syndrome) */

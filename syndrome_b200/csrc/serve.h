@@ -25,7 +25,10 @@ namespace syn {
 
 struct ServeConfig {
   int max_step_cbs = 2048;               // code blocks per GPU step (at least one whole TB)
-  int slots = 8;                         // steps in flight (concurrent on free SMs)
+  // Steps in flight (concurrent on free SMs).  6: the same saturated throughput as 8
+  // and more, with a shorter tail near saturation (concurrent steps share the SMs, so
+  // each waits for its slowest work item longer).
+  int slots = 6;
   long long harq_bytes = 8LL << 30;      // device memory for HARQ accumulators
   long long staging_bytes = 256LL << 20; // device staging of host-memory LLRs, per step
   int iterations = 8;

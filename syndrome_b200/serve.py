@@ -45,7 +45,7 @@ class _LoadReport(ctypes.Structure):
 
 class Server:
     """A serving engine on the current CUDA device.  Zero-valued sizes take the
-    library defaults (2048 code blocks per step, 8 steps in flight, 8 GiB of HARQ
+    library defaults (2048 code blocks per step, 6 steps in flight, 8 GiB of HARQ
     accumulators, 256 MiB of staging for host-memory LLRs)."""
 
     def __init__(self, max_step_code_blocks=0, steps_in_flight=0, harq_bytes=0, staging_bytes=0, iterations=8,
