@@ -295,6 +295,23 @@ def serve_section(batch_gbps, dev, args):
             "steps": st["steps"], "mean_code_blocks_per_step": st["code_blocks"] / max(st["steps"], 1)}
 
 
+def max_over_ranks(ms, world, dist=None, device=None):
+    """The slowest rank's time (every rank takes part in the same collective)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gbps(batch, steps, world, ms):
+    """Information Gbit/s of the whole job: every rank's codewords over the slowest
+    rank's time (weak scaling: each rank decodes its own batch)."""
+    return batch * K_INFO * steps * world / (ms * 1e-3) / 1e9
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -354,14 +371,9 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dist, dev)
     ms_per_step = ms / args.steps
-    total_bits = B * K_INFO * args.steps * world
-    value = total_bits / (ms * 1e-3) / 1e9
+    value = whole_job_gbps(B, args.steps, world, ms)
 
     # ---- end to end through the public API with pinned host buffers ----
     h_llr = torch.from_numpy(llr_h).pin_memory()
@@ -404,12 +416,8 @@ def main():
     f1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    ms_e2e = f0.elapsed_time(f1)
-    if world > 1:
-        t = torch.tensor([ms_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e_value = total_bits / (ms_e2e * 1e-3) / 1e9
+    ms_e2e = max_over_ranks(f0.elapsed_time(f1), world, dist, dev)
+    e2e_value = whole_job_gbps(B, args.steps, world, ms_e2e)
     e2e_ok = bool(np.array_equal(h_packed.numpy(), packed.cpu().numpy()))
 
     # ---- roofline of the decode kernel (HBM) ----
