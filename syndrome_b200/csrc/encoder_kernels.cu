@@ -14,6 +14,7 @@
 #include <string>
 
 #include "encoder.h"
+#include "smem_limit.h"
 
 namespace syn {
 
@@ -147,8 +148,7 @@ cudaError_t Encoder::encode_batch_device(const uint8_t* d_info, long long info_s
   a.count = count;
   const int smem = 4 * words32 + (int)g.n();
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
-  if ((e = cudaFuncSetAttribute(encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-    return e;
+  if ((e = allow_max_dynamic_smem((const void*)encode_kernel)) != cudaSuccess) return e;
   int sms = 0, per_sm = 0;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cur)) != cudaSuccess ||
       (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode_kernel, kEncThreads, smem)) != cudaSuccess)

@@ -30,6 +30,7 @@
 #include <string>
 
 #include "decoder.h"
+#include "smem_limit.h"
 #include "nr_kernels.h"
 
 namespace syn {
@@ -490,7 +491,7 @@ Decoder::Geometry Decoder::geometry(Precision p, long long batch) const {
   geo.smem = table_bytes(g_.edges(), g_.mb, cpb) + (int)(cpb * N * elem);
   geo.maxdeg_tmpl = pick_maxdeg(g_.maxdeg);
   KernelFn fn = kernel_for(p, geo.maxdeg_tmpl);
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, geo.smem);
+  allow_max_dynamic_smem((const void*)fn);
   int per_sm = 0, sms = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, geo.threads, geo.smem);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ < 0 ? 0 : device_);

@@ -34,6 +34,7 @@
 #include <type_traits>
 
 #include "nr_graph.cuh"
+#include "smem_limit.h"
 #include "nr_kernels.h"
 
 namespace syn {
@@ -411,7 +412,7 @@ cudaError_t launch_bg(const NrCommon& c, const int* shifts, bool clamp, int sms,
   const int threads = ((c.cpb * c.z + 31) / 32) * 32;
   const int smem = al16(c.cpb * 4) + state_bytes<BG>(threads) + c.cpb * slot_bytes<BG>(c.z);
   auto fn = clamp ? nr_i8_kernel<BG, true> : nr_i8_kernel<BG, false>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = allow_max_dynamic_smem((const void*)fn);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);

@@ -20,6 +20,7 @@
 #include <cstdint>
 
 #include "nr_kernels.h"
+#include "smem_limit.h"
 #include "nr_pair.cuh"
 
 namespace syn {
@@ -379,7 +380,7 @@ cudaError_t launch(const NrCommon& c0, const int* shifts, int sms, cudaStream_t 
   const int threads = ((a.c.cpb * c0.z + 31) / 32) * 32;
   const int smem = pair_smem_bytes<BG>(a.c.cpb, c0.z, threads);
   auto fn = nr_pair_kernel<BG, ZT, FILL>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = allow_max_dynamic_smem((const void*)fn);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
