@@ -75,43 +75,57 @@ __device__ __forceinline__ uint32_t mul_fixed(uint32_t x, const uint32_t (*m)[25
   return m[0][x & 0xFFu] ^ m[1][(x >> 8) & 0xFFu] ^ m[2][(x >> 16) & 0xFFu];
 }
 
-__global__ void serve_combine_kernel(const ServeCb* __restrict__ cbs, float scale) {
-  const ServeCb cb = cbs[blockIdx.y];
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= cb.ncb) return;
-  if (p >= cb.fs && p < cb.fe) {  // filler positions: never transmitted, decoder pins them
-    if (cb.first) cb.acc[p] = 0.0f;
-    if (cb.llr) cb.llr[p] = 0;
-    return;
-  }
-  const int c = p < cb.fs ? p : p - (cb.fe - cb.fs);
-  int k = c - cb.c0 % cb.m;
-  if (k < 0) k += cb.m;
-  float a = cb.first ? 0.0f : cb.acc[p];
-  if (cb.qm == 1) {
-    for (long long kk = k; kk < cb.e_len; kk += cb.m) a = __fadd_rn(a, cb.e[kk]);
-  } else {
-    // received index of selection kk: q = (kk % qm) * rows + kk / qm; add in q order
-    const long long rows = cb.e_len / cb.qm;
-    long long q[8];
-    int n = 0;
-    for (long long kk = k; kk < cb.e_len && n < 8; kk += cb.m) {
-      const long long v = (kk % cb.qm) * rows + kk / cb.qm;
-      int i = n++;
-      while (i > 0 && q[i - 1] > v) {
-        q[i] = q[i - 1];
-        --i;
-      }
-      q[i] = v;
+constexpr int kCombThreads = 256, kCombPer = 4;  // positions per thread (block-strided)
+constexpr int kCombMaxAdds = 16;  // contributions per position: E <= 8 * ncb and M >= ncb / 2
+
+__global__ void __launch_bounds__(kCombThreads) serve_combine_kernel(const ServeCb* __restrict__ cbs, float scale) {
+  // Only the fields used, once per thread, and 32-bit index arithmetic throughout (the
+  // kernel is otherwise bound by its integer instructions, not by memory).
+  const ServeCb* cbp = cbs + blockIdx.y;
+  const int ncb = cbp->ncb, fs = cbp->fs, fe = cbp->fe, m = cbp->m, e_len = cbp->e_len, qm = cbp->qm;
+  const int first = cbp->first, c0 = cbp->c0 % m;
+  float* __restrict__ acc = cbp->acc;
+  const float* __restrict__ e = cbp->e;
+  int8_t* __restrict__ llr = cbp->llr;
+  const int rows = e_len / qm;
+#pragma unroll
+  for (int i = 0; i < kCombPer; ++i) {
+    const int p = (blockIdx.x * kCombPer + i) * kCombThreads + threadIdx.x;
+    if (p >= ncb) break;
+    if (p >= fs && p < fe) {  // filler positions: never transmitted, decoder pins them
+      if (first) acc[p] = 0.0f;
+      if (llr) llr[p] = 0;
+      continue;
     }
-    for (int i = 0; i < n; ++i) a = __fadd_rn(a, cb.e[q[i]]);
+    const int c = p < fs ? p : p - (fe - fs);
+    int k = c - c0;
+    if (k < 0) k += m;
+    float a = first ? 0.0f : acc[p];
+    if (qm == 1) {
+      for (int kk = k; kk < e_len; kk += m) a = __fadd_rn(a, e[kk]);
+    } else {
+      // received index of selection kk: q = (kk % qm) * rows + kk / qm; add in q order
+      int q[kCombMaxAdds];
+      int n = 0;
+      for (int kk = k; kk < e_len && n < kCombMaxAdds; kk += m) {
+        const int d = kk / qm;
+        const int v = (kk - d * qm) * rows + d;
+        int j = n++;
+        while (j > 0 && q[j - 1] > v) {
+          q[j] = q[j - 1];
+          --j;
+        }
+        q[j] = v;
+      }
+      for (int j = 0; j < n; ++j) a = __fadd_rn(a, e[q[j]]);
+    }
+    acc[p] = a;
+    if (!llr) continue;  // f32 decode: the accumulator is the decoder input
+    const float v = __fmul_rn(a, scale);
+    int qv = 0;
+    if (!isnan(v)) qv = (int)fminf(fmaxf(roundf(v), -127.0f), 127.0f);
+    llr[p] = (int8_t)qv;
   }
-  cb.acc[p] = a;
-  if (!cb.llr) return;  // f32 decode: the accumulator is the decoder input
-  const float v = __fmul_rn(a, scale);
-  int qv = 0;
-  if (!isnan(v)) qv = (int)fminf(fmaxf(roundf(v), -127.0f), 127.0f);
-  cb.llr[p] = (int8_t)qv;
 }
 
 constexpr int kCrcWarps = 4;
@@ -199,8 +213,9 @@ uint32_t crc24_xpow_host(long long n, uint32_t poly) { return crc_xpow(n, poly);
 
 cudaError_t serve_combine_launch(const ServeCb* d_cbs, int n_cbs, int max_ncb, float scale, cudaStream_t stream) {
   if (n_cbs <= 0) return cudaSuccess;
-  const dim3 grid((unsigned)((max_ncb + 255) / 256), (unsigned)n_cbs);
-  serve_combine_kernel<<<grid, 256, 0, stream>>>(d_cbs, scale);
+  const int per_block = kCombThreads * kCombPer;
+  const dim3 grid((unsigned)((max_ncb + per_block - 1) / per_block), (unsigned)n_cbs);
+  serve_combine_kernel<<<grid, kCombThreads, 0, stream>>>(d_cbs, scale);
   return cudaGetLastError();
 }
 
