@@ -160,3 +160,20 @@ def test_pipeline_back_pressure_and_misuse():
     pipe.release(r)
     with pytest.raises(S.SyndromeError):  # released twice
         pipe.release(r)
+
+
+def test_dlsch_decoder_f32_256qam_and_repetition():
+    for i, (a, r, qm, g, eb) in enumerate([(40000, 0.8, 8, 50000, 3.0), (200, 0.5, 2, 2600, -1.0)]):
+        tb, llrs = transmissions(a, r, qm, g, eb, 1200 + i)
+        dec = S.DlSchDecoder(a, r, qm, g, 8, BETA)
+        ref = O.DlSchDecoder(a, r, qm, g, iterations=8, f32_beta=BETA)
+        for n, rv in enumerate(RVS):
+            out = np.zeros(a, np.uint8)
+            got = dec.decode(llrs[n], rv, out)
+            want = ref.decode(llrs[n], rv)
+            assert (got.crc_ok, got.harq_tx_count, got.max_iters_used) == (want["crc_ok"], want["harq_tx"],
+                                                                           want["max_iters"])
+            assert list(got.cb_crc) == list(want["cb_crc"])
+            if got.crc_ok:
+                assert np.array_equal(out, tb)
+                break

@@ -185,3 +185,13 @@ def test_serve_large_transport_blocks_match_oracle():
     assert any(v[-1]["crc_ok"] for v in reports.values())
     check_against_oracle(data, reports, payloads)
     server.close()
+
+
+def test_serve_256qam_and_repetition_match_oracle():
+    """Qm = 8 (the combine's interleaved gather) and a code block sent almost twice
+    over (E close to 2 * ncb, up to three contributions per buffer position)."""
+    cases = [(40000, 0.8, 8, 50000, 3.0), (200, 0.5, 2, 2600, -1.0), (200, 0.5, 2, 2600, 2.0)]
+    server = S.Server(iterations=8)
+    data, reports, payloads = run_sequences(server, cases, seed0=800)
+    check_against_oracle(data, reports, payloads)
+    server.close()
