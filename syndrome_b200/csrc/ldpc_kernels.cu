@@ -504,7 +504,10 @@ size_t Decoder::workspace_bytes(Precision p, long long batch) const {
   const long long groups = (batch + geo.cpb - 1) / geo.cpb;
   const long long ctas = std::min<long long>(groups, geo.max_ctas);
   const long long elem = p == Precision::kInt8 ? 1 : 4;
-  return (size_t)(ctas * geo.cpb * g_.edge_buffer() * elem);
+  size_t bytes = (size_t)(ctas * geo.cpb * g_.edge_buffer() * elem);
+  if (p == Precision::kF32 && nr_bg_ >= 0 && nr_f32_applies(nr_bg_, g_.z))
+    bytes = std::max(bytes, nr_f32_workspace_bytes(nr_bg_, sms_));
+  return bytes;
 }
 
 cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t stream,
@@ -560,6 +563,32 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
     if (req.kernel == 3 && !pair_ok) return bad("the paired 5G NR kernel needs app_clamp >= 3938 (7874 with filler)");
     if (pair_ok && req.kernel != 2) return nr_pair_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream);
     return nr_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream);
+  }
+  // f32 5G NR at Z = 384: the compressed-message kernel, when the caller's workspace
+  // holds its extension posteriors (else the generic kernel below).
+  if (p == Precision::kF32 && nr_bg_ >= 0 && nr_f32_applies(nr_bg_, g_.z) && !req.shorten && req.kernel != 1 &&
+      req.workspace && req.workspace_bytes >= nr_f32_workspace_bytes(nr_bg_, sms_)) {
+    NrF32Common c;
+    c.llr = static_cast<const float*>(req.llr);
+    c.llr_stride = req.llr_stride;
+    c.llr_offset = req.llr_offset;
+    c.batch = req.batch;
+    c.iterations = req.iterations;
+    c.beta = req.beta;
+    c.prologue = req.prologue_5g;
+    c.k_prime = req.n_filler > g_.k() ? 0 : g_.k() - req.n_filler;
+    c.hard_packed = req.hard_packed;
+    c.hard_bits = req.hard_bits;
+    c.hard_words_stride = req.hard_words_stride;
+    c.iters = req.iters;
+    c.app_out = static_cast<float*>(req.app);
+    c.app_stride = req.app_stride;
+    c.edge_r_out = static_cast<float*>(req.edge_r);
+    c.edge_r_stride = req.edge_r_stride;
+    c.hard_out = req.hard;
+    c.hard_stride = req.hard_stride;
+    c.ext_ws = static_cast<float*>(req.workspace);
+    return nr_f32_decode(nr_bg_, c, sms_, stream);
   }
   const Geometry geo = geometry(p, req.batch);
   const long long groups = (req.batch + geo.cpb - 1) / geo.cpb;

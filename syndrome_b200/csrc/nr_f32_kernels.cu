@@ -1,0 +1,292 @@
+// f32 layered offset min-sum for the 5G NR base graphs at Z = 384 on sm_100a, with the
+// check-to-variable messages compressed in shared memory.
+//
+// Arithmetic of syndrome src/qc_ldpc.rs:1146-1205 (the scalar f32 pass): Q = app - R_old,
+// min1/min2 of |Q| (a tie moves min1 to min2), R_new = sign * max(mex - beta, 0) with
+// mex = min2 where |Q| == min1 and min1 elsewhere, sign = the row's sign parity times
+// Q's sign, app += R_new - R_old; all in round-to-nearest f32 in the reference's order.
+// The messages of a row are therefore a function of two magnitudes,
+// max(min1 - beta, 0) and max(min2 - beta, 0), and two bits per edge (|Q| == min1,
+// R's sign bit), from which R_old is rebuilt bit for bit (signed zeros included):
+// 8 bytes per row plus 2 bits per edge instead of 4 bytes per edge.
+//
+// One codeword per CTA of 384 threads (thread z owns row z of every layer and the
+// variables (column, z)).  Shared memory: the f32 posteriors of the KB + 4 core columns
+// and the compressed state (magnitudes and code bits word-major per thread).  The
+// extension columns' posteriors (one per layer >= 4, touched only by that layer's row
+// z) cannot be recomputed from channel value + message (f32 rounding makes the running
+// sum path-dependent), so each thread keeps its own in a per-CTA global buffer: a
+// coalesced load per row, issued early (global and shared accesses never alias).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cstdint>
+
+#include "nr_graph.cuh"
+#include "nr_kernels.h"
+#include "smem_limit.h"
+
+namespace syn {
+namespace nrf {
+
+using nr::barrier_after;
+using nr::deg_of;
+using nr::ext_pos;
+using nr::static_for;
+using nr::Tab;
+
+constexpr int kZ = 384;
+constexpr int kThreads = 384;
+
+extern __shared__ __align__(16) unsigned char f32_smem[];
+
+template <int BG>
+struct Layout {
+  static constexpr int CORE = Tab<BG>::KB + 4, NEXT = Tab<BG>::MB - 4;
+  static constexpr int NMAG = 2 * Tab<BG>::MB;                // two magnitudes per row
+  static constexpr int NCODE = (2 * Tab<BG>::E + 31) / 32;    // 2 bits per edge, packed across rows
+  static constexpr int APP = 16;                              // byte offset of the core posteriors
+  static constexpr int MAG = APP + CORE * kZ * 4;             // state words: [word][thread]
+  static constexpr int CODE = MAG + NMAG * kThreads * 4;
+  static constexpr int BYTES = CODE + NCODE * kThreads * 4;
+};
+
+template <int BG>
+struct Ctx {
+  int tid;
+  int z4;
+  float* ext;  // this CTA's extension posteriors, [layer - 4][z]
+  template <int GE>
+  __device__ __forceinline__ int vb() const {
+    int zl = z4;
+    asm volatile("" : "+r"(zl));  // keeps the unrolled graph's addresses from being hoisted
+    const unsigned r = (unsigned)(zl + Tab<BG>::z384_shift(GE) * 4);
+    const unsigned rr = min(r, r - (unsigned)(kZ * 4));
+    return (int)rr + Tab<BG>::col(GE) * kZ * 4;
+  }
+  __device__ __forceinline__ float ld_ap(int b) const {
+    return *reinterpret_cast<const float*>(f32_smem + Layout<BG>::APP + b);
+  }
+  __device__ __forceinline__ void st_ap(int b, float v) const {
+    *reinterpret_cast<float*>(f32_smem + Layout<BG>::APP + b) = v;
+  }
+  __device__ __forceinline__ float ld_mag(int w) const {
+    return *reinterpret_cast<const float*>(f32_smem + Layout<BG>::MAG + 4 * (w * kThreads + tid));
+  }
+  __device__ __forceinline__ void st_mag(int w, float v) const {
+    *reinterpret_cast<float*>(f32_smem + Layout<BG>::MAG + 4 * (w * kThreads + tid)) = v;
+  }
+  __device__ __forceinline__ uint32_t ld_code(int w) const {
+    return *reinterpret_cast<const uint32_t*>(f32_smem + Layout<BG>::CODE + 4 * (w * kThreads + tid));
+  }
+  __device__ __forceinline__ void st_code(int w, uint32_t v) const {
+    *reinterpret_cast<uint32_t*>(f32_smem + Layout<BG>::CODE + 4 * (w * kThreads + tid)) = v;
+  }
+  __device__ __forceinline__ float ld_ext(int i) const { return ext[i * kZ + (z4 >> 2)]; }
+  __device__ __forceinline__ void st_ext(int i, float v) const { ext[i * kZ + (z4 >> 2)] = v; }
+};
+
+// R_old of edge e from the row's magnitudes and the edge's two code bits
+// (bit 0: |Q| was the row minimum, bit 1: R's sign).
+__device__ __forceinline__ float message(float magA, float magB, unsigned bb) {
+  return __uint_as_float(__float_as_uint((bb & 1u) ? magB : magA) | ((bb & 2u) << 30));
+}
+
+template <int BG, int L>
+__device__ __forceinline__ void row(const Ctx<BG>& c, float beta) {
+  constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L);
+  constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
+  constexpr int b0 = 2 * lb, w0 = b0 >> 5, w1 = (b0 + 2 * deg - 1) >> 5, sh = b0 & 31;
+  float av[deg], qv[deg];
+  int vb[deg];
+  // the extension posterior first: a global load, the longest latency of the row
+  if constexpr (ep >= 0) av[ep] = c.ld_ext(L - 4);
+  const float magA = c.ld_mag(2 * L), magB = c.ld_mag(2 * L + 1);
+  const uint32_t lo = c.ld_code(w0);
+  const uint32_t hi = w1 != w0 ? c.ld_code(w1) : 0u;
+  const unsigned long long word = ((unsigned long long)hi << 32) | lo;
+  const unsigned long long bits = word >> sh;
+  float m1 = FLT_MAX, m2 = FLT_MAX;
+  unsigned sx = 0u;
+  static_for<0, deg>([&](auto ei) {
+    constexpr int e = decltype(ei)::value;
+    if constexpr (e != ep) {
+      vb[e] = c.template vb<lb + e>();
+      av[e] = c.ld_ap(vb[e]);
+    }
+    const float ro = message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u);
+    const float q = __fsub_rn(av[e], ro);
+    qv[e] = q;
+    const unsigned b = __float_as_uint(q);
+    const float aq = __uint_as_float(b & 0x7FFFFFFFu);
+    sx ^= b & 0x80000000u;
+    if (aq <= m1) {
+      m2 = m1;
+      m1 = aq;
+    } else if (aq < m2) {
+      m2 = aq;
+    }
+  });
+  if (m1 == FLT_MAX) m1 = 0.0f;
+  if (m2 == FLT_MAX) m2 = m1;
+  float nA = __fsub_rn(m1, beta), nB = __fsub_rn(m2, beta);  // messages of the non-minimum / minimum edges
+  if (nA < 0.0f) nA = 0.0f;
+  if (nB < 0.0f) nB = 0.0f;
+  unsigned long long nbits = 0ull;
+  static_for<0, deg>([&](auto ei) {
+    constexpr int e = decltype(ei)::value;
+    const unsigned b = __float_as_uint(qv[e]);
+    const float aq = __uint_as_float(b & 0x7FFFFFFFu);
+    const unsigned sgn = sx ^ (b & 0x80000000u);
+    const bool is_min = aq == m1;
+    const float nr = __uint_as_float(__float_as_uint(is_min ? nB : nA) | sgn);
+    const float ro = message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u);
+    const float nv = __fadd_rn(av[e], __fsub_rn(nr, ro));
+    if constexpr (e == ep)
+      c.st_ext(L - 4, nv);
+    else
+      c.st_ap(vb[e], nv);
+    nbits |= (unsigned long long)((is_min ? 1u : 0u) | (sgn >> 30)) << (2 * e);
+  });
+  c.st_mag(2 * L, nA);
+  c.st_mag(2 * L + 1, nB);
+  constexpr unsigned long long mask = ((deg >= 32 ? 0ull : (1ull << (2 * deg))) - 1ull) << sh;
+  const unsigned long long nw = (word & ~mask) | ((nbits << sh) & mask);
+  c.st_code(w0, (uint32_t)nw);
+  if constexpr (w1 != w0) c.st_code(w1, (uint32_t)(nw >> 32));
+}
+
+// Odd parity of any check row of this thread (qc_ldpc.rs:1231-1252: negative = app < 0).
+template <int BG>
+__device__ __forceinline__ bool rows_fail(const Ctx<BG>& c) {
+  bool fail = false;
+  static_for<0, Tab<BG>::MB>([&](auto li) {
+    constexpr int L = decltype(li)::value;
+    constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L);
+    constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
+    unsigned par = 0u;
+    static_for<0, deg>([&](auto ei) {
+      constexpr int e = decltype(ei)::value;
+      const float v = e == ep ? c.ld_ext(L - 4) : c.ld_ap(c.template vb<lb + e>());
+      par ^= v < 0.0f ? 1u : 0u;
+    });
+    fail = fail || par != 0u;
+  });
+  return fail;
+}
+
+template <int BG>
+__global__ void __launch_bounds__(kThreads, 1) nr_f32_kernel(const __grid_constant__ NrF32Common a) {
+  using T = Tab<BG>;
+  using LY = Layout<BG>;
+  constexpr int CORE = LY::CORE, NEXT = LY::NEXT, N = T::NB * kZ, K = T::KB * kZ;
+  const int tid = threadIdx.x, z = tid;
+  Ctx<BG> c;
+  c.tid = tid;
+  c.z4 = z * 4;
+  c.ext = a.ext_ws + (long long)blockIdx.x * NEXT * kZ;
+  float* A = reinterpret_cast<float*>(f32_smem + LY::APP);
+  const int lane = tid & 31, warp = tid >> 5;
+  for (long long cw = blockIdx.x; cw < a.batch; cw += gridDim.x) {
+    __syncthreads();
+    // ---- load (the f32 kernels' prologue: [0, llr_offset) erased, 5G init on top)
+    const float* src = a.llr + cw * a.llr_stride;
+    auto value = [&](int j) -> float {
+      float v = j >= a.llr_offset ? src[j - a.llr_offset] : 0.0f;
+      if (a.prologue) {
+        if (j < 2 * kZ)
+          v = 0.0f;
+        else if (j >= a.k_prime && j < K)
+          v = 1000000.0f;
+      }
+      return v;
+    };
+    for (int col = 0; col < CORE; ++col) A[col * kZ + z] = value(col * kZ + z);
+    for (int i = 0; i < NEXT; ++i) c.ext[i * kZ + z] = value((CORE + i) * kZ + z);
+#pragma unroll 1
+    for (int w = 0; w < LY::NMAG; ++w) c.st_mag(w, 0.0f);
+#pragma unroll 1
+    for (int w = 0; w < LY::NCODE; ++w) c.st_code(w, 0u);
+    __syncthreads();
+    // ---- iterations with early stop on a zero syndrome (qc_ldpc.rs:1146-1221)
+    int used = 0;
+    bool active = true;
+    for (int it = 0; it < a.iterations; ++it) {
+      if (!__syncthreads_or(active)) break;
+      ++used;
+      static_for<0, T::MB>([&](auto li) {
+        constexpr int L = decltype(li)::value;
+        row<BG, L>(c, a.beta);
+        if constexpr (barrier_after<BG>(L)) __syncthreads();
+      });
+      active = __syncthreads_or(rows_fail<BG>(c)) != 0;
+    }
+    // ---- outputs
+    if (tid == 0 && a.iters) a.iters[cw] = used;
+    auto app_at = [&](int j) -> float { return j < CORE * kZ ? A[j] : c.ext[j - CORE * kZ]; };
+    if (a.app_out) {
+      float* dst = a.app_out + cw * a.app_stride;
+      for (int col = 0; col < T::NB; ++col) dst[col * kZ + z] = col < CORE ? A[col * kZ + z] : c.ld_ext(col - CORE);
+    }
+    if (a.hard_out) {
+      uint8_t* dst = a.hard_out + cw * a.hard_stride;
+      for (int col = 0; col < T::NB; ++col)
+        dst[col * kZ + z] = (col < CORE ? A[col * kZ + z] : c.ld_ext(col - CORE)) < 0.0f ? 1 : 0;
+    }
+    if (a.edge_r_out) {
+      float* er = a.edge_r_out + cw * a.edge_r_stride;
+      static_for<0, T::MB>([&](auto li) {
+        constexpr int L = decltype(li)::value;
+        constexpr int lb = T::loff(L), deg = deg_of<BG>(L);
+        constexpr int b0 = 2 * lb, w0 = b0 >> 5, w1 = (b0 + 2 * deg - 1) >> 5, sh = b0 & 31;
+        const float magA = c.ld_mag(2 * L), magB = c.ld_mag(2 * L + 1);
+        const unsigned long long word =
+            ((unsigned long long)(w1 != w0 ? c.ld_code(w1) : 0u) << 32) | c.ld_code(w0);
+        static_for<0, deg>([&](auto ei) {
+          constexpr int e = decltype(ei)::value;
+          er[(long long)(lb + e) * kZ + z] = message(magA, magB, (unsigned)((word >> sh) >> (2 * e)) & 3u);
+        });
+      });
+    }
+    if (a.hard_packed) {
+      // the extension posteriors are in global memory, written by their own threads
+      __syncthreads();
+      uint32_t* dst = a.hard_packed + cw * a.hard_words_stride;
+      const int nwords = (a.hard_bits + 31) >> 5;
+      for (int w = warp; w < nwords; w += kThreads / 32) {
+        const int j = (w << 5) + lane;
+        const bool bit = j < a.hard_bits && app_at(j) < 0.0f;
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+        if (lane == 0) dst[w] = m;
+      }
+    }
+  }
+  (void)N;
+}
+
+}  // namespace nrf
+
+bool nr_f32_applies(int bg, int z) { return (bg == 0 || bg == 1) && z == nrf::kZ; }
+
+size_t nr_f32_workspace_bytes(int bg, int sms) {
+  const int next = bg == 0 ? nr::Tab<0>::MB - 4 : nr::Tab<1>::MB - 4;
+  return (size_t)std::max(sms, 1) * next * nrf::kZ * sizeof(float);
+}
+
+cudaError_t nr_f32_decode(int bg, const NrF32Common& c, int sms, cudaStream_t stream) {
+  if (c.batch <= 0) return cudaSuccess;
+  const int ctas = (int)std::min<long long>(c.batch, std::max(sms, 1));
+  if (bg == 0) {
+    cudaError_t e = allow_max_dynamic_smem((const void*)nrf::nr_f32_kernel<0>);
+    if (e != cudaSuccess) return e;
+    nrf::nr_f32_kernel<0><<<ctas, nrf::kThreads, nrf::Layout<0>::BYTES, stream>>>(c);
+  } else {
+    cudaError_t e = allow_max_dynamic_smem((const void*)nrf::nr_f32_kernel<1>);
+    if (e != cudaSuccess) return e;
+    nrf::nr_f32_kernel<1><<<ctas, nrf::kThreads, nrf::Layout<1>::BYTES, stream>>>(c);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace syn

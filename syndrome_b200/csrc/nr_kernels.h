@@ -95,6 +95,33 @@ cudaError_t nr_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, 
 // app_clamp >= 3938 (>= 7874 with filler bits), where no posterior of a non-filler
 // variable can reach the clamp.  c.cpb is chosen by the launcher.
 bool nr_pair_applies(const NrCommon& c);
+
+// f32 5G NR decode at Z = 384 with compressed messages (nr_f32_kernels.cu): the same
+// results as the generic f32 kernel.  ext_ws: nr_f32_workspace_bytes(bg, sms) bytes.
+struct NrF32Common {
+  const float* llr = nullptr;
+  long long llr_stride = 0;
+  int llr_offset = 0;
+  long long batch = 0;
+  int iterations = 0;
+  float beta = 0.0f;
+  int prologue = 0;
+  long long k_prime = 0;
+  uint32_t* hard_packed = nullptr;
+  int hard_bits = 0;
+  long long hard_words_stride = 0;
+  int32_t* iters = nullptr;
+  float* app_out = nullptr;
+  long long app_stride = 0;
+  float* edge_r_out = nullptr;
+  long long edge_r_stride = 0;
+  uint8_t* hard_out = nullptr;
+  long long hard_stride = 0;
+  float* ext_ws = nullptr;
+};
+bool nr_f32_applies(int bg, int z);
+size_t nr_f32_workspace_bytes(int bg, int sms);
+cudaError_t nr_f32_decode(int bg, const NrF32Common& c, int sms, cudaStream_t stream);
 // Paired mixed-shape kernel (same MixArgs as mixed_decode_launch; needs app_clamp >=
 // 7874).  Work items hold up to pair_mixed_capacity codewords of one shape.
 int pair_mixed_capacity(int bg, int z);

@@ -244,7 +244,9 @@ class QcLdpcDecoder:
             edge_r = torch.empty((b, self.required_edge_buffer()), dtype=edge_dtype, device=dev)
         if want_hard:
             hard = torch.empty((b, n), dtype=torch.uint8, device=dev)
-        if edge_r is None and workspace is None:
+        # f32: a workspace also when the messages go to edge_r (the 5G NR Z=384 kernel keeps
+        # its extension-column posteriors there)
+        if workspace is None and (edge_r is None or kind == "f32"):
             need = self.batch_workspace_size(b, "f32" if kind == "f32" else "int8")
             workspace = self._ws.get((dev, kind))
             if workspace is None or workspace.numel() < need:
