@@ -157,37 +157,98 @@ __device__ __forceinline__ void row(const Ctx<BG>& c, float beta) {
   if constexpr (w1 != w0) c.st_code(w1, (uint32_t)(nw >> 32));
 }
 
-// Odd parity of any check row of this thread (qc_ldpc.rs:1231-1252: negative = app < 0).
+// Odd parity of check row (L, z) (qc_ldpc.rs:1231-1252: negative = app < 0).
+template <int BG, int L>
+__device__ __forceinline__ bool row_odd(const Ctx<BG>& c) {
+  constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L);
+  constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
+  unsigned par = 0u;
+  static_for<0, deg>([&](auto ei) {
+    constexpr int e = decltype(ei)::value;
+    const float v = e == ep ? c.ld_ext(L - 4) : c.ld_ap(c.template vb<lb + e>());
+    par ^= v < 0.0f ? 1u : 0u;
+  });
+  return par != 0u;
+}
+
+// The syndrome check in two stages: the few smallest layers for every iteration, the
+// others only when those pass (nr::is_quick); the second stage out of line.
 template <int BG>
-__device__ __forceinline__ bool rows_fail(const Ctx<BG>& c) {
-  bool fail = false;
+__device__ __forceinline__ bool quick_odd(const Ctx<BG>& c) {
+  bool odd = false;
   static_for<0, Tab<BG>::MB>([&](auto li) {
     constexpr int L = decltype(li)::value;
-    constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L);
-    constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
-    unsigned par = 0u;
-    static_for<0, deg>([&](auto ei) {
-      constexpr int e = decltype(ei)::value;
-      const float v = e == ep ? c.ld_ext(L - 4) : c.ld_ap(c.template vb<lb + e>());
-      par ^= v < 0.0f ? 1u : 0u;
-    });
-    fail = fail || par != 0u;
+    if constexpr (nr::is_quick<BG>(L)) odd = odd || row_odd<BG, L>(c);
   });
-  return fail;
+  return odd;
+}
+template <int BG>
+__device__ __noinline__ bool rest_odd(const Ctx<BG> c) {
+  bool odd = false;
+  static_for<0, Tab<BG>::MB>([&](auto li) {
+    constexpr int L = decltype(li)::value;
+    if constexpr (!nr::is_quick<BG>(L)) odd = odd || row_odd<BG, L>(c);
+  });
+  return odd;
+}
+
+// Results of codeword cw (out of line: keeps the iteration loop's registers free).
+template <int BG>
+__device__ __noinline__ void write_out(const NrF32Common* a, const Ctx<BG> c, long long cw, int used) {
+  using T = Tab<BG>;
+  constexpr int CORE = Layout<BG>::CORE;
+  const int tid = c.tid, z = tid, lane = tid & 31, warp = tid >> 5;
+  const float* A = reinterpret_cast<const float*>(f32_smem + Layout<BG>::APP);
+  if (tid == 0 && a->iters) a->iters[cw] = used;
+  if (a->app_out) {
+    float* dst = a->app_out + cw * a->app_stride;
+    for (int col = 0; col < T::NB; ++col) dst[col * kZ + z] = col < CORE ? A[col * kZ + z] : c.ld_ext(col - CORE);
+  }
+  if (a->hard_out) {
+    uint8_t* dst = a->hard_out + cw * a->hard_stride;
+    for (int col = 0; col < T::NB; ++col)
+      dst[col * kZ + z] = (col < CORE ? A[col * kZ + z] : c.ld_ext(col - CORE)) < 0.0f ? 1 : 0;
+  }
+  if (a->edge_r_out) {
+    float* er = a->edge_r_out + cw * a->edge_r_stride;
+    static_for<0, T::MB>([&](auto li) {
+      constexpr int L = decltype(li)::value;
+      constexpr int lb = T::loff(L), deg = deg_of<BG>(L);
+      constexpr int b0 = 2 * lb, w0 = b0 >> 5, w1 = (b0 + 2 * deg - 1) >> 5, sh = b0 & 31;
+      const float magA = c.ld_mag(2 * L), magB = c.ld_mag(2 * L + 1);
+      const unsigned long long word = ((unsigned long long)(w1 != w0 ? c.ld_code(w1) : 0u) << 32) | c.ld_code(w0);
+      static_for<0, deg>([&](auto ei) {
+        constexpr int e = decltype(ei)::value;
+        er[(long long)(lb + e) * kZ + z] = message(magA, magB, (unsigned)((word >> sh) >> (2 * e)) & 3u);
+      });
+    });
+  }
+  if (a->hard_packed) {
+    // the extension posteriors are in global memory, written by their own threads
+    __syncthreads();
+    uint32_t* dst = a->hard_packed + cw * a->hard_words_stride;
+    const int nwords = (a->hard_bits + 31) >> 5;
+    for (int w = warp; w < nwords; w += kThreads / 32) {
+      const int j = (w << 5) + lane;
+      bool bit = false;
+      if (j < a->hard_bits) bit = (j < CORE * kZ ? A[j] : c.ext[j - CORE * kZ]) < 0.0f;
+      const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+      if (lane == 0) dst[w] = m;
+    }
+  }
 }
 
 template <int BG>
 __global__ void __launch_bounds__(kThreads, 1) nr_f32_kernel(const __grid_constant__ NrF32Common a) {
   using T = Tab<BG>;
   using LY = Layout<BG>;
-  constexpr int CORE = LY::CORE, NEXT = LY::NEXT, N = T::NB * kZ, K = T::KB * kZ;
+  constexpr int CORE = LY::CORE, NEXT = LY::NEXT, K = T::KB * kZ;
   const int tid = threadIdx.x, z = tid;
   Ctx<BG> c;
   c.tid = tid;
   c.z4 = z * 4;
   c.ext = a.ext_ws + (long long)blockIdx.x * NEXT * kZ;
   float* A = reinterpret_cast<float*>(f32_smem + LY::APP);
-  const int lane = tid & 31, warp = tid >> 5;
   for (long long cw = blockIdx.x; cw < a.batch; cw += gridDim.x) {
     __syncthreads();
     // ---- load (the f32 kernels' prologue: [0, llr_offset) erased, 5G init on top)
@@ -220,49 +281,12 @@ __global__ void __launch_bounds__(kThreads, 1) nr_f32_kernel(const __grid_consta
         row<BG, L>(c, a.beta);
         if constexpr (barrier_after<BG>(L)) __syncthreads();
       });
-      active = __syncthreads_or(rows_fail<BG>(c)) != 0;
+      bool odd = __syncthreads_or(quick_odd<BG>(c)) != 0;
+      if (!odd) odd = __syncthreads_or(rest_odd<BG>(c)) != 0;
+      active = odd;
     }
-    // ---- outputs
-    if (tid == 0 && a.iters) a.iters[cw] = used;
-    auto app_at = [&](int j) -> float { return j < CORE * kZ ? A[j] : c.ext[j - CORE * kZ]; };
-    if (a.app_out) {
-      float* dst = a.app_out + cw * a.app_stride;
-      for (int col = 0; col < T::NB; ++col) dst[col * kZ + z] = col < CORE ? A[col * kZ + z] : c.ld_ext(col - CORE);
-    }
-    if (a.hard_out) {
-      uint8_t* dst = a.hard_out + cw * a.hard_stride;
-      for (int col = 0; col < T::NB; ++col)
-        dst[col * kZ + z] = (col < CORE ? A[col * kZ + z] : c.ld_ext(col - CORE)) < 0.0f ? 1 : 0;
-    }
-    if (a.edge_r_out) {
-      float* er = a.edge_r_out + cw * a.edge_r_stride;
-      static_for<0, T::MB>([&](auto li) {
-        constexpr int L = decltype(li)::value;
-        constexpr int lb = T::loff(L), deg = deg_of<BG>(L);
-        constexpr int b0 = 2 * lb, w0 = b0 >> 5, w1 = (b0 + 2 * deg - 1) >> 5, sh = b0 & 31;
-        const float magA = c.ld_mag(2 * L), magB = c.ld_mag(2 * L + 1);
-        const unsigned long long word =
-            ((unsigned long long)(w1 != w0 ? c.ld_code(w1) : 0u) << 32) | c.ld_code(w0);
-        static_for<0, deg>([&](auto ei) {
-          constexpr int e = decltype(ei)::value;
-          er[(long long)(lb + e) * kZ + z] = message(magA, magB, (unsigned)((word >> sh) >> (2 * e)) & 3u);
-        });
-      });
-    }
-    if (a.hard_packed) {
-      // the extension posteriors are in global memory, written by their own threads
-      __syncthreads();
-      uint32_t* dst = a.hard_packed + cw * a.hard_words_stride;
-      const int nwords = (a.hard_bits + 31) >> 5;
-      for (int w = warp; w < nwords; w += kThreads / 32) {
-        const int j = (w << 5) + lane;
-        const bool bit = j < a.hard_bits && app_at(j) < 0.0f;
-        const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
-        if (lane == 0) dst[w] = m;
-      }
-    }
+    write_out<BG>(&a, c, cw, used);
   }
-  (void)N;
 }
 
 }  // namespace nrf
