@@ -506,7 +506,7 @@ size_t Decoder::workspace_bytes(Precision p, long long batch) const {
   const long long elem = p == Precision::kInt8 ? 1 : 4;
   size_t bytes = (size_t)(ctas * geo.cpb * g_.edge_buffer() * elem);
   if (p == Precision::kF32 && nr_bg_ >= 0 && nr_f32_applies(nr_bg_, g_.z))
-    bytes = std::max(bytes, nr_f32_workspace_bytes(nr_bg_, sms_));
+    bytes = std::max(bytes, nr_f32_workspace_bytes(nr_bg_, g_.z, batch, sms_));
   return bytes;
 }
 
@@ -564,10 +564,10 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
     if (pair_ok && req.kernel != 2) return nr_pair_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream);
     return nr_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream);
   }
-  // f32 5G NR at Z = 384: the compressed-message kernel, when the caller's workspace
-  // holds its extension posteriors (else the generic kernel below).
+  // f32 5G NR: the compressed-message kernel, when the caller's workspace holds its
+  // extension posteriors (else the generic kernel below).
   if (p == Precision::kF32 && nr_bg_ >= 0 && nr_f32_applies(nr_bg_, g_.z) && !req.shorten && req.kernel != 1 &&
-      req.workspace && req.workspace_bytes >= nr_f32_workspace_bytes(nr_bg_, sms_)) {
+      req.workspace && req.workspace_bytes >= nr_f32_workspace_bytes(nr_bg_, g_.z, req.batch, sms_)) {
     NrF32Common c;
     c.llr = static_cast<const float*>(req.llr);
     c.llr_stride = req.llr_stride;
@@ -588,7 +588,7 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
     c.hard_out = req.hard;
     c.hard_stride = req.hard_stride;
     c.ext_ws = static_cast<float*>(req.workspace);
-    return nr_f32_decode(nr_bg_, c, sms_, stream);
+    return nr_f32_decode(nr_bg_, c, g_.z, g_.shifts.data(), sms_, stream);
   }
   const Geometry geo = geometry(p, req.batch);
   const long long groups = (req.batch + geo.cpb - 1) / geo.cpb;

@@ -36,8 +36,8 @@ using nr::ext_pos;
 using nr::static_for;
 using nr::Tab;
 
-constexpr int kZ = 384;
-constexpr int kThreads = 384;
+constexpr int kZ = 384;        // the compile-time lifting size
+constexpr int kThreads = 384;  // most threads (codeword rows) per CTA
 
 extern __shared__ __align__(16) unsigned char f32_smem[];
 
@@ -52,39 +52,74 @@ struct Layout {
   static constexpr int BYTES = CODE + NCODE * kThreads * 4;
 };
 
+// Any lifting size (ZT = 0): cpb = min(384 / Z, batch) codewords per CTA, thread t
+// owning row t % Z of codeword slot t / Z.  Shared memory: a flag word per slot and
+// stage, the state words laid out as at Z = 384 (compile-time offsets), then the slots'
+// core posteriors.
 template <int BG>
+struct RtLayout {
+  static constexpr int FLAGS = 0;
+  static constexpr int MAG = 2 * kThreads * 4;
+  static constexpr int CODE = MAG + Layout<BG>::NMAG * kThreads * 4;
+  static constexpr int APP = CODE + Layout<BG>::NCODE * kThreads * 4;
+  __host__ __device__ static constexpr int bytes(int z, int cpb) { return APP + cpb * Layout<BG>::CORE * z * 4; }
+};
+
+template <int BG>
+struct F32Args {
+  NrF32Common c;
+  int z, cpb;
+  int sh4[Tab<BG>::E];  // 4 * shift of each edge, reduced mod z (ZT = 0)
+  int cz4[Tab<BG>::E];  // 4 * col * z
+};
+
+// ZT = 384: shifts, column bases and the shared-memory layout are compile-time
+// constants.  ZT = 0: any Z, shifts and column bases from the kernel parameters.
+template <int BG, int ZT>
 struct Ctx {
+  static constexpr int MAGB = ZT > 0 ? Layout<BG>::MAG : RtLayout<BG>::MAG;
+  static constexpr int CODEB = ZT > 0 ? Layout<BG>::CODE : RtLayout<BG>::CODE;
   int tid;
   int z4;
-  float* ext;  // this CTA's extension posteriors, [layer - 4][z]
+  int Z4;   // 4 * Z (ZT = 0)
+  int ap;   // byte offset of this slot's core posteriors (ZT = 0)
+  float* ext;  // this thread's extension posteriors: ext[(layer - 4) * 384]
+  const F32Args<BG>* a;
   template <int GE>
   __device__ __forceinline__ int vb() const {
     int zl = z4;
     asm volatile("" : "+r"(zl));  // keeps the unrolled graph's addresses from being hoisted
-    const unsigned r = (unsigned)(zl + Tab<BG>::z384_shift(GE) * 4);
-    const unsigned rr = min(r, r - (unsigned)(kZ * 4));
-    return (int)rr + Tab<BG>::col(GE) * kZ * 4;
+    if constexpr (ZT > 0) {
+      const unsigned r = (unsigned)(zl + Tab<BG>::z384_shift(GE) * 4);
+      const unsigned rr = min(r, r - (unsigned)(kZ * 4));
+      return (int)rr + Tab<BG>::col(GE) * kZ * 4;
+    } else {
+      const unsigned r = (unsigned)(zl + a->sh4[GE]);
+      const unsigned rr = min(r, r - (unsigned)Z4);
+      return (int)rr + a->cz4[GE];
+    }
   }
+  __device__ __forceinline__ int apb() const { return ZT > 0 ? Layout<BG>::APP : ap; }
   __device__ __forceinline__ float ld_ap(int b) const {
-    return *reinterpret_cast<const float*>(f32_smem + Layout<BG>::APP + b);
+    return *reinterpret_cast<const float*>(f32_smem + apb() + b);
   }
   __device__ __forceinline__ void st_ap(int b, float v) const {
-    *reinterpret_cast<float*>(f32_smem + Layout<BG>::APP + b) = v;
+    *reinterpret_cast<float*>(f32_smem + apb() + b) = v;
   }
   __device__ __forceinline__ float ld_mag(int w) const {
-    return *reinterpret_cast<const float*>(f32_smem + Layout<BG>::MAG + 4 * (w * kThreads + tid));
+    return *reinterpret_cast<const float*>(f32_smem + MAGB + 4 * (w * kThreads + tid));
   }
   __device__ __forceinline__ void st_mag(int w, float v) const {
-    *reinterpret_cast<float*>(f32_smem + Layout<BG>::MAG + 4 * (w * kThreads + tid)) = v;
+    *reinterpret_cast<float*>(f32_smem + MAGB + 4 * (w * kThreads + tid)) = v;
   }
   __device__ __forceinline__ uint32_t ld_code(int w) const {
-    return *reinterpret_cast<const uint32_t*>(f32_smem + Layout<BG>::CODE + 4 * (w * kThreads + tid));
+    return *reinterpret_cast<const uint32_t*>(f32_smem + CODEB + 4 * (w * kThreads + tid));
   }
   __device__ __forceinline__ void st_code(int w, uint32_t v) const {
-    *reinterpret_cast<uint32_t*>(f32_smem + Layout<BG>::CODE + 4 * (w * kThreads + tid)) = v;
+    *reinterpret_cast<uint32_t*>(f32_smem + CODEB + 4 * (w * kThreads + tid)) = v;
   }
-  __device__ __forceinline__ float ld_ext(int i) const { return ext[i * kZ + (z4 >> 2)]; }
-  __device__ __forceinline__ void st_ext(int i, float v) const { ext[i * kZ + (z4 >> 2)] = v; }
+  __device__ __forceinline__ float ld_ext(int i) const { return ext[i * kThreads]; }
+  __device__ __forceinline__ void st_ext(int i, float v) const { ext[i * kThreads] = v; }
 };
 
 // R_old of edge e from the row's magnitudes and the edge's two code bits
@@ -93,8 +128,8 @@ __device__ __forceinline__ float message(float magA, float magB, unsigned bb) {
   return __uint_as_float(__float_as_uint((bb & 1u) ? magB : magA) | ((bb & 2u) << 30));
 }
 
-template <int BG, int L>
-__device__ __forceinline__ void row(const Ctx<BG>& c, float beta) {
+template <int BG, int ZT, int L>
+__device__ __forceinline__ void row(const Ctx<BG, ZT>& c, float beta) {
   constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L);
   constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
   constexpr int b0 = 2 * lb, w0 = b0 >> 5, w1 = (b0 + 2 * deg - 1) >> 5, sh = b0 & 31;
@@ -158,8 +193,8 @@ __device__ __forceinline__ void row(const Ctx<BG>& c, float beta) {
 }
 
 // Odd parity of check row (L, z) (qc_ldpc.rs:1231-1252: negative = app < 0).
-template <int BG, int L>
-__device__ __forceinline__ bool row_odd(const Ctx<BG>& c) {
+template <int BG, int ZT, int L>
+__device__ __forceinline__ bool row_odd(const Ctx<BG, ZT>& c) {
   constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L);
   constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
   unsigned par = 0u;
@@ -173,144 +208,247 @@ __device__ __forceinline__ bool row_odd(const Ctx<BG>& c) {
 
 // The syndrome check in two stages: the few smallest layers for every iteration, the
 // others only when those pass (nr::is_quick); the second stage out of line.
-template <int BG>
-__device__ __forceinline__ bool quick_odd(const Ctx<BG>& c) {
+template <int BG, int ZT>
+__device__ __forceinline__ bool quick_odd(const Ctx<BG, ZT>& c) {
   bool odd = false;
   static_for<0, Tab<BG>::MB>([&](auto li) {
     constexpr int L = decltype(li)::value;
-    if constexpr (nr::is_quick<BG>(L)) odd = odd || row_odd<BG, L>(c);
+    if constexpr (nr::is_quick<BG>(L)) odd = odd || row_odd<BG, ZT, L>(c);
   });
   return odd;
 }
-template <int BG>
-__device__ __noinline__ bool rest_odd(const Ctx<BG> c) {
+template <int BG, int ZT>
+__device__ __noinline__ bool rest_odd(const Ctx<BG, ZT> c) {
   bool odd = false;
   static_for<0, Tab<BG>::MB>([&](auto li) {
     constexpr int L = decltype(li)::value;
-    if constexpr (!nr::is_quick<BG>(L)) odd = odd || row_odd<BG, L>(c);
+    if constexpr (!nr::is_quick<BG>(L)) odd = odd || row_odd<BG, ZT, L>(c);
   });
   return odd;
 }
 
-// Results of codeword cw (out of line: keeps the iteration loop's registers free).
-template <int BG>
-__device__ __noinline__ void write_out(const NrF32Common* a, const Ctx<BG> c, long long cw, int used) {
+// Results of the codewords of group g (out of line: keeps the iteration loop's registers
+// free).  on: this thread's row z of slot `slot` holds codeword g * cpb + slot.
+template <int BG, int ZT>
+__device__ __noinline__ void write_out(const F32Args<BG>* pa, const Ctx<BG, ZT> c, long long g, int slot, int z,
+                                       bool on, int used) {
   using T = Tab<BG>;
   constexpr int CORE = Layout<BG>::CORE;
-  const int tid = c.tid, z = tid, lane = tid & 31, warp = tid >> 5;
-  const float* A = reinterpret_cast<const float*>(f32_smem + Layout<BG>::APP);
-  if (tid == 0 && a->iters) a->iters[cw] = used;
-  if (a->app_out) {
-    float* dst = a->app_out + cw * a->app_stride;
-    for (int col = 0; col < T::NB; ++col) dst[col * kZ + z] = col < CORE ? A[col * kZ + z] : c.ld_ext(col - CORE);
-  }
-  if (a->hard_out) {
-    uint8_t* dst = a->hard_out + cw * a->hard_stride;
-    for (int col = 0; col < T::NB; ++col)
-      dst[col * kZ + z] = (col < CORE ? A[col * kZ + z] : c.ld_ext(col - CORE)) < 0.0f ? 1 : 0;
-  }
-  if (a->edge_r_out) {
-    float* er = a->edge_r_out + cw * a->edge_r_stride;
-    static_for<0, T::MB>([&](auto li) {
-      constexpr int L = decltype(li)::value;
-      constexpr int lb = T::loff(L), deg = deg_of<BG>(L);
-      constexpr int b0 = 2 * lb, w0 = b0 >> 5, w1 = (b0 + 2 * deg - 1) >> 5, sh = b0 & 31;
-      const float magA = c.ld_mag(2 * L), magB = c.ld_mag(2 * L + 1);
-      const unsigned long long word = ((unsigned long long)(w1 != w0 ? c.ld_code(w1) : 0u) << 32) | c.ld_code(w0);
-      static_for<0, deg>([&](auto ei) {
-        constexpr int e = decltype(ei)::value;
-        er[(long long)(lb + e) * kZ + z] = message(magA, magB, (unsigned)((word >> sh) >> (2 * e)) & 3u);
+  const NrF32Common* a = &pa->c;
+  const int Z = ZT > 0 ? kZ : pa->z, cpb = ZT > 0 ? 1 : pa->cpb;
+  const int lane = c.tid & 31, warp = c.tid >> 5;
+  const long long cw = g * cpb + slot;
+  if (on) {
+    const float* A = reinterpret_cast<const float*>(f32_smem + c.apb());
+    if (z == 0 && a->iters) a->iters[cw] = used;
+    if (a->app_out) {
+      float* dst = a->app_out + cw * a->app_stride;
+      for (int col = 0; col < T::NB; ++col) dst[col * Z + z] = col < CORE ? A[col * Z + z] : c.ld_ext(col - CORE);
+    }
+    if (a->hard_out) {
+      uint8_t* dst = a->hard_out + cw * a->hard_stride;
+      for (int col = 0; col < T::NB; ++col)
+        dst[col * Z + z] = (col < CORE ? A[col * Z + z] : c.ld_ext(col - CORE)) < 0.0f ? 1 : 0;
+    }
+    if (a->edge_r_out) {
+      float* er = a->edge_r_out + cw * a->edge_r_stride;
+      static_for<0, T::MB>([&](auto li) {
+        constexpr int L = decltype(li)::value;
+        constexpr int lb = T::loff(L), deg = deg_of<BG>(L);
+        constexpr int b0 = 2 * lb, w0 = b0 >> 5, w1 = (b0 + 2 * deg - 1) >> 5, sh = b0 & 31;
+        const float magA = c.ld_mag(2 * L), magB = c.ld_mag(2 * L + 1);
+        const unsigned long long word =
+            ((unsigned long long)(w1 != w0 ? c.ld_code(w1) : 0u) << 32) | c.ld_code(w0);
+        static_for<0, deg>([&](auto ei) {
+          constexpr int e = decltype(ei)::value;
+          er[(long long)(lb + e) * Z + z] = message(magA, magB, (unsigned)((word >> sh) >> (2 * e)) & 3u);
+        });
       });
-    });
+    }
   }
   if (a->hard_packed) {
     // the extension posteriors are in global memory, written by their own threads
     __syncthreads();
-    uint32_t* dst = a->hard_packed + cw * a->hard_words_stride;
     const int nwords = (a->hard_bits + 31) >> 5;
-    for (int w = warp; w < nwords; w += kThreads / 32) {
+    const int nwarps = (int)(blockDim.x >> 5);
+    const float* X = a->ext_ws + (long long)blockIdx.x * Layout<BG>::NEXT * kThreads;
+    for (int t = warp; t < cpb * nwords; t += nwarps) {
+      const int s = ZT > 0 ? 0 : t / nwords, w = t - s * nwords;
+      if (g * cpb + s >= a->batch) continue;  // warp-uniform
+      const float* A = reinterpret_cast<const float*>(
+          f32_smem + (ZT > 0 ? Layout<BG>::APP : RtLayout<BG>::APP + s * CORE * Z * 4));
       const int j = (w << 5) + lane;
       bool bit = false;
-      if (j < a->hard_bits) bit = (j < CORE * kZ ? A[j] : c.ext[j - CORE * kZ]) < 0.0f;
+      if (j < a->hard_bits) {
+        float v;
+        if (j < CORE * Z) {
+          v = A[j];
+        } else {
+          const int i = (j - CORE * Z) / Z, zz = j - CORE * Z - i * Z;
+          v = X[i * kThreads + s * Z + zz];
+        }
+        bit = v < 0.0f;
+      }
       const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
-      if (lane == 0) dst[w] = m;
+      if (lane == 0) a->hard_packed[(g * cpb + s) * a->hard_words_stride + w] = m;
     }
   }
 }
 
-template <int BG>
-__global__ void __launch_bounds__(kThreads, 1) nr_f32_kernel(const __grid_constant__ NrF32Common a) {
+template <int BG, int ZT>
+__global__ void __launch_bounds__(kThreads, 1) nr_f32_kernel(const __grid_constant__ F32Args<BG> pa) {
   using T = Tab<BG>;
   using LY = Layout<BG>;
-  constexpr int CORE = LY::CORE, NEXT = LY::NEXT, K = T::KB * kZ;
-  const int tid = threadIdx.x, z = tid;
-  Ctx<BG> c;
+  constexpr int CORE = LY::CORE, NEXT = LY::NEXT;
+  const NrF32Common& a = pa.c;
+  const int tid = threadIdx.x;
+  const int Z = ZT > 0 ? kZ : pa.z, cpb = ZT > 0 ? 1 : pa.cpb, K = T::KB * Z;
+  const int slot0 = ZT > 0 ? 0 : tid / Z;
+  const bool live = slot0 < cpb;  // threads past cpb * Z only join the barriers
+  const int slot = min(slot0, cpb - 1);
+  const int z = ZT > 0 ? tid : (live ? tid - slot0 * Z : 0);
+  Ctx<BG, ZT> c;
   c.tid = tid;
   c.z4 = z * 4;
-  c.ext = a.ext_ws + (long long)blockIdx.x * NEXT * kZ;
-  float* A = reinterpret_cast<float*>(f32_smem + LY::APP);
-  for (long long cw = blockIdx.x; cw < a.batch; cw += gridDim.x) {
+  c.Z4 = Z * 4;
+  c.ap = RtLayout<BG>::APP + slot * CORE * Z * 4;
+  c.a = &pa;
+  // [layer - 4][row of the CTA], the row of thread t being t (slot * Z + z)
+  c.ext = a.ext_ws + (long long)blockIdx.x * NEXT * kThreads + tid;
+  int* flag = reinterpret_cast<int*>(f32_smem + RtLayout<BG>::FLAGS);  // ZT = 0: [stage][slot]
+  float* A = reinterpret_cast<float*>(f32_smem + c.apb());
+  for (long long g = blockIdx.x; g * cpb < a.batch; g += gridDim.x) {
+    const long long cw = g * cpb + slot;
+    const bool on = live && cw < a.batch;
     __syncthreads();
     // ---- load (the f32 kernels' prologue: [0, llr_offset) erased, 5G init on top)
-    const float* src = a.llr + cw * a.llr_stride;
-    auto value = [&](int j) -> float {
-      float v = j >= a.llr_offset ? src[j - a.llr_offset] : 0.0f;
-      if (a.prologue) {
-        if (j < 2 * kZ)
-          v = 0.0f;
-        else if (j >= a.k_prime && j < K)
-          v = 1000000.0f;
-      }
-      return v;
-    };
-    for (int col = 0; col < CORE; ++col) A[col * kZ + z] = value(col * kZ + z);
-    for (int i = 0; i < NEXT; ++i) c.ext[i * kZ + z] = value((CORE + i) * kZ + z);
+    if (on) {
+      const float* src = a.llr + cw * a.llr_stride;
+      auto value = [&](int j) -> float {
+        float v = j >= a.llr_offset ? src[j - a.llr_offset] : 0.0f;
+        if (a.prologue) {
+          if (j < 2 * Z)
+            v = 0.0f;
+          else if (j >= a.k_prime && j < K)
+            v = 1000000.0f;
+        }
+        return v;
+      };
+      for (int col = 0; col < CORE; ++col) A[col * Z + z] = value(col * Z + z);
+#pragma unroll 1
+      for (int i = 0; i < NEXT; ++i) c.st_ext(i, value((CORE + i) * Z + z));
+    }
 #pragma unroll 1
     for (int w = 0; w < LY::NMAG; ++w) c.st_mag(w, 0.0f);
 #pragma unroll 1
     for (int w = 0; w < LY::NCODE; ++w) c.st_code(w, 0u);
     __syncthreads();
-    // ---- iterations with early stop on a zero syndrome (qc_ldpc.rs:1146-1221)
+    // ---- iterations with early stop on a zero syndrome (qc_ldpc.rs:1146-1221), per codeword
     int used = 0;
-    bool active = true;
+    bool active = on;
     for (int it = 0; it < a.iterations; ++it) {
       if (!__syncthreads_or(active)) break;
-      ++used;
+      if constexpr (ZT == 0) {
+        if (tid < 2 * cpb) flag[tid] = 0;  // read back only after the layers' barriers
+      }
+      used += active ? 1 : 0;
       static_for<0, T::MB>([&](auto li) {
         constexpr int L = decltype(li)::value;
-        row<BG, L>(c, a.beta);
+        if (ZT > 0 || active) row<BG, ZT, L>(c, a.beta);
         if constexpr (barrier_after<BG>(L)) __syncthreads();
       });
-      bool odd = __syncthreads_or(quick_odd<BG>(c)) != 0;
-      if (!odd) odd = __syncthreads_or(rest_odd<BG>(c)) != 0;
-      active = odd;
+      if constexpr (ZT > 0) {
+        bool odd = __syncthreads_or(quick_odd<BG, ZT>(c)) != 0;
+        if (!odd) odd = __syncthreads_or(rest_odd<BG, ZT>(c)) != 0;
+        active = odd;
+      } else {
+        if (active && quick_odd<BG, ZT>(c)) flag[slot] = 1;
+        __syncthreads();
+        bool odd = active && flag[slot] != 0;
+        const bool rest = active && !odd;
+        if (__syncthreads_or(rest)) {
+          if (rest && rest_odd<BG, ZT>(c)) flag[cpb + slot] = 1;
+          __syncthreads();
+          odd = odd || (rest && flag[cpb + slot] != 0);
+        }
+        active = odd;
+      }
     }
-    write_out<BG>(&a, c, cw, used);
+    write_out<BG, ZT>(&pa, c, g, slot, z, on, used);
   }
+}
+
+// Launch shape of the any-Z kernel: codewords per CTA, threads, shared memory, CTAs.
+struct Plan {
+  int cpb = 1, threads = kThreads, smem = 0;
+  long long ctas = 0;
+};
+
+template <int BG>
+Plan plan(int z, long long batch, int sms) {
+  Plan p;
+  if (batch <= 0) return p;
+  if (z == kZ) {
+    p.smem = Layout<BG>::BYTES;
+    p.ctas = std::min<long long>(batch, std::max(sms, 1));
+    return p;
+  }
+  p.cpb = (int)std::max<long long>(1, std::min<long long>(kThreads / z, batch));
+  p.threads = ((p.cpb * z + 31) / 32) * 32;
+  p.smem = RtLayout<BG>::bytes(z, p.cpb);
+  int per_sm = 0;
+  const void* fn = (const void*)nr_f32_kernel<BG, 0>;
+  if (allow_max_dynamic_smem(fn) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nr_f32_kernel<BG, 0>, p.threads, p.smem) !=
+          cudaSuccess)
+    per_sm = 1;
+  const long long groups = (batch + p.cpb - 1) / p.cpb;
+  p.ctas = std::min<long long>(groups, (long long)std::max(per_sm, 1) * std::max(sms, 1));
+  return p;
+}
+
+template <int BG>
+size_t workspace(int z, long long batch, int sms) {
+  const Plan p = plan<BG>(z, batch, sms);
+  return (size_t)p.ctas * Layout<BG>::NEXT * kThreads * sizeof(float);
+}
+
+template <int BG>
+cudaError_t launch(const NrF32Common& c, int z, const int* shifts, int sms, cudaStream_t stream) {
+  const Plan p = plan<BG>(z, c.batch, sms);
+  if (p.ctas <= 0) return cudaSuccess;
+  F32Args<BG> a;
+  a.c = c;
+  a.z = z;
+  a.cpb = p.cpb;
+  for (int e = 0; e < Tab<BG>::E; ++e) {
+    a.sh4[e] = shifts ? shifts[e] * 4 : 0;
+    a.cz4[e] = Tab<BG>::col(e) * z * 4;
+  }
+  if (z == kZ) {
+    cudaError_t e = allow_max_dynamic_smem((const void*)nr_f32_kernel<BG, kZ>);
+    if (e != cudaSuccess) return e;
+    nr_f32_kernel<BG, kZ><<<(unsigned)p.ctas, kThreads, p.smem, stream>>>(a);
+  } else {
+    if (!shifts) return cudaErrorInvalidValue;
+    cudaError_t e = allow_max_dynamic_smem((const void*)nr_f32_kernel<BG, 0>);
+    if (e != cudaSuccess) return e;
+    nr_f32_kernel<BG, 0><<<(unsigned)p.ctas, p.threads, p.smem, stream>>>(a);
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace nrf
 
-bool nr_f32_applies(int bg, int z) { return (bg == 0 || bg == 1) && z == nrf::kZ; }
+bool nr_f32_applies(int bg, int z) { return (bg == 0 || bg == 1) && z >= 2 && z <= nrf::kZ; }
 
-size_t nr_f32_workspace_bytes(int bg, int sms) {
-  const int next = bg == 0 ? nr::Tab<0>::MB - 4 : nr::Tab<1>::MB - 4;
-  return (size_t)std::max(sms, 1) * next * nrf::kZ * sizeof(float);
+size_t nr_f32_workspace_bytes(int bg, int z, long long batch, int sms) {
+  return bg == 0 ? nrf::workspace<0>(z, batch, sms) : nrf::workspace<1>(z, batch, sms);
 }
 
-cudaError_t nr_f32_decode(int bg, const NrF32Common& c, int sms, cudaStream_t stream) {
+cudaError_t nr_f32_decode(int bg, const NrF32Common& c, int z, const int* shifts, int sms, cudaStream_t stream) {
   if (c.batch <= 0) return cudaSuccess;
-  const int ctas = (int)std::min<long long>(c.batch, std::max(sms, 1));
-  if (bg == 0) {
-    cudaError_t e = allow_max_dynamic_smem((const void*)nrf::nr_f32_kernel<0>);
-    if (e != cudaSuccess) return e;
-    nrf::nr_f32_kernel<0><<<ctas, nrf::kThreads, nrf::Layout<0>::BYTES, stream>>>(c);
-  } else {
-    cudaError_t e = allow_max_dynamic_smem((const void*)nrf::nr_f32_kernel<1>);
-    if (e != cudaSuccess) return e;
-    nrf::nr_f32_kernel<1><<<ctas, nrf::kThreads, nrf::Layout<1>::BYTES, stream>>>(c);
-  }
-  return cudaGetLastError();
+  return bg == 0 ? nrf::launch<0>(c, z, shifts, sms, stream) : nrf::launch<1>(c, z, shifts, sms, stream);
 }
 
 }  // namespace syn

@@ -96,8 +96,9 @@ cudaError_t nr_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, 
 // variable can reach the clamp.  c.cpb is chosen by the launcher.
 bool nr_pair_applies(const NrCommon& c);
 
-// f32 5G NR decode at Z = 384 with compressed messages (nr_f32_kernels.cu): the same
-// results as the generic f32 kernel.  ext_ws: nr_f32_workspace_bytes(bg, sms) bytes.
+// f32 5G NR decode with compressed messages (nr_f32_kernels.cu), any lifting size: the
+// same results as the generic f32 kernel.  ext_ws: nr_f32_workspace_bytes(bg, z, batch,
+// sms) bytes; shifts: per edge in layer order, reduced mod z.
 struct NrF32Common {
   const float* llr = nullptr;
   long long llr_stride = 0;
@@ -120,8 +121,8 @@ struct NrF32Common {
   float* ext_ws = nullptr;
 };
 bool nr_f32_applies(int bg, int z);
-size_t nr_f32_workspace_bytes(int bg, int sms);
-cudaError_t nr_f32_decode(int bg, const NrF32Common& c, int sms, cudaStream_t stream);
+size_t nr_f32_workspace_bytes(int bg, int z, long long batch, int sms);
+cudaError_t nr_f32_decode(int bg, const NrF32Common& c, int z, const int* shifts, int sms, cudaStream_t stream);
 // Paired mixed-shape kernel (same MixArgs as mixed_decode_launch; needs app_clamp >=
 // 7874).  Work items hold up to pair_mixed_capacity codewords of one shape.
 int pair_mixed_capacity(int bg, int z);

@@ -368,22 +368,23 @@ def test_f32_adversarial_inputs():
         assert 1 <= it[b] <= 6 and set(np.unique(hard[b])) <= {0, 1}
 
 
-@pytest.mark.parametrize("bg", [0, 1])
-def test_f32_nr384_compressed_kernel_matches_oracle_and_generic(bg):
-    """The f32 5G NR kernel at Z=384 (compressed messages in shared memory, extension
-    posteriors in a global workspace): bit-identical posteriors, messages, hard
-    decisions and iteration counts to the oracle and to the generic f32 kernel, with
-    the 5G prologue and filler bits, from noisy to clean channels."""
-    z = 384
+@pytest.mark.parametrize("bg,z,count", [(0, 384, 2), (1, 384, 2), (0, 128, 7), (1, 52, 17), (0, 15, 61),
+                                         (1, 2, 3), (0, 208, 3), (1, 320, 2)])
+def test_f32_nr_compressed_kernel_matches_oracle_and_generic(bg, z, count):
+    """The f32 5G NR kernel (compressed messages in shared memory, extension posteriors
+    in a global workspace; at Z < 384 several codewords per CTA, each stopping on its
+    own): bit-identical posteriors, messages, hard decisions and iteration counts to the
+    oracle and to the generic f32 kernel, with the 5G prologue and filler bits, from
+    noisy to clean channels, batches that leave the last CTA's group part-filled."""
     code = O.Code.nr(bg, z)
     dec = S.QcLdpcDecoder.with_lifting_size(bg, z, 0.5)
-    for ebno, n_filler, iters in ((0.5, 0, 6), (1.5, 120, 12), (4.0, 0, 20)):
-        _, llr = codewords(code, 2, ebno, 0xF384000 + bg * 7 + n_filler)
+    for ebno, n_filler, iters in ((0.5, 0, 6), (1.5, min(120, z), 12), (4.0, 0, 20)):
+        _, llr = codewords(code, count, ebno, 0xF384000 + bg * 7 + n_filler + z)
         ref = [code.decode_f32(code.init_5g_f32(x, n_filler), 0.5, iters) for x in llr]
         tx = np.ascontiguousarray(llr[:, 2 * z:])
         kw = dict(llr_offset=2 * z, nr_prologue=True, n_filler=n_filler)
         fast = gpu_f32(dec.set_kernel("auto"), tx, iters, **kw)
-        assert_f32_close(f"bg{bg + 1} z384 f32 {ebno} dB", ref, fast)
+        assert_f32_close(f"bg{bg + 1} z{z} f32 {ebno} dB", ref, fast)
         slow = gpu_f32(dec.set_kernel("generic"), tx, iters, **kw)
         for name in ("iters", "app", "edge_r", "hard", "hard_packed"):
             a, b = getattr(fast, name).cpu().numpy(), getattr(slow, name).cpu().numpy()
