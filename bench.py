@@ -62,6 +62,11 @@ def parse_args():
     p.add_argument("--serve-pool", type=int, default=48)
     p.add_argument("--serve-seconds", type=float, default=1.0)
     p.add_argument("--serve-step-cbs", type=int, default=1024)
+    p.add_argument("--serve-slots", type=int, default=0, help="serving steps in flight (0: the engine's default)")
+    p.add_argument("--serve-latency-steps", type=int, default=0,
+                   help="serving steps in flight without a backlog (0: the engine's default)")
+    p.add_argument("--serve-backlog", type=int, default=0,
+                   help="waiting code blocks that allow more steps in flight (0: the engine's default)")
     p.add_argument("--serve-loads", type=float, nargs="+", default=[0.1, 0.25, 0.5, 0.75],
                    help="offered loads as fractions of the measured serving capacity")
     return p.parse_args()
@@ -256,7 +261,9 @@ def serve_section(batch_gbps, dev, args):
 
     pool = make_serving_pool(args.serve_pool, 0x5E4E, dev)
     mean_bits = float(np.mean([p["tb_size"] for p in pool]))
-    server = S.Server(max_step_code_blocks=args.serve_step_cbs, iterations=ITERS, offset_beta=BETA, scale=SCALE)
+    server = S.Server(max_step_code_blocks=args.serve_step_cbs, steps_in_flight=args.serve_slots, iterations=ITERS,
+                      offset_beta=BETA, scale=SCALE, latency_steps=args.serve_latency_steps,
+                      backlog_code_blocks=args.serve_backlog)
     server.run_load(pool, offered_tb_per_s=200.0, duration_s=0.05, seed=1)  # warm-up
     # capacity: offered load well above what the engine sustains, blocks per second served
     st0 = server.stats()
@@ -288,7 +295,9 @@ def serve_section(batch_gbps, dev, args):
     server.close()
     sat_gbps = sat["info_bits_decoded"] / sat["wall_s"] / 1e9
     return {"workload": SERVE_WORKLOAD, "pool_tbs": len(pool), "mean_tb_bits": mean_bits,
-            "step_code_blocks": args.serve_step_cbs, "points": points,
+            "step_code_blocks": args.serve_step_cbs, "steps_in_flight": args.serve_slots or 6,
+            "latency_steps": args.serve_latency_steps or 3,
+            "backlog_code_blocks": args.serve_backlog or 128, "points": points,
             "capacity_tb_per_s": capacity, "saturated_decoded_gbps": sat_gbps,
             "saturated_goodput_gbps": sat["info_bits_ok"] / sat["wall_s"] / 1e9,
             "saturated_decoded_vs_batch": sat_gbps / batch_gbps, "saturation_diag": sat_diag,

@@ -417,6 +417,10 @@ typedef struct {
   float offset_beta;             /* beta_q = round(offset_beta * scale) clamped to [0, 127] */
   float scale;                   /* LLR quantizer scale (src/quantize.rs DEFAULT_SCALE = 8) */
   int32_t app_clamp;             /* posterior clamp, >= 255 */
+  uint32_t latency_steps;        /* steps in flight while few code blocks wait (0 = 3, at most
+                                    steps_in_flight): fewer steps share the SMs, each ends sooner */
+  uint32_t backlog_code_blocks;  /* waiting code blocks from which up to steps_in_flight steps
+                                    run (0 = 128) */
 } SyndromeServeConfig;
 typedef struct {
   uint64_t tb_id;

@@ -985,6 +985,9 @@ int32_t syndrome_serve_create(const SyndromeServeConfig* config, SyndromeServer*
       c.beta = config->offset_beta;
       c.scale = config->scale;
       c.app_clamp = config->app_clamp;
+      if (config->latency_steps) c.latency_slots = (int)std::min<uint32_t>(config->latency_steps, 16);
+      if (config->backlog_code_blocks)
+        c.backlog_cbs = (int)std::min<uint32_t>(config->backlog_code_blocks, 1u << 30);
     }
     auto* s = new SyndromeServer();
     std::string err;

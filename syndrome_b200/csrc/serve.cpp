@@ -97,6 +97,8 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
   if (cfg_.max_step_cbs < kMaxCbPerTb) cfg_.max_step_cbs = kMaxCbPerTb;
   if (cfg_.max_step_cbs > 65535) return fail("max_step_cbs above 65535");
   cfg_.slots = std::max(1, std::min(cfg_.slots, 16));
+  cfg_.latency_slots = std::max(1, std::min(cfg_.latency_slots, cfg_.slots));
+  if (cfg_.backlog_cbs <= 0) cfg_.backlog_cbs = 128;
   if (cfg_.harq_bytes <= 0 || cfg_.staging_bytes < 0) return fail("negative memory budget");
   if (cfg_.iterations < 0) return fail("iterations must be non-negative");
   if (cfg_.app_clamp < 255) return fail("app_clamp below 255 is not supported by the serving decoder");
@@ -244,6 +246,7 @@ int ServeEngine::submit(uint64_t id, long long tb_size, float rate, int qm, long
     pending_retx_.push_back(pd);
   else
     pending_new_.push_back(pd);
+  pending_cbs_ += t.p.c;
   stats_.max_pending =
       std::max<long long>(stats_.max_pending, (long long)(pending_retx_.size() + pending_new_.size()));
   lk.unlock();
@@ -282,6 +285,7 @@ bool ServeEngine::launch_step(Slot& s) {
         s.txs.push_back(pd);
         tbv.push_back(&t);
         first_tx.push_back(t.tx_count == 0 ? 1 : 0);
+        pending_cbs_ -= t.p.c;
         q.pop_front();
       }
     };
@@ -500,6 +504,7 @@ void ServeEngine::worker() {
             q->pop_front();
             done_.push_back(res);
           }
+        pending_cbs_ = 0;
         cv_done_.notify_all();
       }
       if (order_.empty() && pending_retx_.empty() && pending_new_.empty()) {
@@ -518,7 +523,8 @@ void ServeEngine::worker() {
       bool have;
       {
         std::lock_guard<std::mutex> lk(mu_);
-        have = (!pending_retx_.empty() || !pending_new_.empty()) && fatal_.empty();
+        have = (!pending_retx_.empty() || !pending_new_.empty()) && fatal_.empty() &&
+               ((int)order_.size() < cfg_.latency_slots || pending_cbs_ >= cfg_.backlog_cbs);
       }
       if (have && launch_step(slots_[free_slot])) {
         slots_[free_slot].busy = true;

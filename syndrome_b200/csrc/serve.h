@@ -29,6 +29,12 @@ struct ServeConfig {
   // and more, with a shorter tail near saturation (concurrent steps share the SMs, so
   // each waits for its slowest work item longer).
   int slots = 6;
+  // Steps beyond latency_slots go in flight only while at least backlog_cbs code blocks
+  // wait: a light load keeps few steps sharing the SMs (each finishes sooner), a backlog
+  // gets the concurrency that fills the SMs.  3 and 128: the same saturated throughput
+  // as 6 steps always, p99 per transmission 0.81 instead of 1.10 ms at half of capacity.
+  int latency_slots = 3;
+  int backlog_cbs = 128;
   long long harq_bytes = 8LL << 30;      // device memory for HARQ accumulators
   long long staging_bytes = 256LL << 20; // device staging of host-memory LLRs, per step
   int iterations = 8;
@@ -152,6 +158,7 @@ class ServeEngine {
   std::unordered_map<uint64_t, Tb> tbs_;
   std::deque<Pending> pending_retx_;  // transmissions of blocks that hold accumulators
   std::deque<Pending> pending_new_;   // first transmissions (need accumulators)
+  long long pending_cbs_ = 0;         // code blocks of the two queues
   std::deque<ServeResult> done_;
   ServeStats stats_;
   bool stop_ = false;

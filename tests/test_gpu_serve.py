@@ -95,12 +95,16 @@ def test_serve_matches_oracle_with_harq():
     server.close()
 
 
-def test_serve_same_result_alone_and_in_a_mix():
-    """North-star serving requirement: a result does not depend on what else is in flight."""
+@pytest.mark.parametrize("cfg", [dict(max_step_code_blocks=200),
+                                 dict(max_step_code_blocks=200, latency_steps=1, backlog_code_blocks=1),
+                                 dict(steps_in_flight=16, latency_steps=16)])
+def test_serve_same_result_alone_and_in_a_mix(cfg):
+    """A result does not depend on what else is in flight, nor on how many steps run
+    at once (the backlog policy's settings)."""
     alone = S.Server()
     d1, r1, p1 = run_sequences(alone, [CASES[3]], seed0=50)
     alone.close()
-    mixed = S.Server(max_step_code_blocks=200)
+    mixed = S.Server(**cfg)
     cases = [CASES[0], CASES[4], CASES[3], CASES[1], CASES[5], CASES[2]]
     d2, r2, p2 = run_sequences(mixed, cases, seed0=48)  # CASES[3] gets id 50 here too
     mixed.close()
