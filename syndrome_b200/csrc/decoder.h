@@ -92,6 +92,8 @@ class Decoder {
     int smem;         // dynamic shared memory bytes
     int max_ctas;     // resident CTAs on the device
     int maxdeg_tmpl;  // kernel instantiation
+    int st_words;     // f32: compressed-message state words per thread (0: messages in global memory)
+    int st_off;       // byte offset of that state in shared memory
   };
   Geometry geometry(Precision p, long long batch) const;
 

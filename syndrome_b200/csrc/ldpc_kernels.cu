@@ -38,6 +38,7 @@ namespace syn {
 namespace {
 
 constexpr int kMaxThreads = 384;
+constexpr int kCompressedSmem = 113 * 1024;  // f32 compressed-message CTA: two per SM
 
 struct KArgs {
   int z, mb, n_edges, n, k;
@@ -69,6 +70,8 @@ struct KArgs {
   long long app_stride;
   uint8_t* hard_out;
   long long hard_stride;
+  int st_words;           // f32 compressed messages: state words per thread (0: messages in r_ws / r_out)
+  int st_off;             // byte offset of the state words in shared memory
 };
 
 __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
@@ -306,6 +309,39 @@ __device__ __forceinline__ void layer_f32(const uint32_t* __restrict__ s_edge, i
   }
 }
 
+// The codewords of group grp into shared memory (the f32 kernels' load: [0, llr_offset)
+// erased, the 5G prologue or the Wi-Fi shortened-row rebuild on top).
+__device__ void load_f32_group(const KArgs& a, float* app, long long grp) {
+  const int Z = a.z, N = a.n;
+  for (int sl = 0; sl < a.cpb; ++sl) {
+    const long long cw = grp * a.cpb + sl;
+    if (cw >= a.batch) break;
+    const float* src = reinterpret_cast<const float*>(a.llr) + cw * a.llr_stride;
+    float* dst = app + (long long)sl * N;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+      float v = j >= a.llr_offset ? src[j - a.llr_offset] : 0.0f;
+      if (a.prologue) {
+        if (j < 2 * Z)
+          v = 0.0f;
+        else if (j >= a.k_prime && j < a.k)
+          v = 1000000.0f;
+      }
+      if (a.shorten) {
+        // the row holds the sent bits only: payload, then the parity that was not punctured
+        if (j < a.sh_pay)
+          v = src[j];
+        else if (j < a.k)
+          v = 1000000.0f;  // shortened: known zero (LLR_KNOWN_ZERO, wifi_rate_matching.rs:58)
+        else if (j < a.sh_par_end)
+          v = src[j - (a.k - a.sh_pay)];
+        else
+          v = 0.0f;  // punctured: erasure
+      }
+      dst[j] = v;
+    }
+  }
+}
+
 template <int MAXDEG>
 __global__ void __launch_bounds__(kMaxThreads) loms_f32_kernel(const KArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -322,33 +358,7 @@ __global__ void __launch_bounds__(kMaxThreads) loms_f32_kernel(const KArgs a) {
 
   for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     __syncthreads();
-    for (int sl = 0; sl < a.cpb; ++sl) {
-      const long long cw = grp * a.cpb + sl;
-      if (cw >= a.batch) break;
-      const float* src = reinterpret_cast<const float*>(a.llr) + cw * a.llr_stride;
-      float* dst = s.app + (long long)sl * N;
-      for (int j = threadIdx.x; j < N; j += blockDim.x) {
-        float v = j >= a.llr_offset ? src[j - a.llr_offset] : 0.0f;
-        if (a.prologue) {
-          if (j < 2 * Z)
-            v = 0.0f;
-          else if (j >= a.k_prime && j < a.k)
-            v = 1000000.0f;
-        }
-        if (a.shorten) {
-          // the row holds the sent bits only: payload, then the parity that was not punctured
-          if (j < a.sh_pay)
-            v = src[j];
-          else if (j < a.k)
-            v = 1000000.0f;  // shortened: known zero (LLR_KNOWN_ZERO, wifi_rate_matching.rs:58)
-          else if (j < a.sh_par_end)
-            v = src[j - (a.k - a.sh_pay)];
-          else
-            v = 0.0f;  // punctured: erasure
-        }
-        dst[j] = v;
-      }
-    }
+    load_f32_group(a, s.app, grp);
     __syncthreads();
 
     const long long cw = grp * a.cpb + slot;
@@ -387,6 +397,135 @@ __global__ void __launch_bounds__(kMaxThreads) loms_f32_kernel(const KArgs a) {
   }
 }
 
+// ------------------------------------------------- f32, compressed messages --
+//
+// The reference's f32 messages of a check row are a function of two magnitudes,
+// max(min1 - beta, 0) and max(min2 - beta, 0), and two bits per edge (|Q| was the row
+// minimum, R's sign), from which R_old is rebuilt bit for bit (signed zeros included).
+// loms_f32c_kernel keeps them in shared memory next to the posteriors: per thread and
+// layer two magnitude words and max(1, ceil(deg / 16)) code words, word w of thread t at
+// st[w * threads + t].  Same arithmetic, order and results as loms_f32_kernel.
+
+__device__ __forceinline__ float f32c_message(float magA, float magB, unsigned bb) {
+  return __uint_as_float(__float_as_uint((bb & 1u) ? magB : magA) | ((bb & 2u) << 30));
+}
+
+template <int MAXDEG>
+__device__ __forceinline__ void layer_f32c(const uint32_t* __restrict__ s_edge, int lb, int deg, int Z, int zi,
+                                           float* __restrict__ A, uint32_t* __restrict__ st, int ns, int mw,
+                                           int cwo, float beta) {
+  int vidx[MAXDEG];
+  float av[MAXDEG], qv[MAXDEG];
+  const float magA = __uint_as_float(st[mw * ns]), magB = __uint_as_float(st[(mw + 1) * ns]);
+  const uint32_t lo = st[cwo * ns];
+  const uint32_t hi = deg > 16 ? st[(cwo + 1) * ns] : 0u;
+  const unsigned long long bits = ((unsigned long long)hi << 32) | lo;
+  float m1 = FLT_MAX, m2 = FLT_MAX;
+  unsigned sx = 0;
+#pragma unroll
+  for (int e = 0; e < MAXDEG; ++e) {
+    if (e < deg) {
+      vidx[e] = var_index(s_edge[lb + e], zi, Z);
+      av[e] = A[vidx[e]];
+      const float q = __fsub_rn(av[e], f32c_message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u));
+      qv[e] = q;
+      const unsigned b = __float_as_uint(q);
+      const float aq = __uint_as_float(b & 0x7FFFFFFFu);
+      sx ^= b & 0x80000000u;
+      if (aq <= m1) {
+        m2 = m1;
+        m1 = aq;
+      } else if (aq < m2) {
+        m2 = aq;
+      }
+    }
+  }
+  if (m1 == FLT_MAX) m1 = 0.0f;
+  if (m2 == FLT_MAX) m2 = m1;
+  float nA = __fsub_rn(m1, beta), nB = __fsub_rn(m2, beta);  // messages of the non-minimum / minimum edges
+  if (nA < 0.0f) nA = 0.0f;
+  if (nB < 0.0f) nB = 0.0f;
+  unsigned long long nbits = 0ull;
+#pragma unroll
+  for (int e = 0; e < MAXDEG; ++e) {
+    if (e < deg) {
+      const unsigned b = __float_as_uint(qv[e]);
+      const float aq = __uint_as_float(b & 0x7FFFFFFFu);
+      const unsigned sgn = sx ^ (b & 0x80000000u);
+      const bool is_min = aq == m1;
+      const float nr = __uint_as_float(__float_as_uint(is_min ? nB : nA) | sgn);
+      const float ro = f32c_message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u);
+      A[vidx[e]] = __fadd_rn(av[e], __fsub_rn(nr, ro));
+      nbits |= (unsigned long long)((is_min ? 1u : 0u) | (sgn >> 30)) << (2 * e);
+    }
+  }
+  st[mw * ns] = __float_as_uint(nA);
+  st[(mw + 1) * ns] = __float_as_uint(nB);
+  st[cwo * ns] = (uint32_t)nbits;
+  if (deg > 16) st[(cwo + 1) * ns] = (uint32_t)(nbits >> 32);
+}
+
+template <int MAXDEG>
+__global__ void __launch_bounds__(kMaxThreads) loms_f32c_kernel(const KArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Smem<float> s = carve<float>(smem_raw, a);
+  for (int i = threadIdx.x; i < a.n_edges; i += blockDim.x) s.edge[i] = a.edge[i];
+  for (int i = threadIdx.x; i <= a.mb; i += blockDim.x) s.loff[i] = a.loff[i];
+
+  const int Z = a.z, ns = (int)blockDim.x;
+  const int slot = threadIdx.x / Z;
+  const int zi = threadIdx.x - slot * Z;
+  const bool lane_ok = slot < a.cpb;
+  const long long ngroups = (a.batch + a.cpb - 1) / a.cpb;
+  uint32_t* st = reinterpret_cast<uint32_t*>(smem_raw + a.st_off) + threadIdx.x;
+
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    __syncthreads();
+    load_f32_group(a, s.app, grp);
+    for (int w = 0; w < a.st_words; ++w) st[w * ns] = 0u;  // R = +0 before the first iteration
+    __syncthreads();
+
+    const long long cw = grp * a.cpb + slot;
+    bool active = lane_ok && cw < a.batch;
+    float* A = s.app + (long long)(lane_ok ? slot : 0) * a.n;
+    int used = 0;
+    for (int it = 0; it < a.iterations; ++it) {
+      if (!__syncthreads_or(active)) break;
+      if (active) ++used;
+      int cwo = 2 * a.mb;  // code words follow the 2 * mb magnitude words
+      for (int l = 0; l < a.mb; ++l) {
+        const int lb = s.loff[l], deg = s.loff[l + 1] - lb;
+        if (active) layer_f32c<MAXDEG>(s.edge, lb, deg, Z, zi, A, st, ns, 2 * l, cwo, a.beta);
+        cwo += max(1, (deg + 15) >> 4);
+        __syncthreads();
+      }
+      if (lane_ok && zi == 0) s.fail[slot] = 0;
+      __syncthreads();
+      if (active && syndrome_fails(s.edge, s.loff, a.mb, Z, zi, A)) s.fail[slot] = 1;
+      __syncthreads();
+      if (active && s.fail[slot] == 0) active = false;
+    }
+    if (lane_ok && cw < a.batch) {
+      if (zi == 0 && a.iters) a.iters[cw] = used;
+      if (a.r_out) {  // the messages in the reference's edge_r layout, rebuilt from the state
+        float* Rz = reinterpret_cast<float*>(a.r_out) + cw * a.r_out_stride + zi;
+        int cwo = 2 * a.mb;
+        for (int l = 0; l < a.mb; ++l) {
+          const int lb = s.loff[l], deg = s.loff[l + 1] - lb;
+          const float magA = __uint_as_float(st[2 * l * ns]), magB = __uint_as_float(st[(2 * l + 1) * ns]);
+          const unsigned long long bits =
+              ((unsigned long long)(deg > 16 ? st[(cwo + 1) * ns] : 0u) << 32) | st[cwo * ns];
+          for (int e = 0; e < deg; ++e)
+            Rz[(long long)(lb + e) * Z] = f32c_message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u);
+          cwo += max(1, (deg + 15) >> 4);
+        }
+      }
+    }
+    __syncthreads();
+    write_outputs<float>(a, s, grp);
+  }
+}
+
 typedef void (*KernelFn)(const KArgs);
 
 int pick_maxdeg(int maxdeg) {
@@ -398,7 +537,17 @@ int pick_maxdeg(int maxdeg) {
   return -1;
 }
 
-KernelFn kernel_for(Precision p, int tmpl) {
+KernelFn kernel_for(Precision p, int tmpl, bool compressed = false) {
+  if (p == Precision::kF32 && compressed) {
+    switch (tmpl) {
+      case 8: return loms_f32c_kernel<8>;
+      case 12: return loms_f32c_kernel<12>;
+      case 16: return loms_f32c_kernel<16>;
+      case 20: return loms_f32c_kernel<20>;
+      case 24: return loms_f32c_kernel<24>;
+    }
+    return nullptr;
+  }
   if (p == Precision::kInt8) {
     switch (tmpl) {
       case 8: return loms_i8_kernel<8>;
@@ -490,7 +639,21 @@ Decoder::Geometry Decoder::geometry(Precision p, long long batch) const {
   geo.threads = ((cpb * Z + 31) / 32) * 32;
   geo.smem = table_bytes(g_.edges(), g_.mb, cpb) + (int)(cpb * N * elem);
   geo.maxdeg_tmpl = pick_maxdeg(g_.maxdeg);
-  KernelFn fn = kernel_for(p, geo.maxdeg_tmpl);
+  geo.st_words = 0;
+  geo.st_off = 0;
+  if (p == Precision::kF32) {
+    // compressed messages in shared memory when two CTAs still fit an SM
+    int words = 2 * g_.mb;
+    for (int l = 0; l < g_.mb; ++l) words += std::max(1, (g_.layer_off[l + 1] - g_.layer_off[l] + 15) / 16);
+    const long long off = align16(geo.smem);
+    const long long total = off + (long long)geo.threads * words * 4;
+    if (total <= kCompressedSmem) {
+      geo.st_words = words;
+      geo.st_off = (int)off;
+      geo.smem = (int)total;
+    }
+  }
+  KernelFn fn = kernel_for(p, geo.maxdeg_tmpl, geo.st_words > 0);
   allow_max_dynamic_smem((const void*)fn);
   int per_sm = 0, sms = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, geo.threads, geo.smem);
@@ -593,7 +756,7 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
   const Geometry geo = geometry(p, req.batch);
   const long long groups = (req.batch + geo.cpb - 1) / geo.cpb;
   const long long ctas = std::min<long long>(groups, geo.max_ctas);
-  if (!req.edge_r) {
+  if (!req.edge_r && geo.st_words == 0) {
     const long long elem = p == Precision::kInt8 ? 1 : 4;
     const long long need = ctas * geo.cpb * g_.edge_buffer() * elem;
     if (!req.workspace || (long long)req.workspace_bytes < need) return bad("workspace too small");
@@ -632,7 +795,9 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
   a.app_stride = req.app_stride;
   a.hard_out = req.hard;
   a.hard_stride = req.hard_stride;
-  KernelFn fn = kernel_for(p, geo.maxdeg_tmpl);
+  a.st_words = geo.st_words;
+  a.st_off = geo.st_off;
+  KernelFn fn = kernel_for(p, geo.maxdeg_tmpl, geo.st_words > 0);
   fn<<<(unsigned)ctas, geo.threads, geo.smem, stream>>>(a);
   return cudaGetLastError();
 }
