@@ -293,8 +293,10 @@ int32_t syndrome_ldpc_decode_batch_i8_noalloc(const SyndromeLdpcDecoder* decoder
  * paired 5G NR kernel when it applies, else the 5G NR kernel, else the generic
  * layered kernel), 1 = always the generic kernel, 2 = require the 5G NR kernel,
  * 3 = require the paired 5G NR kernel (two codewords per 32-bit word; needs
- * app_clamp >= 3938, or >= 7874 with filler bits).  2 and 3 return INVALID_PARAM
- * on a request they cannot serve.  All kernels produce identical results. */
+ * app_clamp >= 3938, or >= 7874 with filler bits), 4 = the generic kernel with its
+ * check-to-variable messages in global memory (1 keeps them compressed in shared
+ * memory where they fit).  2 and 3 return INVALID_PARAM on a request they cannot
+ * serve.  All kernels produce identical results. */
 int32_t syndrome_ldpc_decoder_set_kernel(SyndromeLdpcDecoder* decoder, int32_t kernel);
 /* ----------------------------------------------- mixed-shape batches ---- */
 /* One codeword of a mixed 5G NR int8 batch.  No counterpart in the reference

@@ -101,8 +101,9 @@ def tune_tiles(shapes, codewords=None, candidates=None, iterations=8, ebno_db=1.
 
 def tune_kernel(bg, z, batch=None, iterations=8, ebno_db=1.5, repeats=3, offset_beta=0.5, quant=None, seed=0,
                 log=None):
-    """The fastest kernel name ("pair", "nr" or "generic") for plain batches of one
-    (bg, z) shape at quant.app_clamp; kernels that do not apply are skipped."""
+    """The fastest kernel name ("pair", "nr", "generic" or "generic_global") for plain
+    batches of one (bg, z) shape at quant.app_clamp; kernels that do not apply are
+    skipped."""
     import torch
 
     from . import _lib
@@ -115,7 +116,7 @@ def tune_kernel(bg, z, batch=None, iterations=8, ebno_db=1.5, repeats=3, offset_
     out = {"hard_packed": torch.empty((batch, (k + 31) // 32), dtype=torch.int32, device=llr.device),
            "iters": torch.empty((batch,), dtype=torch.int32, device=llr.device)}
     best = None
-    for name in ("pair", "nr", "generic"):
+    for name in ("pair", "nr", "generic", "generic_global"):
         dec.set_kernel(name)
 
         def run():

@@ -55,7 +55,9 @@ struct BatchRequest {
   void* edge_r = nullptr;            // [batch][edge_r_stride] final C->V messages, reference layout
   long long edge_r_stride = 0;
   // Kernel selection: 0 = automatic, 1 = generic layered kernel, 2 = 5G NR kernel,
-  // 3 = paired 5G NR kernel (two codewords per 32-bit word).
+  // 3 = paired 5G NR kernel (two codewords per 32-bit word), 4 = generic layered
+  // kernel with its messages in global memory (1 compresses them into shared memory
+  // where they fit).
   int kernel = 0;
   // Scratch for C->V messages when edge_r is null.
   void* workspace = nullptr;
@@ -95,7 +97,8 @@ class Decoder {
     int st_words;     // f32: compressed-message state words per thread (0: messages in global memory)
     int st_off;       // byte offset of that state in shared memory
   };
-  Geometry geometry(Precision p, long long batch) const;
+  // compress: messages compressed in shared memory where they fit (else in global memory)
+  Geometry geometry(Precision p, long long batch, bool compress = true) const;
 
  private:
   Graph g_;

@@ -189,6 +189,30 @@ __device__ void write_outputs(const KArgs& a, const Smem<App>& s, long long grp)
   }
 }
 
+// The codewords of group grp into shared memory (the int8 kernels' load: int8 or int16
+// input, [0, llr_offset) erased, the 5G prologue, the posterior clamp).
+__device__ void load_i8_group(const KArgs& a, int16_t* app, long long grp) {
+  const int Z = a.z, N = a.n, C = a.app_clamp;
+  for (int sl = 0; sl < a.cpb; ++sl) {
+    const long long cw = grp * a.cpb + sl;
+    if (cw >= a.batch) break;
+    const int8_t* src8 = reinterpret_cast<const int8_t*>(a.llr) + cw * a.llr_stride;
+    const int16_t* src16 = reinterpret_cast<const int16_t*>(a.llr) + cw * a.llr_stride;
+    int16_t* dst = app + (long long)sl * N;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+      int v = 0;
+      if (j >= a.llr_offset) v = a.llr_i16 ? (int)src16[j - a.llr_offset] : (int)src8[j - a.llr_offset];
+      if (a.prologue) {
+        if (j < 2 * Z)
+          v = 0;
+        else if (j >= a.k_prime && j < a.k)
+          v = C;
+      }
+      dst[j] = (int16_t)min(max(v, -C), C);
+    }
+  }
+}
+
 template <int MAXDEG>
 __global__ void __launch_bounds__(kMaxThreads) loms_i8_kernel(const KArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -205,24 +229,7 @@ __global__ void __launch_bounds__(kMaxThreads) loms_i8_kernel(const KArgs a) {
 
   for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     __syncthreads();
-    for (int sl = 0; sl < a.cpb; ++sl) {
-      const long long cw = grp * a.cpb + sl;
-      if (cw >= a.batch) break;
-      const int8_t* src8 = reinterpret_cast<const int8_t*>(a.llr) + cw * a.llr_stride;
-      const int16_t* src16 = reinterpret_cast<const int16_t*>(a.llr) + cw * a.llr_stride;
-      int16_t* dst = s.app + (long long)sl * N;
-      for (int j = threadIdx.x; j < N; j += blockDim.x) {
-        int v = 0;
-        if (j >= a.llr_offset) v = a.llr_i16 ? (int)src16[j - a.llr_offset] : (int)src8[j - a.llr_offset];
-        if (a.prologue) {
-          if (j < 2 * Z)
-            v = 0;
-          else if (j >= a.k_prime && j < a.k)
-            v = C;
-        }
-        dst[j] = (int16_t)min(max(v, -C), C);
-      }
-    }
+    load_i8_group(a, s.app, grp);
     __syncthreads();
 
     const long long cw = grp * a.cpb + slot;
@@ -254,6 +261,131 @@ __global__ void __launch_bounds__(kMaxThreads) loms_i8_kernel(const KArgs a) {
       if (used == 0 && a.r_out) {
         int8_t* Rz = reinterpret_cast<int8_t*>(a.r_out) + cw * a.r_out_stride;
         for (long long j = zi; j < ez; j += Z) Rz[j] = 0;
+      }
+    }
+    __syncthreads();
+    write_outputs<int16_t>(a, s, grp);
+  }
+}
+
+// ------------------------------------------------ int8, compressed messages --
+//
+// The int8 messages of a check row are +-max(m1 - beta_q, 0) on the edges whose |Q| is
+// not the row minimum and +-max(m2 - beta_q, 0) on those that are (qc_ldpc.rs:1700-1718),
+// so a row is one word (both magnitudes, 0..127, in bytes 0 and 1) plus two bits per edge
+// (|Q| == m1, R negative).  loms_i8c_kernel keeps that in shared memory: per thread and
+// layer one magnitude word and max(1, ceil(deg / 16)) code words, word w of thread t
+// at st[w * threads + t].  Same arithmetic and results as loms_i8_kernel.
+
+__device__ __forceinline__ int i8c_message(uint32_t mags, unsigned bb) {
+  const int mag = (int)((mags >> ((bb & 1u) << 3)) & 0xFFu);
+  return (bb & 2u) ? -mag : mag;
+}
+
+template <int MAXDEG>
+__device__ __forceinline__ void layer_i8c(const uint32_t* __restrict__ s_edge, int lb, int deg, int Z, int zi,
+                                          int16_t* __restrict__ A, uint32_t* __restrict__ st, int ns, int mw,
+                                          int cwo, int beta_q, int C) {
+  int vidx[MAXDEG], av[MAXDEG], qv[MAXDEG], ro[MAXDEG];
+  const uint32_t mags = st[mw * ns];
+  const uint32_t lo = st[cwo * ns];
+  const uint32_t hi = deg > 16 ? st[(cwo + 1) * ns] : 0u;
+  const unsigned long long bits = ((unsigned long long)hi << 32) | lo;
+  int m1 = 127, m2 = 127;
+  unsigned sx = 0;
+#pragma unroll
+  for (int e = 0; e < MAXDEG; ++e) {
+    if (e < deg) {
+      vidx[e] = var_index(s_edge[lb + e], zi, Z);
+      av[e] = A[vidx[e]];
+      ro[e] = i8c_message(mags, (unsigned)(bits >> (2 * e)) & 3u);
+      const int q = min(max(av[e] - ro[e], -127), 127);
+      qv[e] = q;
+      const int aq = abs(q);
+      sx ^= (unsigned)q;
+      const int om1 = m1;
+      m1 = min(om1, aq);
+      m2 = min(m2, max(om1, aq));
+    }
+  }
+  if (deg < 2) {
+    if (deg == 0) m1 = 0;
+    m2 = m1;
+  }
+  const int nA = max(m1 - beta_q, 0), nB = max(m2 - beta_q, 0);
+  unsigned long long nbits = 0ull;
+#pragma unroll
+  for (int e = 0; e < MAXDEG; ++e) {
+    if (e < deg) {
+      const int q = qv[e];
+      const int aq = abs(q);
+      const bool is_min = aq == m1;
+      const int mag = is_min ? nB : nA;
+      const bool neg = ((sx ^ (unsigned)q) >> 31) != 0u;
+      const int nr = neg ? -mag : mag;
+      A[vidx[e]] = (int16_t)min(max(av[e] + nr - ro[e], -C), C);
+      nbits |= (unsigned long long)((is_min ? 1u : 0u) | (neg ? 2u : 0u)) << (2 * e);
+    }
+  }
+  st[mw * ns] = (uint32_t)nA | ((uint32_t)nB << 8);
+  st[cwo * ns] = (uint32_t)nbits;
+  if (deg > 16) st[(cwo + 1) * ns] = (uint32_t)(nbits >> 32);
+}
+
+template <int MAXDEG>
+__global__ void __launch_bounds__(kMaxThreads) loms_i8c_kernel(const KArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Smem<int16_t> s = carve<int16_t>(smem_raw, a);
+  for (int i = threadIdx.x; i < a.n_edges; i += blockDim.x) s.edge[i] = a.edge[i];
+  for (int i = threadIdx.x; i <= a.mb; i += blockDim.x) s.loff[i] = a.loff[i];
+
+  const int Z = a.z, C = a.app_clamp, ns = (int)blockDim.x;
+  const int slot = threadIdx.x / Z;
+  const int zi = threadIdx.x - slot * Z;
+  const bool lane_ok = slot < a.cpb;
+  const long long ngroups = (a.batch + a.cpb - 1) / a.cpb;
+  uint32_t* st = reinterpret_cast<uint32_t*>(smem_raw + a.st_off) + threadIdx.x;
+
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    __syncthreads();
+    load_i8_group(a, s.app, grp);
+    for (int w = 0; w < a.st_words; ++w) st[w * ns] = 0u;  // R = 0 before the first iteration
+    __syncthreads();
+
+    const long long cw = grp * a.cpb + slot;
+    bool active = lane_ok && cw < a.batch;
+    int16_t* A = s.app + (long long)(lane_ok ? slot : 0) * a.n;
+    int used = 0;
+    for (int it = 0; it < a.iterations; ++it) {
+      if (!__syncthreads_or(active)) break;
+      if (active) ++used;
+      int cwo = a.mb;  // code words follow the mb magnitude words
+      for (int l = 0; l < a.mb; ++l) {
+        const int lb = s.loff[l], deg = s.loff[l + 1] - lb;
+        if (active) layer_i8c<MAXDEG>(s.edge, lb, deg, Z, zi, A, st, ns, l, cwo, a.beta_q, C);
+        cwo += max(1, (deg + 15) >> 4);
+        __syncthreads();
+      }
+      if (lane_ok && zi == 0) s.fail[slot] = 0;
+      __syncthreads();
+      if (active && syndrome_fails(s.edge, s.loff, a.mb, Z, zi, A)) s.fail[slot] = 1;
+      __syncthreads();
+      if (active && s.fail[slot] == 0) active = false;
+    }
+    if (lane_ok && cw < a.batch) {
+      if (zi == 0 && a.iters) a.iters[cw] = used;
+      if (a.r_out) {  // the messages in the reference's edge_r layout, rebuilt from the state
+        int8_t* Rz = reinterpret_cast<int8_t*>(a.r_out) + cw * a.r_out_stride + zi;
+        int cwo = a.mb;
+        for (int l = 0; l < a.mb; ++l) {
+          const int lb = s.loff[l], deg = s.loff[l + 1] - lb;
+          const uint32_t mags = st[l * ns];
+          const unsigned long long bits =
+              ((unsigned long long)(deg > 16 ? st[(cwo + 1) * ns] : 0u) << 32) | st[cwo * ns];
+          for (int e = 0; e < deg; ++e)
+            Rz[(long long)(lb + e) * Z] = (int8_t)i8c_message(mags, (unsigned)(bits >> (2 * e)) & 3u);
+          cwo += max(1, (deg + 15) >> 4);
+        }
       }
     }
     __syncthreads();
@@ -415,7 +547,7 @@ __device__ __forceinline__ void layer_f32c(const uint32_t* __restrict__ s_edge, 
                                            float* __restrict__ A, uint32_t* __restrict__ st, int ns, int mw,
                                            int cwo, float beta) {
   int vidx[MAXDEG];
-  float av[MAXDEG], qv[MAXDEG];
+  float av[MAXDEG], qv[MAXDEG], ro[MAXDEG];
   const float magA = __uint_as_float(st[mw * ns]), magB = __uint_as_float(st[(mw + 1) * ns]);
   const uint32_t lo = st[cwo * ns];
   const uint32_t hi = deg > 16 ? st[(cwo + 1) * ns] : 0u;
@@ -427,7 +559,8 @@ __device__ __forceinline__ void layer_f32c(const uint32_t* __restrict__ s_edge, 
     if (e < deg) {
       vidx[e] = var_index(s_edge[lb + e], zi, Z);
       av[e] = A[vidx[e]];
-      const float q = __fsub_rn(av[e], f32c_message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u));
+      ro[e] = f32c_message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u);
+      const float q = __fsub_rn(av[e], ro[e]);
       qv[e] = q;
       const unsigned b = __float_as_uint(q);
       const float aq = __uint_as_float(b & 0x7FFFFFFFu);
@@ -454,8 +587,7 @@ __device__ __forceinline__ void layer_f32c(const uint32_t* __restrict__ s_edge, 
       const unsigned sgn = sx ^ (b & 0x80000000u);
       const bool is_min = aq == m1;
       const float nr = __uint_as_float(__float_as_uint(is_min ? nB : nA) | sgn);
-      const float ro = f32c_message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u);
-      A[vidx[e]] = __fadd_rn(av[e], __fsub_rn(nr, ro));
+      A[vidx[e]] = __fadd_rn(av[e], __fsub_rn(nr, ro[e]));
       nbits |= (unsigned long long)((is_min ? 1u : 0u) | (sgn >> 30)) << (2 * e);
     }
   }
@@ -538,6 +670,16 @@ int pick_maxdeg(int maxdeg) {
 }
 
 KernelFn kernel_for(Precision p, int tmpl, bool compressed = false) {
+  if (p == Precision::kInt8 && compressed) {
+    switch (tmpl) {
+      case 8: return loms_i8c_kernel<8>;
+      case 12: return loms_i8c_kernel<12>;
+      case 16: return loms_i8c_kernel<16>;
+      case 20: return loms_i8c_kernel<20>;
+      case 24: return loms_i8c_kernel<24>;
+    }
+    return nullptr;
+  }
   if (p == Precision::kF32 && compressed) {
     switch (tmpl) {
       case 8: return loms_f32c_kernel<8>;
@@ -627,7 +769,7 @@ bool Decoder::init(const Graph& g, float offset_beta, std::string* err) {
   return cudaGetLastError() == cudaSuccess;
 }
 
-Decoder::Geometry Decoder::geometry(Precision p, long long batch) const {
+Decoder::Geometry Decoder::geometry(Precision p, long long batch, bool compress) const {
   Geometry geo{};
   const int elem = p == Precision::kInt8 ? 2 : 4;
   const int Z = g_.z;
@@ -641,9 +783,10 @@ Decoder::Geometry Decoder::geometry(Precision p, long long batch) const {
   geo.maxdeg_tmpl = pick_maxdeg(g_.maxdeg);
   geo.st_words = 0;
   geo.st_off = 0;
-  if (p == Precision::kF32) {
-    // compressed messages in shared memory when two CTAs still fit an SM
-    int words = 2 * g_.mb;
+  if (compress) {
+    // compressed messages in shared memory when two CTAs still fit an SM: per layer
+    // two magnitude words (f32) or one (int8, both magnitudes in bytes), then code words
+    int words = (p == Precision::kF32 ? 2 : 1) * g_.mb;
     for (int l = 0; l < g_.mb; ++l) words += std::max(1, (g_.layer_off[l + 1] - g_.layer_off[l] + 15) / 16);
     const long long off = align16(geo.smem);
     const long long total = off + (long long)geo.threads * words * 4;
@@ -663,7 +806,9 @@ Decoder::Geometry Decoder::geometry(Precision p, long long batch) const {
 }
 
 size_t Decoder::workspace_bytes(Precision p, long long batch) const {
-  const Geometry geo = geometry(p, batch);
+  // the messages of the global-memory kernel (kernel 4, or where the compressed state
+  // does not fit shared memory); the compressed kernels need none
+  const Geometry geo = geometry(p, batch, false);
   const long long groups = (batch + geo.cpb - 1) / geo.cpb;
   const long long ctas = std::min<long long>(groups, geo.max_ctas);
   const long long elem = p == Precision::kInt8 ? 1 : 4;
@@ -698,7 +843,8 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
   }
   const bool nr_ok = p == Precision::kInt8 && nr_bg_ >= 0 && !req.llr_i16 && req.app_clamp >= 255;
   if ((req.kernel == 2 || req.kernel == 3) && !nr_ok) return bad("the 5G NR kernel does not apply to this request");
-  if (nr_ok && req.kernel != 1) {
+  const bool generic_only = req.kernel == 1 || req.kernel == 4;
+  if (nr_ok && !generic_only) {
     NrCommon c{};
     c.z = g_.z;
     c.beta_q = req.beta_q;
@@ -729,7 +875,7 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
   }
   // f32 5G NR: the compressed-message kernel, when the caller's workspace holds its
   // extension posteriors (else the generic kernel below).
-  if (p == Precision::kF32 && nr_bg_ >= 0 && nr_f32_applies(nr_bg_, g_.z) && !req.shorten && req.kernel != 1 &&
+  if (p == Precision::kF32 && nr_bg_ >= 0 && nr_f32_applies(nr_bg_, g_.z) && !req.shorten && !generic_only &&
       req.workspace && req.workspace_bytes >= nr_f32_workspace_bytes(nr_bg_, g_.z, req.batch, sms_)) {
     NrF32Common c;
     c.llr = static_cast<const float*>(req.llr);
@@ -753,7 +899,7 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
     c.ext_ws = static_cast<float*>(req.workspace);
     return nr_f32_decode(nr_bg_, c, g_.z, g_.shifts.data(), sms_, stream);
   }
-  const Geometry geo = geometry(p, req.batch);
+  const Geometry geo = geometry(p, req.batch, req.kernel != 4);
   const long long groups = (req.batch + geo.cpb - 1) / geo.cpb;
   const long long ctas = std::min<long long>(groups, geo.max_ctas);
   if (!req.edge_r && geo.st_words == 0) {
@@ -868,7 +1014,7 @@ cudaError_t Decoder::decode_i8_noalloc(const BatchRequest& req, cudaStream_t str
   void* scratch = nullptr;
   e = noalloc_scratch(cur, &scratch);
   if (e != cudaSuccess) return e;
-  const Geometry geo = geometry(Precision::kInt8, req.batch);
+  const Geometry geo = geometry(Precision::kInt8, req.batch, false);
   const long long per_cta = (long long)geo.cpb * g_.edge_buffer();
   if (per_cta > (long long)kNoAllocScratchBytes)
     return bad("the messages of one CTA (" + std::to_string(per_cta) + " bytes) exceed the " +

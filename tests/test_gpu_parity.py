@@ -49,7 +49,7 @@ def gpu_i8(dec, llr_i8, iters, quant, kernel="auto", **kw):
     return r
 
 
-KERNELS = ["generic", "nr", "pair"]
+KERNELS = ["generic", "generic_global", "nr", "pair"]
 
 
 def assert_i8_equal(label, ref, r):
@@ -168,11 +168,13 @@ def test_int8_pair_kernel_lanes_finish_apart(count):
         assert_i8_equal(f"pair z{z} count{count}", refs, r)
 
 
-def test_int8_wifi_matrices():
-    """tests/ldpc_int8_kernel_equivalence.rs:217-236."""
-    for z, rn, rd in ((27, 1, 2), (54, 2, 3), (81, 5, 6), (27, 3, 4)):
+@pytest.mark.parametrize("kernel", ["auto", "generic_global"])
+def test_int8_wifi_matrices(kernel):
+    """tests/ldpc_int8_kernel_equivalence.rs:217-236 (auto: messages compressed in
+    shared memory; generic_global: in global memory)."""
+    for z, rn, rd in ((27, 1, 2), (54, 2, 3), (81, 5, 6), (27, 3, 4), (81, 1, 2)):
         code = O.Code.wifi(z, rn, rd)
-        dec = S.wifi_ldpc_decoder(z, rn, rd, 0.5)
+        dec = S.wifi_ldpc_decoder(z, rn, rd, 0.5).set_kernel(kernel)
         for ebno in (1.0, 3.0):
             _, llr = codewords(code, 5, ebno, 0x01F10000 ^ (z << 4) ^ rd)
             apps = np.stack([O.quantize_i16(x) for x in llr])
@@ -302,17 +304,23 @@ def test_f32_golden_convergence_trajectory():
     assert int(r.iters[0]) == g["iterations_used"]
 
 
+@pytest.mark.parametrize("kernel", ["auto", "generic_global"])
 @pytest.mark.parametrize("kind,a,b", [("nr", 0, 32), ("nr", 1, 52), ("nr", 0, 384), ("wifi", 27, (1, 2)),
-                                      ("wifi", 81, (5, 6)), ("wifi", 54, (3, 4))])
-def test_f32_graphs(kind, a, b):
+                                      ("wifi", 81, (5, 6)), ("wifi", 54, (3, 4)), ("wifi", 81, (2, 3)),
+                                      ("nr", 0, 2)])
+def test_f32_graphs(kind, a, b, kernel):
+    """auto: the 5G NR f32 kernel or the generic kernel with messages compressed in
+    shared memory (every 802.11 matrix; 5G NR at small Z); generic_global: messages in
+    global memory."""
     if kind == "nr":
         code, dec = O.Code.nr(a, b), S.QcLdpcDecoder.with_lifting_size(a, b, 0.5)
     else:
         code, dec = O.Code.wifi(a, *b), S.wifi_ldpc_decoder(a, *b, 0.5)
+    dec.set_kernel(kernel)
     for ebno in (0.5, 2.0):
         _, llr = codewords(code, 3, ebno, 0xF320000 + code.z)
         ref = [code.decode_f32(x, 0.5, 20) for x in llr]
-        assert_f32_close(f"{kind} {a} {b} {ebno}", ref, gpu_f32(dec, llr, 20))
+        assert_f32_close(f"{kind} {a} {b} {ebno} {kernel}", ref, gpu_f32(dec, llr, 20))
 
 
 def test_f32_5g_prologue_and_drop_in():
