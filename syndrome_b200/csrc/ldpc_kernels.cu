@@ -105,6 +105,84 @@ __device__ __forceinline__ int var_index(uint32_t w, int zi, int Z) {
   return (int)(w >> 16) + r;
 }
 
+// The two smallest of v[0..D) (min1, then the second smallest counting ties: the
+// reference's sequential rule "|Q| <= min1: min2 = min1, min1 = |Q|; else |Q| < min2:
+// min2 = |Q|" started at FLT_MAX, whose result does not depend on the order) as a
+// pairwise min/max tree: depth log2(D) instead of a D-long dependent chain.  The
+// caller clamps each |Q| to FLT_MAX first (fminf drops NaN), which is what the
+// sequential rule does with +inf and NaN (never taken), so the pair is bit-identical.
+template <int N>
+__device__ __forceinline__ void merge_min2(float* lo, float* hi) {
+  if constexpr (N > 1) {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const float l1 = lo[2 * i], l2 = lo[2 * i + 1], h = fminf(hi[2 * i], hi[2 * i + 1]);
+      lo[i] = fminf(l1, l2);
+      hi[i] = fminf(fmaxf(l1, l2), h);
+    }
+    if constexpr ((N & 1) != 0) {
+      lo[N / 2] = lo[N - 1];
+      hi[N / 2] = hi[N - 1];
+    }
+    merge_min2<(N + 1) / 2>(lo, hi);
+  }
+}
+template <int D>
+__device__ __forceinline__ void min2_tree(const float* v, float& m1, float& m2) {
+  constexpr int P = (D + 1) / 2;
+  float lo[P], hi[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    if (2 * i + 1 < D) {
+      lo[i] = fminf(v[2 * i], v[2 * i + 1]);
+      hi[i] = fmaxf(v[2 * i], v[2 * i + 1]);
+    } else {
+      lo[i] = v[2 * i];
+      hi[i] = FLT_MAX;
+    }
+  }
+  merge_min2<P>(lo, hi);
+  m1 = lo[0];
+  m2 = hi[0];
+}
+
+// Integer form of min2_tree (int8 path: |Q| <= 127, padding 127, the start of both
+// minima in qc_ldpc.rs's int8 pass).
+template <int N>
+__device__ __forceinline__ void merge_min2_i(int* lo, int* hi) {
+  if constexpr (N > 1) {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const int l1 = lo[2 * i], l2 = lo[2 * i + 1], h = min(hi[2 * i], hi[2 * i + 1]);
+      lo[i] = min(l1, l2);
+      hi[i] = min(max(l1, l2), h);
+    }
+    if constexpr ((N & 1) != 0) {
+      lo[N / 2] = lo[N - 1];
+      hi[N / 2] = hi[N - 1];
+    }
+    merge_min2_i<(N + 1) / 2>(lo, hi);
+  }
+}
+template <int D>
+__device__ __forceinline__ void min2_tree_i(const int* v, int& m1, int& m2) {
+  constexpr int P = (D + 1) / 2;
+  int lo[P], hi[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    if (2 * i + 1 < D) {
+      lo[i] = min(v[2 * i], v[2 * i + 1]);
+      hi[i] = max(v[2 * i], v[2 * i + 1]);
+    } else {
+      lo[i] = v[2 * i];
+      hi[i] = 127;
+    }
+  }
+  merge_min2_i<P>(lo, hi);
+  m1 = lo[0];
+  m2 = hi[0];
+}
+
 // ---------------------------------------------------------------- int8 path --
 
 template <int MAXDEG>
@@ -291,10 +369,12 @@ __device__ __forceinline__ void layer_i8c(const uint32_t* __restrict__ s_edge, i
   const uint32_t lo = st[cwo * ns];
   const uint32_t hi = deg > 16 ? st[(cwo + 1) * ns] : 0u;
   const unsigned long long bits = ((unsigned long long)hi << 32) | lo;
-  int m1 = 127, m2 = 127;
+  constexpr bool kTree = MAXDEG >= 16;  // as in layer_f32c
+  int m1 = 127, m2 = 127, ak[MAXDEG];
   unsigned sx = 0;
 #pragma unroll
   for (int e = 0; e < MAXDEG; ++e) {
+    ak[e] = 127;  // edges past deg: 127, the starting value of both minima
     if (e < deg) {
       vidx[e] = var_index(s_edge[lb + e], zi, Z);
       av[e] = A[vidx[e]];
@@ -303,11 +383,16 @@ __device__ __forceinline__ void layer_i8c(const uint32_t* __restrict__ s_edge, i
       qv[e] = q;
       const int aq = abs(q);
       sx ^= (unsigned)q;
-      const int om1 = m1;
-      m1 = min(om1, aq);
-      m2 = min(m2, max(om1, aq));
+      if constexpr (kTree) {
+        ak[e] = aq;
+      } else {
+        const int om1 = m1;
+        m1 = min(om1, aq);
+        m2 = min(m2, max(om1, aq));
+      }
     }
   }
+  if constexpr (kTree) min2_tree_i<MAXDEG>(ak, m1, m2);
   if (deg < 2) {
     if (deg == 0) m1 = 0;
     m2 = m1;
@@ -552,10 +637,14 @@ __device__ __forceinline__ void layer_f32c(const uint32_t* __restrict__ s_edge, 
   const uint32_t lo = st[cwo * ns];
   const uint32_t hi = deg > 16 ? st[(cwo + 1) * ns] : 0u;
   const unsigned long long bits = ((unsigned long long)hi << 32) | lo;
-  float m1 = FLT_MAX, m2 = FLT_MAX;
+  // rows of up to 12 edges: the sequential rule (the tree's extra registers would cost
+  // a resident CTA); longer rows: the tree
+  constexpr bool kTree = MAXDEG >= 16;
+  float m1 = FLT_MAX, m2 = FLT_MAX, ak[MAXDEG];
   unsigned sx = 0;
 #pragma unroll
   for (int e = 0; e < MAXDEG; ++e) {
+    ak[e] = FLT_MAX;  // edges past deg: FLT_MAX, which the two smallest never need
     if (e < deg) {
       vidx[e] = var_index(s_edge[lb + e], zi, Z);
       av[e] = A[vidx[e]];
@@ -565,7 +654,9 @@ __device__ __forceinline__ void layer_f32c(const uint32_t* __restrict__ s_edge, 
       const unsigned b = __float_as_uint(q);
       const float aq = __uint_as_float(b & 0x7FFFFFFFu);
       sx ^= b & 0x80000000u;
-      if (aq <= m1) {
+      if constexpr (kTree) {
+        ak[e] = fminf(aq, FLT_MAX);
+      } else if (aq <= m1) {
         m2 = m1;
         m1 = aq;
       } else if (aq < m2) {
@@ -573,6 +664,7 @@ __device__ __forceinline__ void layer_f32c(const uint32_t* __restrict__ s_edge, 
       }
     }
   }
+  if constexpr (kTree) min2_tree<MAXDEG>(ak, m1, m2);
   if (m1 == FLT_MAX) m1 = 0.0f;
   if (m2 == FLT_MAX) m2 = m1;
   float nA = __fsub_rn(m1, beta), nB = __fsub_rn(m2, beta);  // messages of the non-minimum / minimum edges

@@ -122,6 +122,47 @@ struct Ctx {
   __device__ __forceinline__ void st_ext(int i, float v) const { ext[i * kThreads] = v; }
 };
 
+// The two smallest of v[0..D) (min1, then the second smallest counting ties: the
+// reference's sequential rule "|Q| <= min1: min2 = min1, min1 = |Q|; else |Q| < min2:
+// min2 = |Q|" started at FLT_MAX, whose result does not depend on the order) as a
+// pairwise min/max tree: depth log2(D) instead of a D-long dependent chain.  The
+// caller clamps each |Q| to FLT_MAX first (fminf drops NaN), which is what the
+// sequential rule does with +inf and NaN (never taken), so the pair is bit-identical.
+template <int N>
+__device__ __forceinline__ void merge_min2(float* lo, float* hi) {
+  if constexpr (N > 1) {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const float l1 = lo[2 * i], l2 = lo[2 * i + 1], h = fminf(hi[2 * i], hi[2 * i + 1]);
+      lo[i] = fminf(l1, l2);
+      hi[i] = fminf(fmaxf(l1, l2), h);
+    }
+    if constexpr ((N & 1) != 0) {
+      lo[N / 2] = lo[N - 1];
+      hi[N / 2] = hi[N - 1];
+    }
+    merge_min2<(N + 1) / 2>(lo, hi);
+  }
+}
+template <int D>
+__device__ __forceinline__ void min2_tree(const float* v, float& m1, float& m2) {
+  constexpr int P = (D + 1) / 2;
+  float lo[P], hi[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    if (2 * i + 1 < D) {
+      lo[i] = fminf(v[2 * i], v[2 * i + 1]);
+      hi[i] = fmaxf(v[2 * i], v[2 * i + 1]);
+    } else {
+      lo[i] = v[2 * i];
+      hi[i] = FLT_MAX;
+    }
+  }
+  merge_min2<P>(lo, hi);
+  m1 = lo[0];
+  m2 = hi[0];
+}
+
 // R_old of edge e from the row's magnitudes and the edge's two code bits
 // (bit 0: |Q| was the row minimum, bit 1: R's sign).
 __device__ __forceinline__ float message(float magA, float magB, unsigned bb) {
@@ -142,7 +183,7 @@ __device__ __forceinline__ void row(const Ctx<BG, ZT>& c, float beta) {
   const uint32_t hi = w1 != w0 ? c.ld_code(w1) : 0u;
   const unsigned long long word = ((unsigned long long)hi << 32) | lo;
   const unsigned long long bits = word >> sh;
-  float m1 = FLT_MAX, m2 = FLT_MAX;
+  float m1, m2, ak[deg];
   unsigned sx = 0u;
   static_for<0, deg>([&](auto ei) {
     constexpr int e = decltype(ei)::value;
@@ -154,15 +195,10 @@ __device__ __forceinline__ void row(const Ctx<BG, ZT>& c, float beta) {
     const float q = __fsub_rn(av[e], ro);
     qv[e] = q;
     const unsigned b = __float_as_uint(q);
-    const float aq = __uint_as_float(b & 0x7FFFFFFFu);
+    ak[e] = fminf(__uint_as_float(b & 0x7FFFFFFFu), FLT_MAX);
     sx ^= b & 0x80000000u;
-    if (aq <= m1) {
-      m2 = m1;
-      m1 = aq;
-    } else if (aq < m2) {
-      m2 = aq;
-    }
   });
+  min2_tree<deg>(ak, m1, m2);
   if (m1 == FLT_MAX) m1 = 0.0f;
   if (m2 == FLT_MAX) m2 = m1;
   float nA = __fsub_rn(m1, beta), nB = __fsub_rn(m2, beta);  // messages of the non-minimum / minimum edges
