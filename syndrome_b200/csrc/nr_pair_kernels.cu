@@ -204,6 +204,15 @@ __device__ __noinline__ void write_rows(const DevCtx<BG, ZT, APC>* cx, const NrC
   }
 }
 
+// A codeword's stored channel LLRs (bytes [0, bytes) of its row) into L2, one 128-byte
+// line per thread and step: issued for the CTA's next group while this one decodes, so
+// that the next load phase reads L2 instead of waiting on HBM.  Every address lies
+// inside the row.
+__device__ __noinline__ void prefetch_row_l2(const int8_t* row, long long bytes, int z, int Z) {
+  for (long long i = 128LL * z; i < bytes; i += 128LL * Z)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(row + i)));
+}
+
 template <int BG, int ZT, bool FILL>
 __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_constant__ PairArgs<BG> a) {
   using T = Tab<BG>;
@@ -278,6 +287,10 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
       });
 #pragma unroll 1
       for (int w = 0; w < NW; ++w) st_base[w * ns + tid] = 0u;
+      const long long gn = (grp + gridDim.x) * P + p;  // this slot's next codeword pair
+      const long long row_bytes = (long long)T::NB * Z - c.llr_offset;
+      if (2 * gn < c.batch) prefetch_row_l2(c.llr + 2 * gn * c.llr_stride, row_bytes, z, Z);
+      if (2 * gn + 1 < c.batch) prefetch_row_l2(c.llr + (2 * gn + 1) * c.llr_stride, row_bytes, z, Z);
     }
     __syncthreads();
 
