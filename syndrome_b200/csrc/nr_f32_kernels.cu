@@ -263,6 +263,13 @@ __device__ __noinline__ bool rest_odd(const Ctx<BG, ZT> c) {
   return odd;
 }
 
+// Bytes [0, bytes) of a codeword's row into L2, one 128-byte line per thread and step;
+// every address lies inside the row.
+__device__ __noinline__ void prefetch_row_l2(const char* row, long long bytes, int z, int Z) {
+  for (long long i = 128LL * z; i < bytes; i += 128LL * Z)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(row + i)));
+}
+
 // Results of the codewords of group g (out of line: keeps the iteration loop's registers
 // free).  on: this thread's row z of slot `slot` holds codeword g * cpb + slot.
 template <int BG, int ZT>
@@ -374,6 +381,10 @@ __global__ void __launch_bounds__(kThreads, 1) nr_f32_kernel(const __grid_consta
 #pragma unroll 1
       for (int i = 0; i < NEXT; ++i) c.st_ext(i, value((CORE + i) * Z + z));
     }
+    // this slot's next codeword into L2 while this one decodes (its load then reads L2)
+    if (live && (g + gridDim.x) * cpb + slot < a.batch)
+      prefetch_row_l2(reinterpret_cast<const char*>(a.llr + ((g + gridDim.x) * cpb + slot) * a.llr_stride),
+                      4LL * (T::NB * Z - a.llr_offset), z, Z);
 #pragma unroll 1
     for (int w = 0; w < LY::NMAG; ++w) c.st_mag(w, 0.0f);
 #pragma unroll 1
