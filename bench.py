@@ -160,7 +160,39 @@ def cpu_lib():
     L.cpb_pipeline_i8.argtypes = ([ctypes.c_int] * 4 + [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int,
                                    ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong])
+    L.cpb_bench_shape_ns.restype = ctypes.c_double
+    L.cpb_bench_shape_ns.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
     return L
+
+
+def oracle_data(batch, rank):
+    """The GPU arm's inputs (make_data) rebuilt without the decoder library: the same
+    seeded information bits, the oracle's encoder and channel, int8 at scale 8.  The
+    oracle's generator is byte-identical to the library's (tests/test_capi_cpu.py)."""
+    path = os.path.join(ROOT, "oracle", "liboracle.so")
+    if not os.path.exists(path):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"])
+    L = ctypes.CDLL(path)
+    vp, lg = ctypes.c_void_p, ctypes.c_long
+    L.orc_params_5g.restype = vp
+    L.orc_params_5g.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.orc_params_free.argtypes = [vp]
+    L.orc_batch_channel_i8.restype = ctypes.c_int
+    L.orc_batch_channel_i8.argtypes = [vp, vp, lg, vp, ctypes.c_float, vp, ctypes.c_float, lg, vp, lg, ctypes.c_int]
+    rng = np.random.default_rng(0x5EED0000 + rank)
+    info = rng.integers(0, 2, size=(batch, K_INFO), dtype=np.uint8)
+    seeds = np.arange(batch, dtype=np.uint64) + np.uint64(1 + rank * 10_000_000)
+    eb = np.full(batch, EBNO, np.float32)
+    llr = np.zeros((batch, N_TX), np.int8)
+    h = L.orc_params_5g(BG, Z)
+    try:
+        rc = L.orc_batch_channel_i8(h, info.ctypes.data, batch, eb.ctypes.data, RATE, seeds.ctypes.data, SCALE, PUNCT,
+                                    llr.ctypes.data, N_TX, 0)
+    finally:
+        L.orc_params_free(h)
+    if rc != 0:
+        raise RuntimeError("oracle encoder failed")
+    return info, llr
 
 
 def host_cores():
@@ -170,8 +202,35 @@ def host_cores():
         return os.cpu_count() or 1
 
 
+def cpu_info():
+    """CPU model and topology of this host, as far as /proc and /sys tell."""
+    model, sockets, phys = None, set(), set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            cur = {}
+            for ln in f:
+                if ":" in ln:
+                    k, v = (x.strip() for x in ln.split(":", 1))
+                    cur[k] = v
+                    if k == "model name" and model is None:
+                        model = v
+                elif cur:
+                    if "physical id" in cur and "core id" in cur:
+                        phys.add((cur["physical id"], cur["core id"]))
+                        sockets.add(cur["physical id"])
+                    cur = {}
+    except Exception:
+        pass
+    allowed = host_cores()
+    out = {"model": model, "threads_usable": allowed, "logical_cpus_total": os.cpu_count()}
+    if phys:
+        out["physical_cores_total"] = len(phys)
+        out["threads_per_core"] = (os.cpu_count() or 1) // max(len(phys), 1)
+    return out
+
+
 def time_cpu(llr, count, workers):
-    """Runs `count` codewords of llr through the CPU pipeline; returns (seconds, iters)."""
+    """Runs `count` codewords of llr through the CPU pipeline; returns (seconds, iters, packed)."""
     L = cpu_lib()
     x = np.ascontiguousarray(llr[:count])
     its = np.zeros(count, np.int32)
@@ -182,44 +241,93 @@ def time_cpu(llr, count, workers):
     return sec, its, packed
 
 
-def cpu_sample(llr, target_seconds):
-    """Sizes a bounded sample of the workload for about target_seconds of wall time."""
-    workers = max(1, host_cores())
-    probe = min(len(llr), 2 * workers)
+def cpu_figure(llr, target_seconds, workers, max_count=None):
+    """Information Gbit/s of `workers` pipeline threads on a sample sized for about
+    target_seconds of wall time (the first codewords of the workload)."""
+    n = len(llr) if max_count is None else min(len(llr), max_count)
+    probe = min(n, 2 * workers)
     sec, _, _ = time_cpu(llr, probe, workers)
-    per_cw = sec / probe
-    count = int(min(len(llr), max(probe, target_seconds / max(per_cw, 1e-6))))
-    sec, its, _ = time_cpu(llr, count, workers)
-    return {"value": count * K_INFO / sec / 1e9, "unit": "Gbit/s", "cores": workers, "kind": "port",
-            "sample": f"{count} of the {len(llr)} codewords, {sec:.2f} s wall, mean {its.mean():.2f} iterations; "
-                      "AVX2 int8 kernels + LdpcPipeline restated in C++ (oracle/cpu_baseline.cpp)"}
+    count = int(min(n, max(probe, target_seconds / max(sec / probe, 1e-6))))
+    sec, its, packed = time_cpu(llr, count, workers)
+    return {"value": count * K_INFO / sec / 1e9, "unit": "Gbit/s", "workers": workers, "codewords": count,
+            "seconds": sec, "mean_iterations": float(its.mean())}, its, packed
+
+
+def bench_shape_sanity():
+    """One core on the reference's own int8 benchmark (BG1 Z=384, beta 0.25, 10
+    iterations, +-0.5 input at scale 8), in its unit, beside its published figure."""
+    L = cpu_lib()
+    n = 68 * Z
+    app = np.where(np.arange(n) % 2 == 0, 4, -4).astype(np.int16)
+    used = ctypes.c_int()
+    ns = L.cpb_bench_shape_ns(BG, Z, 2, 32767, app.ctypes.data, 10, 31, ctypes.byref(used))
+    return {"melem_per_s": n * used.value / (ns * 1e-9) / 1e6, "ns_per_decode": ns, "iterations": used.value,
+            "reference_published_melem_per_s": 847.94,
+            "reference_source": "bench/results/ldpc_rust.json:4 (loms_i8_runtime_simd, its own host)"}
+
+
+def pipeline_workers():
+    """Worker threads for the all-core CPU figure: every usable host thread but one,
+    which the pipeline's submitting thread needs (it loads frames and spins on the
+    done rings; with a worker on every thread as well, measured here, 8 workers on 8
+    cores ran at 0.7x the rate of 7)."""
+    return max(1, host_cores() - 1)
+
+
+def cpu_sample(llr, target_seconds):
+    """The GPU arm's cpu_baseline leg: all host threads on a bounded sample."""
+    workers = pipeline_workers()
+    fig, its, packed = cpu_figure(llr, target_seconds, workers)
+    base = {"value": fig["value"], "unit": "Gbit/s", "cores": workers, "kind": "port",
+            "sample": f"{fig['codewords']} of the {len(llr)} codewords, {fig['seconds']:.2f} s wall, mean "
+                      f"{fig['mean_iterations']:.2f} iterations, {workers} pipeline workers; AVX2 int8 kernels + "
+                      "LdpcPipeline restated in C++ (oracle/cpu_baseline.cpp)",
+            "cpu": cpu_info()}
+    return base, its, packed
+
+
+def bench_config(batch, world):
+    """The workload description shared by both arms."""
+    return {"workload": WORKLOAD, "codewords_per_gpu": batch, "info_bits_per_codeword": K_INFO,
+            "iterations_max": ITERS, "l2": "inputs 415 MB per step > 126 MB L2 (no flush needed)",
+            "parallelism": f"replicas x{world}"}
 
 
 def run_reference(args):
+    """The reference's CPU decode path (its AVX2 int8 kernels and LdpcPipeline,
+    restated in C++) on this host's cores, timed on the same 16384 codewords per step
+    as the GPU arm.  Inputs come from the oracle, so no decoder library is loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    workers = max(1, host_cores())
-    count = min(16384, max(64, 128 * workers))
-    _, llr = make_data(count, 0)
-    time_cpu(llr, min(count, 2 * workers), workers)  # page in
-    vals = []
+    workers = pipeline_workers()
+    B = args.batch
+    _, llr = oracle_data(B, 0)
+    time_cpu(llr, min(B, 2 * workers), workers)  # page in
     for _ in range(args.warmup):
-        time_cpu(llr, count, workers)
+        time_cpu(llr, B, workers)
+    vals = []
     for _ in range(args.steps):
-        sec, its, _ = time_cpu(llr, count, workers)
+        sec, its, _ = time_cpu(llr, B, workers)
         vals.append((sec, float(its.mean())))
     tot = sum(s for s, _ in vals)
-    value = count * K_INFO * args.steps / tot / 1e9
+    value = B * K_INFO * args.steps / tot / 1e9
+    one, _, _ = cpu_figure(llr, 3.0, 1)
+    eight, _, _ = cpu_figure(llr, 3.0, min(8, workers))  # src/ldpc_pipeline.rs:375 clamps to 8 workers
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gbit/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "codewords_per_step": count,
-                   "mean_iterations": statistics.mean(i for _, i in vals)},
+        "config": bench_config(B, args.gpus),
+        "result": {"mean_iterations": statistics.mean(i for _, i in vals)},
         "cpu_baseline": {"value": value, "unit": "Gbit/s", "cores": workers, "kind": "port",
-                         "sample": f"{count} codewords per step on {workers} worker threads; AVX2 int8 kernels + "
-                                   "LdpcPipeline restated in C++ (the Rust reference has no toolchain here)"},
+                         "sample": f"all {B} codewords of the workload per step, {workers} LdpcPipeline worker "
+                                   "threads (every usable host thread but the submitting one; the reference clamps "
+                                   "its pipeline to 8 workers, reported below); AVX2 int8 kernels + LdpcPipeline "
+                                   "restated in C++ (oracle/cpu_baseline.cpp), inputs from the oracle's encoder and "
+                                   "channel",
+                         "cpu": cpu_info(), "workers_1": one, "workers_8": eight,
+                         "single_core_bench_shape": bench_shape_sanity()},
         "e2e": {"value": value, "unit": "Gbit/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -429,53 +537,70 @@ def main():
     e2e_value = whole_job_gbps(B, args.steps, world, ms_e2e)
     e2e_ok = bool(np.array_equal(h_packed.numpy(), packed.cpu().numpy()))
 
-    # ---- roofline of the decode kernel (HBM) ----
-    peak, peak_kind = measured_peaks()
+    # ---- roofline of the decode kernel ----
+    # Binding resource: instruction issue (min-sum is compare/select integer work on
+    # operands in shared memory, not a contraction, and moves ~26 KB of HBM per codeword).
+    # Instructions per edge update come from an ncu capture of this same kernel
+    # (profiles/decode_i8_bg1_z384_traffic.json names it); the edge-update rate and the
+    # launch time are measured here.
+    peak_hbm, peak_kind = measured_peaks()
     hbm_bytes = B * (N_TX + WORDS * 4 + 4)
-    achieved = hbm_bytes / (ms_per_step * 1e-3) / 1e9
-    traffic, instr_per_update = None, None
+    hbm_achieved = hbm_bytes / (ms_per_step * 1e-3) / 1e9
+    traffic, instr_per_update, capture = None, None, None
     prof = os.path.join(ROOT, "profiles", "decode_i8_bg1_z384_traffic.json")
     if os.path.exists(prof):
         with open(prof) as f:
             pj = json.load(f)
         traffic = pj["dram_bytes_per_codeword"] * B
         instr_per_update = pj.get("thread_instructions_per_codeword_edge_update")
+        capture = {"kernel": pj.get("kernel"), "capture": pj.get("capture"), "command": pj.get("source")}
     edge_updates = float(mean_iters) * 316 * Z * B
-    smem_peak = 128.0 * 148 * 1.965e9  # bytes/s: 128 B/clk/SM (one 32-lane LDS.32 per clock), 148 SMs, max clock
+    clk_sum = clk.summary()
+    sm_hz = (clk_sum["sm_mhz"] if clk_sum else 1965.0) * 1e6
+    issue_peak = 148 * 4 * 32 * sm_hz  # thread instructions/s: one warp instruction per scheduler per clock
+    smem_peak = 128.0 * 148 * sm_hz  # bytes/s: 128 B/clk/SM (32 lanes x 4 B per shared-memory wavefront)
+    upd_per_s = edge_updates / (ms_per_step * 1e-3)
+    roofline = {"bound": "hbm", "achieved": hbm_achieved, "peak": peak_hbm, "unit": "GB/s",
+                "frac": hbm_achieved / peak_hbm, "traffic": traffic, "peak_source": peak_kind}
+    if instr_per_update is not None:
+        issue = upd_per_s * instr_per_update
+        roofline = {"bound": "issue", "achieved": issue / 1e12, "peak": issue_peak / 1e12,
+                    "unit": "T thread-instructions/s", "frac": issue / issue_peak, "traffic": traffic,
+                    "instructions_per_edge_update": instr_per_update, "edge_updates_per_s": upd_per_s,
+                    "peak_note": "148 SMs x 4 schedulers x 32 lanes x the median SM clock sampled in the timed region",
+                    "capture": capture,
+                    "hbm": {"achieved": hbm_achieved, "peak": peak_hbm, "unit": "GB/s", "frac": hbm_achieved / peak_hbm,
+                            "algorithmic_bytes_per_codeword": N_TX + WORDS * 4 + 4, "traffic": traffic,
+                            "peak_source": peak_kind}}
+    smem = {"edge_updates_per_s": upd_per_s, "algorithmic_bytes_per_update": 6,
+            "achieved_GBps": upd_per_s * 6 / 1e9, "peak_GBps": smem_peak / 1e9, "frac": upd_per_s * 6 / smem_peak,
+            "note": "int8 path: i16 posterior read for Q plus i16 posterior read-modify-write per edge update; the "
+                    "peak is the 128 B/clk/SM specification figure, not a measurement"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "Gbit/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "codewords_per_gpu": B, "info_bits_per_codeword": K_INFO,
-                   "kernel": args.kernel,
-                   "mean_iterations": mean_iters, "frames_correct": int(frame_ok.sum()),
-                   "l2": "inputs 415 MB per step > 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"},
+        "config": bench_config(B, world),
+        "result": {"kernel": args.kernel, "mean_iterations": mean_iters, "frames_correct": int(frame_ok.sum())},
         "e2e": {"value": e2e_value, "unit": "Gbit/s", "h2d_bytes_per_step": int(B * N_TX),
                 "d2h_bytes_per_step": int(B * (WORDS * 4 + 4)), "chunks": nchunk, "outputs_match": e2e_ok},
         "gpu_launches": args.steps,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_codeword": N_TX + WORDS * 4 + 4,
-                     "note": "LOMS is issue/shared-memory bound, not HBM bound; see smem"},
-        "issue": None if instr_per_update is None else {
-            "note": "binding resource: SM instruction issue (integer ALU pipe); instructions per edge update "
-                    "from the committed ncu profile, edge updates per second measured here",
-            "thread_instructions_per_edge_update": instr_per_update,
-            "achieved_thread_instr_per_s": edge_updates / (ms_per_step * 1e-3) * instr_per_update,
-            "peak_thread_instr_per_s": 148 * 4 * 32 * 1.965e9,
-            "frac": edge_updates / (ms_per_step * 1e-3) * instr_per_update / (148 * 4 * 32 * 1.965e9)},
-        "smem": {"edge_updates_per_s": edge_updates / (ms_per_step * 1e-3),
-                 "algorithmic_bytes_per_update": 4,
-                 "achieved_GBps": edge_updates * 4 / (ms_per_step * 1e-3) / 1e9,
-                 "peak_GBps": smem_peak / 1e9,
-                 "frac": edge_updates * 4 / (ms_per_step * 1e-3) / smem_peak},
+        "roofline": roofline,
+        "smem": smem,
     }
-    clk = clk.summary()
-    if clk:
-        line["clocks"] = clk
+    if clk_sum:
+        line["clocks"] = clk_sum
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(llr_h, args.cpu_seconds)
+        base, c_its, c_packed = cpu_sample(llr_h, args.cpu_seconds)
+        m = len(c_its)
+        g_its = iters.cpu().numpy()[:m]
+        g_packed = packed.cpu().numpy().view(np.uint32)[:m]
+        bad = int(((g_its != c_its) | (g_packed != c_packed).any(axis=1)).sum())
+        line["cpu_baseline"] = base
+        line["parity_vs_cpu"] = {"mismatches": bad, "of": m,
+                                 "compared": "iteration count and packed information bits of each codeword of the "
+                                             "CPU sample, GPU output of the timed launches vs the CPU pipeline"}
     if rank == 0 and world == 1 and not args.no_serve:
         line["serve"] = serve_section(value, dev, args)
     if rank == 0:

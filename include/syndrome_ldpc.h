@@ -276,9 +276,14 @@ int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const
  * SYNDROME_NOALLOC_SCRATCH_BYTES / (codewords per CTA * edges * Z) CTAs; a code whose
  * per-CTA messages exceed the array is rejected with SYNDROME_INVALID_PARAM.  The
  * first call on a device looks up the array's address (cudaGetSymbolAddress), so make
- * that first call before any stream capture.  Nothing in the array must start at zero
+ * that first call before any stream capture; the address is kept for the process, so
+ * calls must not cross a cudaDeviceReset.  Nothing in the array must start at zero
  * and it keeps the last call's contents; calls that overlap on the GPU share the
- * array and race.  The current device must be the decoder's. */
+ * array and race.  The current device must be the decoder's.  The array is used when
+ * d_edge_r is NULL (with d_edge_r the messages go there instead).  The kernel choice
+ * of syndrome_ldpc_decoder_set_kernel does not apply: this entry always runs the
+ * generic layered kernel with its messages in global memory, the throughput of
+ * kernel 4; every call also queries the kernel's occupancy on the host. */
 #define SYNDROME_NOALLOC_SCRATCH_BYTES (32u << 20)
 int32_t syndrome_ldpc_decode_batch_i8_noalloc(const SyndromeLdpcDecoder* decoder,
                                               const int8_t* d_llr, size_t llr_stride,

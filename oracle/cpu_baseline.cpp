@@ -377,6 +377,30 @@ int cpb_decode_i8(int bg, int z, int beta_q, int app_clamp, int16_t* app, int8_t
   return used;
 }
 
+// Median single-threaded decode time (ns) of the reference's own int8 benchmark shape
+// (src/bin/ldpc_bench_export.rs:111-215: every variable's LLR +0.5 / -0.5 alternating,
+// quantized at the default scale, no 5G prologue, a fixed iteration count that never
+// converges), over `reps` decodes of one preallocated frame on the calling thread.
+double cpb_bench_shape_ns(int bg, int z, int beta_q, int app_clamp, const int16_t* app0, int iterations,
+                         int reps, int* iters_used) {
+  Layout L;
+  if (!make_layout(bg, z, &L) || reps < 1) return -1.0;
+  Frame f;
+  init_frame(L, f);
+  std::vector<double> ns;
+  int used = 0;
+  for (int r = 0; r < reps; ++r) {
+    std::copy(app0, app0 + L.n(), f.app.begin());
+    const auto t0 = std::chrono::steady_clock::now();
+    used = decode_i8_avx2(L, beta_q, std::max(app_clamp, 0), f, iterations);
+    const auto t1 = std::chrono::steady_clock::now();
+    ns.push_back(std::chrono::duration<double, std::nano>(t1 - t0).count());
+  }
+  if (iters_used) *iters_used = used;
+  std::sort(ns.begin(), ns.end());
+  return ns[ns.size() / 2];
+}
+
 // Decodes `count` codewords (int8 channel rows, variables [llr_offset, n)) through
 // the restated LdpcPipeline with `workers` spinning worker threads.  Writes the
 // iterations used per codeword and the packed hard bits of the first `hard_bits`

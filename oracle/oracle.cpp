@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <thread>
 #include <vector>
 #include <algorithm>
 
@@ -967,6 +968,135 @@ long orc_wifi_decode_shortened(const void* h, float beta, long payload_bits, con
   for (long i = 0; i < par; ++i) codeword_llr[k + i] = rx[payload_bits + i];
   for (long i = k + par; i < n; ++i) codeword_llr[i] = 0.0f;
   return orc_decode_f32(h, beta, codeword_llr, edge_r, hard, iterations, nullptr);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ batch helpers --
+// Threaded loops over the single-codeword functions above, so that the checker and
+// the CPU reference arm can cover the benchmark's batch sizes without loading the
+// decoder library.  Every codeword runs the same single-threaded code as the
+// per-codeword entries; threads only split the batch.
+
+namespace {
+
+template <class F>
+void orc_parallel(long count, int threads, F&& f) {
+  if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  threads = (int)std::min<long>(threads, std::max<long>(count, 1));
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([=, &f]() {
+      for (long b = t; b < count; b += threads) f(b);
+    });
+  for (auto& th : pool) th.join();
+}
+
+void orc_pack(const uint8_t* hard, long bits, uint32_t* dst) {
+  for (long w = 0; w < (bits + 31) / 32; ++w) {
+    uint32_t m = 0;
+    for (long b = 0; b < 32 && w * 32 + b < bits; ++b) m |= (uint32_t)(hard[w * 32 + b] & 1u) << b;
+    dst[w] = m;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Info bits [count][K] -> codewords (orc_encode) -> BPSK/AWGN over all N bits with
+// seed seeds[b] (orc_awgn_transmit) -> int8 LLRs of bits [tx_begin, N) at `scale`
+// (orc_quantize_i16, which saturates at +-127) into out[b * out_stride ...].
+// Returns 0, or -1 if a codeword could not be encoded.
+int orc_batch_channel_i8(void* h, const uint8_t* info, long count, const float* ebno, float rate,
+                         const uint64_t* seeds, float scale, long tx_begin, int8_t* out, long out_stride,
+                         int threads) {
+  Params* p = static_cast<Params*>(h);
+  ensure_encoder(p);  // built once here, read-only in the threads
+  const long n = (long)p->nb * p->z, k = (long)(p->nb - p->mb) * p->z;
+  std::vector<int> rc((size_t)std::max<long>(count, 1), 0);
+  orc_parallel(count, threads, [&](long b) {
+    std::vector<uint8_t> cw((size_t)n);
+    std::vector<float> llr((size_t)n);
+    std::vector<int16_t> q((size_t)n);
+    rc[(size_t)b] = orc_encode(p, info + b * k, cw.data());
+    orc_awgn_transmit(ebno[b], rate, seeds[b], cw.data(), n, llr.data());
+    orc_quantize_i16(llr.data(), q.data(), n, scale);
+    for (long i = tx_begin; i < n; ++i) out[b * out_stride + (i - tx_begin)] = (int8_t)q[(size_t)i];
+  });
+  for (long b = 0; b < count; ++b)
+    if (rc[(size_t)b] != 0) return -1;
+  return 0;
+}
+
+// int8 decode of a batch the way the batched device API sees it: row b holds the
+// int8 channel values of variables [llr_offset, N); the punctured [0, llr_offset)
+// are zero; with nr_prologue the 5G prologue (orc_prologue_5g_i8: filler to
+// app_clamp, the first 2Z to 0) follows.  Writes iterations, the packed hard
+// decisions of the first hard_bits variables, and for the first `detail` codewords
+// the final posteriors [N] and messages [E*Z].
+void orc_decode_i8_batch(const void* h, int beta_q, int app_clamp, const int8_t* llr, long llr_stride,
+                         long llr_offset, int nr_prologue, long n_filler, long count, long iterations,
+                         int threads, int32_t* iters, uint32_t* packed, long hard_bits, long words_stride,
+                         int16_t* app_out, int8_t* edge_r_out, long detail) {
+  const Params* p = static_cast<const Params*>(h);
+  const long n = (long)p->nb * p->z, ez = (long)p->cols.size() * p->z;
+  orc_parallel(count, threads, [&](long b) {
+    std::vector<int16_t> app((size_t)n, 0);
+    std::vector<int8_t> er((size_t)ez);
+    std::vector<uint8_t> hard((size_t)n);
+    for (long i = llr_offset; i < n; ++i) app[(size_t)i] = llr[b * llr_stride + (i - llr_offset)];
+    if (nr_prologue) orc_prologue_5g_i8(p, app.data(), n_filler, app_clamp);
+    iters[b] = (int32_t)orc_decode_i8(p, beta_q, app_clamp, app.data(), er.data(), hard.data(), iterations);
+    if (packed) orc_pack(hard.data(), hard_bits, packed + b * words_stride);
+    if (b < detail) {
+      if (app_out) std::copy(app.begin(), app.end(), app_out + b * n);
+      if (edge_r_out) std::copy(er.begin(), er.end(), edge_r_out + b * ez);
+    }
+  });
+}
+
+// f32 counterpart: row b holds the f32 channel LLRs of variables [llr_offset, N);
+// with nr_prologue orc_init_5g_f32 runs first.  Final posteriors of the first
+// `detail` codewords go to app_out.
+void orc_decode_f32_batch(const void* h, float beta, const float* llr, long llr_stride, long llr_offset,
+                          int nr_prologue, long n_filler, long count, long iterations, int threads,
+                          int32_t* iters, uint32_t* packed, long hard_bits, long words_stride, float* app_out,
+                          long detail) {
+  const Params* p = static_cast<const Params*>(h);
+  const long n = (long)p->nb * p->z, ez = (long)p->cols.size() * p->z;
+  orc_parallel(count, threads, [&](long b) {
+    std::vector<float> app((size_t)n, 0.0f), er((size_t)ez);
+    std::vector<uint8_t> hard((size_t)n);
+    for (long i = llr_offset; i < n; ++i) app[(size_t)i] = llr[b * llr_stride + (i - llr_offset)];
+    if (nr_prologue) orc_init_5g_f32(p, app.data(), n_filler);
+    iters[b] = (int32_t)orc_decode_f32(p, beta, app.data(), er.data(), hard.data(), iterations, nullptr);
+    if (packed) orc_pack(hard.data(), hard_bits, packed + b * words_stride);
+    if (b < detail && app_out) std::copy(app.begin(), app.end(), app_out + b * n);
+  });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// f32 counterpart of orc_batch_channel_i8: the channel LLRs of bits [tx_begin, N).
+int orc_batch_channel_f32(void* h, const uint8_t* info, long count, const float* ebno, float rate,
+                          const uint64_t* seeds, long tx_begin, float* out, long out_stride, int threads) {
+  Params* p = static_cast<Params*>(h);
+  ensure_encoder(p);
+  const long n = (long)p->nb * p->z, k = (long)(p->nb - p->mb) * p->z;
+  std::vector<int> rc((size_t)std::max<long>(count, 1), 0);
+  orc_parallel(count, threads, [&](long b) {
+    std::vector<uint8_t> cw((size_t)n);
+    std::vector<float> llr((size_t)n);
+    rc[(size_t)b] = orc_encode(p, info + b * k, cw.data());
+    orc_awgn_transmit(ebno[b], rate, seeds[b], cw.data(), n, llr.data());
+    for (long i = tx_begin; i < n; ++i) out[b * out_stride + (i - tx_begin)] = llr[(size_t)i];
+  });
+  for (long b = 0; b < count; ++b)
+    if (rc[(size_t)b] != 0) return -1;
+  return 0;
 }
 
 }  // extern "C"

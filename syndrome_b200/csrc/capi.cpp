@@ -553,6 +553,9 @@ int32_t syndrome_ldpc_decode_batch_i8(const SyndromeLdpcDecoder* decoder, const 
   });
 }
 
+static_assert(SYNDROME_NOALLOC_SCRATCH_BYTES == syn::Decoder::kNoAllocScratchBytes,
+              "the header's allocation-free scratch size must be the kernel's");
+
 int32_t syndrome_ldpc_decode_batch_i8_noalloc(const SyndromeLdpcDecoder* decoder, const int8_t* d_llr,
                                               size_t llr_stride, size_t llr_offset, size_t batch,
                                               int32_t nr_prologue, size_t n_filler, size_t iterations,

@@ -85,7 +85,10 @@ class Decoder {
   // Generic int8 decode with its message scratch in a static device array instead
   // of a caller workspace: allocates nothing.  See ldpc_kernels.cu for the limits.
   cudaError_t decode_i8_noalloc(const BatchRequest& req, cudaStream_t stream, std::string* err) const;
-  static size_t noalloc_scratch_bytes();
+  // Size of that static array (the public header's SYNDROME_NOALLOC_SCRATCH_BYTES,
+  // checked equal at compile time in capi.cpp).
+  static constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+  static constexpr size_t noalloc_scratch_bytes() { return kNoAllocScratchBytes; }
 
   // Kernel launch geometry chosen for this code (exposed for the tuner and tests).
   struct Geometry {

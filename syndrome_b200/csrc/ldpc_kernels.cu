@@ -1060,7 +1060,7 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
 // ordering) share the array and race.
 
 namespace {
-constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+constexpr size_t kNoAllocScratchBytes = Decoder::kNoAllocScratchBytes;
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[kNoAllocMaxDevices] = {};
@@ -1069,7 +1069,10 @@ void* g_noalloc_addr[kNoAllocMaxDevices] = {};
 static __device__ __align__(256) int8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Device address of the static scratch on the current device, looked up once per
-// device (the first call on a device does the lookup).
+// device (the first call on a device does the lookup) and kept for the life of the
+// process: a cudaDeviceReset, or anything else that tears down and recreates the
+// device's primary context, leaves the kept address stale, so calls must not cross
+// one.
 static cudaError_t noalloc_scratch(int device, void** out) {
   if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
@@ -1082,8 +1085,6 @@ static cudaError_t noalloc_scratch(int device, void** out) {
   *out = g_noalloc_addr[device];
   return cudaSuccess;
 }
-
-size_t Decoder::noalloc_scratch_bytes() { return kNoAllocScratchBytes; }
 
 cudaError_t Decoder::decode_i8_noalloc(const BatchRequest& req, cudaStream_t stream, std::string* err) const {
   auto bad = [&](const std::string& m) {

@@ -289,3 +289,85 @@ def wifi_decode_shortened(code, beta, payload_bits, rx, iterations):
                                        edge_r.ctypes.data, hard.ctypes.data, iterations)
     assert used >= 0
     return dict(iters=int(used), llr=cw, edge_r=edge_r, hard=hard)
+
+
+# ---- threaded batch helpers (same single-codeword code, the batch split over threads) ----
+def _batch_lib():
+    L = lib()
+    if not getattr(L, "_batch_bound", False):
+        vp, lg = ctypes.c_void_p, ctypes.c_long
+        L.orc_batch_channel_i8.restype = ctypes.c_int
+        L.orc_batch_channel_i8.argtypes = [vp, vp, lg, vp, ctypes.c_float, vp, ctypes.c_float, lg, vp, lg,
+                                           ctypes.c_int]
+        L.orc_batch_channel_f32.restype = ctypes.c_int
+        L.orc_batch_channel_f32.argtypes = [vp, vp, lg, vp, ctypes.c_float, vp, lg, vp, lg, ctypes.c_int]
+        L.orc_decode_i8_batch.restype = None
+        L.orc_decode_i8_batch.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, lg, lg, ctypes.c_int, lg, lg, lg,
+                                          ctypes.c_int, vp, vp, lg, lg, vp, vp, lg]
+        L.orc_decode_f32_batch.restype = None
+        L.orc_decode_f32_batch.argtypes = [vp, ctypes.c_float, vp, lg, lg, ctypes.c_int, lg, lg, lg, ctypes.c_int,
+                                           vp, vp, lg, lg, vp, lg]
+        L._batch_bound = True
+    return L
+
+
+def batch_channel_i8(code, info, ebno, rate, seeds, scale=8.0, tx_begin=0, threads=0):
+    """info [count, K] -> int8 LLRs [count, N - tx_begin]: oracle encoder, the reference
+    channel over all N bits (seed per row), quantized at `scale`."""
+    info = np.ascontiguousarray(info, dtype=np.uint8)
+    count = info.shape[0]
+    eb = np.ascontiguousarray(np.broadcast_to(np.asarray(ebno, dtype=np.float32), (count,)))
+    sd = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64).reshape(count))
+    out = np.zeros((count, code.n - tx_begin), dtype=np.int8)
+    rc = _batch_lib().orc_batch_channel_i8(code.h, info.ctypes.data, count, eb.ctypes.data, rate, sd.ctypes.data,
+                                           scale, tx_begin, out.ctypes.data, out.shape[1], threads)
+    assert rc == 0
+    return out
+
+
+def batch_channel_f32(code, info, ebno, rate, seeds, tx_begin=0, threads=0):
+    """info [count, K] -> f32 channel LLRs [count, N - tx_begin] (oracle encoder + channel)."""
+    info = np.ascontiguousarray(info, dtype=np.uint8)
+    count = info.shape[0]
+    eb = np.ascontiguousarray(np.broadcast_to(np.asarray(ebno, dtype=np.float32), (count,)))
+    sd = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64).reshape(count))
+    out = np.zeros((count, code.n - tx_begin), dtype=np.float32)
+    rc = _batch_lib().orc_batch_channel_f32(code.h, info.ctypes.data, count, eb.ctypes.data, rate, sd.ctypes.data,
+                                            tx_begin, out.ctypes.data, out.shape[1], threads)
+    assert rc == 0
+    return out
+
+
+def decode_i8_batch(code, llr, beta_q, iterations, llr_offset=0, nr_prologue=False, n_filler=0, app_clamp=32767,
+                    hard_bits=None, detail=0, threads=0):
+    """Oracle int8 decode of int8 rows [count, N - llr_offset] (the batched device API's
+    input).  Returns iters [count], packed hard bits [count, words] and, for the first
+    `detail` codewords, posteriors [detail, N] and messages [detail, E*Z]."""
+    llr = np.ascontiguousarray(llr, dtype=np.int8)
+    count = llr.shape[0]
+    hb = code.n if hard_bits is None else hard_bits
+    words = (hb + 31) // 32
+    iters = np.zeros(count, np.int32)
+    packed = np.zeros((count, words), np.uint32)
+    app = np.zeros((max(detail, 0), code.n), np.int16)
+    er = np.zeros((max(detail, 0), code.edges * code.z), np.int8)
+    _batch_lib().orc_decode_i8_batch(code.h, beta_q, app_clamp, llr.ctypes.data, llr.shape[1], llr_offset,
+                                     1 if nr_prologue else 0, n_filler, count, iterations, threads, iters.ctypes.data,
+                                     packed.ctypes.data, hb, words, app.ctypes.data, er.ctypes.data, detail)
+    return dict(iters=iters, packed=packed, app=app, edge_r=er)
+
+
+def decode_f32_batch(code, llr, beta, iterations, llr_offset=0, nr_prologue=False, n_filler=0, hard_bits=None,
+                     detail=0, threads=0):
+    """Oracle f32 decode of f32 rows [count, N - llr_offset]."""
+    llr = np.ascontiguousarray(llr, dtype=np.float32)
+    count = llr.shape[0]
+    hb = code.n if hard_bits is None else hard_bits
+    words = (hb + 31) // 32
+    iters = np.zeros(count, np.int32)
+    packed = np.zeros((count, words), np.uint32)
+    app = np.zeros((max(detail, 0), code.n), np.float32)
+    _batch_lib().orc_decode_f32_batch(code.h, beta, llr.ctypes.data, llr.shape[1], llr_offset,
+                                      1 if nr_prologue else 0, n_filler, count, iterations, threads,
+                                      iters.ctypes.data, packed.ctypes.data, hb, words, app.ctypes.data, detail)
+    return dict(iters=iters, packed=packed, app=app)

@@ -13,6 +13,18 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 
 
-REFERENCE_ROOT = os.environ.get("SYNDROME_REFERENCE_ROOT", "/root/reference")
+def _reference_root():
+    """The reference tree the oracle's recipe reads (oracle/Makefile, `print-ref`)."""
+    import subprocess
+
+    try:
+        out = subprocess.run(["make", "-s", "--no-print-directory", "-C", os.path.join(ROOT, "oracle"), "print-ref"],
+                             capture_output=True, text=True, timeout=30)
+        return out.stdout.strip()
+    except Exception:
+        return ""
+
+
+REFERENCE_ROOT = _reference_root()
 HAVE_REFERENCE = os.path.isdir(os.path.join(REFERENCE_ROOT, "src"))
 needs_reference = pytest.mark.skipif(not HAVE_REFERENCE, reason="reference source tree not present")
