@@ -57,7 +57,7 @@ def parse_args():
     p.add_argument("--chunks", type=int, default=8, help="e2e copy/compute pipeline depth")
     p.add_argument("--cpu-seconds", type=float, default=8.0, help="target CPU work of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--kernel", choices=["auto", "generic", "nr", "pair"], default="auto")
+    p.add_argument("--kernel", choices=["auto", "generic", "nr", "pair", "pair_smem"], default="auto")
     p.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     p.add_argument("--serve-pool", type=int, default=48)
     p.add_argument("--serve-seconds", type=float, default=1.0)

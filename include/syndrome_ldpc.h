@@ -300,8 +300,11 @@ int32_t syndrome_ldpc_decode_batch_i8_noalloc(const SyndromeLdpcDecoder* decoder
  * 3 = require the paired 5G NR kernel (two codewords per 32-bit word; needs
  * app_clamp >= 3938, or >= 7874 with filler bits), 4 = the generic kernel with its
  * check-to-variable messages in global memory (1 keeps them compressed in shared
- * memory where they fit).  2 and 3 return INVALID_PARAM on a request they cannot
- * serve.  All kernels produce identical results. */
+ * memory where they fit), 5 = the paired kernel with all its check-row state in
+ * shared memory, one codeword pair per SM (at Z = 384, 0 and 3 run the variant that
+ * keeps most of that state in tensor memory, two pairs per SM).  2, 3 and 5 return
+ * INVALID_PARAM on a request they cannot serve.  All kernels produce identical
+ * results. */
 int32_t syndrome_ldpc_decoder_set_kernel(SyndromeLdpcDecoder* decoder, int32_t kernel);
 /* ----------------------------------------------- mixed-shape batches ---- */
 /* One codeword of a mixed 5G NR int8 batch.  No counterpart in the reference

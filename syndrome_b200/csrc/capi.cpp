@@ -194,7 +194,7 @@ const char* syndrome_last_error(void) { return g_last_error.c_str(); }
 
 int32_t syndrome_ldpc_decoder_set_kernel(SyndromeLdpcDecoder* decoder, int32_t kernel) {
   if (!decoder) return SYNDROME_NULL_POINTER;
-  if (kernel < 0 || kernel > 4) return fail(SYNDROME_INVALID_PARAM, "kernel must be 0, 1, 2, 3 or 4");
+  if (kernel < 0 || kernel > 5) return fail(SYNDROME_INVALID_PARAM, "kernel must be 0 to 5");
   decoder->kernel = kernel;
   return SYNDROME_OK;
 }

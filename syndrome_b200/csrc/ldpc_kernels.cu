@@ -934,7 +934,8 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
     if (req.llr_stride < req.shorten_tx) return bad("llr_stride smaller than the transmitted bits");
   }
   const bool nr_ok = p == Precision::kInt8 && nr_bg_ >= 0 && !req.llr_i16 && req.app_clamp >= 255;
-  if ((req.kernel == 2 || req.kernel == 3) && !nr_ok) return bad("the 5G NR kernel does not apply to this request");
+  if ((req.kernel == 2 || req.kernel == 3 || req.kernel == 5) && !nr_ok)
+    return bad("the 5G NR kernel does not apply to this request");
   const bool generic_only = req.kernel == 1 || req.kernel == 4;
   if (nr_ok && !generic_only) {
     NrCommon c{};
@@ -961,8 +962,10 @@ cudaError_t Decoder::decode(Precision p, const BatchRequest& req, cudaStream_t s
     c.hard_out = req.hard;
     c.hard_stride = req.hard_stride;
     const bool pair_ok = nr_pair_applies(c);
-    if (req.kernel == 3 && !pair_ok) return bad("the paired 5G NR kernel needs app_clamp >= 3938 (7874 with filler)");
-    if (pair_ok && req.kernel != 2) return nr_pair_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream);
+    if ((req.kernel == 3 || req.kernel == 5) && !pair_ok)
+      return bad("the paired 5G NR kernel needs app_clamp >= 3938 (7874 with filler)");
+    if (pair_ok && req.kernel != 2)
+      return nr_pair_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream, req.kernel != 5);
     return nr_decode_i8(nr_bg_, c, g_.shifts.data(), sms_, stream);
   }
   // f32 5G NR: the compressed-message kernel, when the caller's workspace holds its

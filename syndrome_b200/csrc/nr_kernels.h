@@ -128,6 +128,9 @@ cudaError_t nr_f32_decode(int bg, const NrF32Common& c, int z, const int* shifts
 int pair_mixed_capacity(int bg, int z);
 cudaError_t pair_mixed_prepare();
 cudaError_t pair_mixed_launch(const MixArgs& m, int sms, cudaStream_t stream);
-cudaError_t nr_pair_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream);
+// tmem: at Z = 384, the variant that keeps most check-row state in tensor memory (two
+// codeword pairs per SM) instead of the one that keeps it all in shared memory.
+cudaError_t nr_pair_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream,
+                              bool tmem = true);
 
 }  // namespace syn

@@ -215,23 +215,32 @@ __host__ __device__ __forceinline__ uint32_t ext_lanes(uint32_t xreg, int xi) {
 //   template <int GE> int vb() const     byte offset in the pair's posterior array
 //                                        of edge GE's variable (column, (z + shift) mod Z)
 //   uint32_t ld_ap(int) / void st_ap(int, uint32_t)
-//   uint32_t ld_st(int w) / void st_st(int w, uint32_t)   state word w of this row group
+//   template <int L, int N> void row_load(uint32_t (&w)[N])    the N = 1 + ncw(deg) state
+//   template <int L, int N> void row_store(const uint32_t (&w)[N])  words of layer L's row
+//                                        (meta word, then the code words)
+//   template <int L> void row_next()     called once per row after row_load: the context
+//                                        may start fetching the state of the row after L
+//   template <int L> uint32_t row_word(int i) const   state word i of layer L's row (cold
+//                                        paths: syndrome, outputs)
 //   uint32_t xr(int i) const             extension channel register i
 //   uint32_t selc() const, c7f() const   the constants 0xC480 and 0x7F7F7F7F (registers)
 
-// Offset beta_q in the key domain, both lanes (the pair_row argument).
+// Offset beta_q in the key domain (beta_q * 256 in both lanes; the pair_row argument).
 __host__ __device__ constexpr uint32_t pair_beta(int beta_q) { return (uint32_t)beta_q * 0x01000100u; }
 
 template <int BG, int L, bool FILL, class C>
 __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
-  constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L), NC = ncw(deg), W = state_off<BG>(L);
+  constexpr int lb = Tab<BG>::loff(L), deg = deg_of<BG>(L), NC = ncw(deg);
   constexpr int ep = L >= 4 ? ext_pos<BG>(L) : -1;
   const uint32_t selc = c.selc(), c7f = c.c7f();
-  const uint32_t meta = c.ld_st(W);
+  uint32_t rw[1 + NC];
+  c.template row_load<L, 1 + NC>(rw);
+  c.template row_next<L>();
+  const uint32_t meta = rw[0];
   uint32_t code[NC];
   static_for<0, NC>([&](auto ki) {
     constexpr int k = decltype(ki)::value;
-    code[k] = c.ld_st(W + 1 + k);
+    code[k] = rw[1 + k];
   });
   uint32_t tlo, thi;
   tables(meta, c7f, tlo, thi);
@@ -316,21 +325,48 @@ __host__ __device__ __forceinline__ void pair_row(C& c, uint32_t bq2) {
       c.st_ap(vb[e], v);
     }
   });
-  c.st_st(W, nmeta);
+  uint32_t nw[1 + NC];
+  nw[0] = nmeta;
   static_for<0, NC>([&](auto ki) {
     constexpr int k = decltype(ki)::value;
-    c.st_st(W + 1 + k, nc[k]);
+    nw[1 + k] = nc[k];
   });
+  c.template row_store<L, 1 + NC>(nw);
 }
 
 // Message lanes (127 + R) of edge e of layer L from the stored state.
 template <int BG, int L, int E, class C>
 __host__ __device__ __forceinline__ uint32_t pair_message(const C& c) {
-  constexpr int W = state_off<BG>(L);
   uint32_t lo, hi;
-  tables(c.ld_st(W), 0x7F7F7F7Fu, lo, hi);
-  return prmt(lo, hi, code_sel(c.ld_st(W + 1 + (E >> 3)), code_shift(E), 0xC480u));
+  tables(c.template row_word<L>(0), 0x7F7F7F7Fu, lo, hi);
+  return prmt(lo, hi, code_sel(c.template row_word<L>(1 + (E >> 3)), code_shift(E), 0xC480u));
 }
+
+// Row-level state access over word accessors ld_st(w) / st_st(w, v) (w = state word
+// index, state_off<BG>(L) + i for word i of layer L's row): the storage of the
+// one-pair-per-SM kernel and of the host emulation.  B is the base graph, D the
+// context deriving from this.
+template <int BG, class D>
+struct WordRows {
+  template <int L, int N>
+  __host__ __device__ __forceinline__ void row_load(uint32_t (&w)[N]) const {
+    static_for<0, N>([&](auto ii) { w[decltype(ii)::value] = self().ld_st(state_off<BG>(L) + decltype(ii)::value); });
+  }
+  template <int L, int N>
+  __host__ __device__ __forceinline__ void row_store(const uint32_t (&w)[N]) {
+    static_for<0, N>([&](auto ii) { self().st_st(state_off<BG>(L) + decltype(ii)::value, w[decltype(ii)::value]); });
+  }
+  template <int L>
+  __host__ __device__ __forceinline__ void row_next() {}
+  template <int L>
+  __host__ __device__ __forceinline__ uint32_t row_word(int i) const {
+    return self().ld_st(state_off<BG>(L) + i);
+  }
+
+ private:
+  __host__ __device__ __forceinline__ const D& self() const { return static_cast<const D&>(*this); }
+  __host__ __device__ __forceinline__ D& self() { return static_cast<D&>(*this); }
+};
 
 // Posterior lanes (PB + app) of the extension column of layer L >= 4.
 template <int BG, int L, class C>

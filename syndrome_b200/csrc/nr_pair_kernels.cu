@@ -47,7 +47,7 @@ struct PairArgs {
 // shared memory.  APC: byte offset of the posteriors in pair_smem when ZT > 0 (the
 // CTA then holds one codeword pair at a fixed place).
 template <int BG, int ZT, int APC = 16>
-struct DevCtx {
+struct DevCtx : WordRows<BG, DevCtx<BG, ZT, APC>> {
   static_assert(ZT == 0 || ZT == 384 || ZT == -1, "compile-time lifting size must be 384");
   static constexpr int NX = ext_regs<BG>();
   static constexpr int NS = ZT > 0 ? kPairThreads : 0;
@@ -125,7 +125,8 @@ static __constant__ HeadTab kHeadTab = make_head_tab();
 // Row context of head layer l (0..3) over a DevCtx<0, 384, APC>: layer 0's compile-time
 // structure with layer l's addresses and state words.
 template <class Base>
-struct HeadCtx {
+struct HeadCtx : WordRows<0, HeadCtx<Base>> {
+  __device__ HeadCtx(Base& base, int layer) : b(base), l(layer) {}
   Base& b;
   int l;
   __device__ __forceinline__ uint32_t selc() const { return b.selc(); }
@@ -165,8 +166,8 @@ __device__ __forceinline__ int lane_of(uint32_t w, int lane, uint32_t bias = kPB
 // of its context so that the hot loop's registers stay where they are).
 
 // Parity of every check row outside the quick-stage layers (bit 0 lane A odd, bit 1 lane B).
-template <int BG, int ZT, int APC>
-__device__ __noinline__ uint32_t full_parity(const DevCtx<BG, ZT, APC>* cx) {
+template <int BG, class Ctx>
+__device__ __noinline__ uint32_t full_parity(const Ctx* cx) {
   uint32_t odd = 0u;
   static_for<0, Tab<BG>::MB>([&](auto li) {
     constexpr int L = decltype(li)::value;
@@ -176,18 +177,17 @@ __device__ __noinline__ uint32_t full_parity(const DevCtx<BG, ZT, APC>* cx) {
 }
 
 // This thread's share of lane X's results: its extension posteriors / hard decisions
-// (also into the shared-memory byte array eh for the packed output) and the messages
-// of its check rows in the reference's edge_r layout.
-template <int BG, int ZT, int APC>
-__device__ __noinline__ void write_rows(const DevCtx<BG, ZT, APC>* cx, const NrCommon* c, int X, long long cw, int Z,
-                                        int z, int eh_off) {
-  unsigned char* eh = pair_smem + eh_off;
+// (also into the shared-memory byte array eh for the packed output, unless eh_off < 0)
+// and the messages of its check rows in the reference's edge_r layout.
+template <int BG, class Ctx>
+__device__ __noinline__ void write_rows(const Ctx* cx, const NrCommon* c, int X, long long cw, int Z, int z,
+                                        int eh_off) {
   using T = Tab<BG>;
   static_for<4, T::MB>([&](auto li) {
     constexpr int L = decltype(li)::value;
     const int v = lane_of(pair_ext_app<BG, L>(*cx), X);
     const int j = (T::KB + L) * Z + z;
-    eh[(L - 4) * Z + z] = v < 0 ? 1 : 0;
+    if (eh_off >= 0) pair_smem[eh_off + (L - 4) * Z + z] = v < 0 ? 1 : 0;
     if (c->app_out) c->app_out[cw * c->app_stride + j] = (int16_t)v;
     if (c->hard_out) c->hard_out[cw * c->hard_stride + j] = v < 0 ? 1 : 0;
   });
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
           const long long cw = 2 * g + X;
           if (z == 0 && c.iters) c.iters[cw] = it;
           const DevCtx<BG, ZT> copy = cx;
-          write_rows(&copy, &c, X, cw, Z, z, (int)(eh - smem));
+          write_rows<BG>(&copy, &c, X, cw, Z, z, (int)(eh - smem));
         }
         __syncthreads();
         for (int q = 0; q < P; ++q) {
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
 #pragma unroll 1
         for (int l = 0; l < 4; ++l) {
           if (lane_ok) {
-            HeadCtx<DevCtx<BG, ZT>> h{cx, l};
+            HeadCtx<DevCtx<BG, ZT>> h(cx, l);
             pair_row<BG, 0, FILL>(h, bq2);
           }
           __syncthreads();
@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_kernel(const __grid_c
       const uint32_t pass = act & ~(uint32_t)(lane_ok ? s_fail[p] : 0);
       if (pass) {
         const DevCtx<BG, ZT> copy = cx;
-        const uint32_t odd = full_parity(&copy) & pass;
+        const uint32_t odd = full_parity<BG>(&copy) & pass;
         if (odd) atomicOr(&s_fail[p], (int)odd);
       }
       __syncthreads();
@@ -411,6 +411,491 @@ cudaError_t launch_bg(const NrCommon& c, const int* shifts, bool fill, int sms, 
     return fill ? launch<BG, 384, true>(c, shifts, sms, stream) : launch<BG, 384, false>(c, shifts, sms, stream);
   return fill ? launch<BG, 0, true>(c, shifts, sms, stream) : launch<BG, 0, false>(c, shifts, sms, stream);
 }
+
+// ------------------------------------------------------- TMEM-backed variant --
+//
+// Z = 384, one codeword pair per CTA and two CTAs per SM.  The kernel above holds a
+// pair's whole check-row state (158 KB at BG1) and posteriors in shared memory, one
+// pair per SM: three warps per scheduler, all reaching the layer barriers together,
+// so the row updates between barriers are latency-bound.  Here most of each thread's
+// check-row state lives in tensor memory (TMEM, 256 KB per SM, used purely as
+// per-thread storage: tcgen05.ld / tcgen05.st of the thread's own lane), which lets
+// two CTAs of independent codeword pairs share an SM; their barriers do not line up,
+// so one CTA's row updates fill the other's waits.
+//
+// Per CTA: 256 TMEM columns (half of the SM's 512).  Lane quarter q of TMEM (lanes
+// 32q .. 32q + 31) is reachable from warps q, q + 4 and q + 8 of the CTA, so each
+// thread owns an 85-column slot: columns 85 * (warp / 4) .. + 84 of lane
+// 32 * (warp % 4) + lane (at most column 254).  The rows of the compressed state go
+// to the slot in layer order, each padded to 2 or 4 words so that one tcgen05.ld.x2 /
+// .x4 moves it; the quick-stage syndrome layers and the rows that do not fit stay in
+// shared memory, as do the extension columns' channel values (a word per two layers)
+// and the posteriors.  While a row is updated, the next TMEM row is already being
+// loaded (row_next); the wait for it comes at that row's start.  Every TMEM access is
+// warp-uniform: one CTA holds one pair, so every branch around an access (iteration
+// control, done lanes, syndrome stages) is the same for all threads of the CTA.
+namespace tm {
+
+constexpr int kCols = 256;  // TMEM columns per CTA
+constexpr int kSlot = 85;   // columns per thread: three warps share each lane quarter
+
+__host__ __device__ constexpr int pow2ceil(int x) {
+  int p = 1;
+  while (p < x) p *= 2;
+  return p;
+}
+template <int BG>
+__host__ __device__ constexpr int row_len(int L) {
+  return 1 + ncw(deg_of<BG>(L));
+}
+template <int BG>
+__host__ __device__ constexpr int row_pad(int L) {
+  return pow2ceil(row_len<BG>(L));
+}
+// Storage plan of a base graph's rows: in TMEM greedily in layer order, skipping the
+// quick-stage layers (read every iteration by the syndrome check); the TMEM column or
+// shared state word of each row.  Computed once per base graph.
+struct Plan {
+  bool in[48];
+  int col[49];
+  int smw[49];
+};
+template <int BG>
+__host__ __device__ constexpr Plan make_plan() {
+  Plan p{};
+  constexpr int MB = Tab<BG>::MB;
+  int deg[48] = {};
+  for (int l = 0; l < MB; ++l) deg[l] = deg_of<BG>(l);
+  int used = 0, w = 0;
+  for (int l = 0; l < MB; ++l) {
+    int rank = 0;  // nr::is_quick
+    for (int m = 0; m < MB; ++m)
+      if (deg[m] < deg[l] || (deg[m] == deg[l] && m < l)) ++rank;
+    const int len = 1 + ncw(deg[l]), pad = pow2ceil(len);
+    p.col[l] = used;
+    p.smw[l] = w;
+    p.in[l] = rank >= nr::kQuick && used + pad <= kSlot;
+    if (p.in[l])
+      used += pad;
+    else
+      w += len;
+  }
+  p.col[MB] = used;
+  p.smw[MB] = w;
+  return p;
+}
+template <int BG>
+struct PlanOf {
+  static constexpr Plan v = make_plan<BG>();
+};
+template <int BG>
+__host__ __device__ constexpr bool in_tm(int L) {
+  return PlanOf<BG>::v.in[L];
+}
+template <int BG>
+__host__ __device__ constexpr int tm_col(int L) {
+  return PlanOf<BG>::v.col[L];
+}
+template <int BG>
+__host__ __device__ constexpr int sm_word(int L) {
+  return PlanOf<BG>::v.smw[L];
+}
+template <int BG>
+__host__ __device__ constexpr int sm_words() {
+  return sm_word<BG>(Tab<BG>::MB);
+}
+template <int BG>
+__host__ __device__ constexpr int tm_words() {
+  return tm_col<BG>(Tab<BG>::MB);
+}
+static_assert(tm_words<0>() <= kSlot && tm_words<1>() <= kSlot, "TMEM slot overflow");
+static_assert(in_tm<0>(0) && in_tm<0>(1) && in_tm<0>(2) && in_tm<0>(3) && tm_col<0>(1) == 4 && tm_col<0>(3) == 12,
+              "BG1 head layers take TMEM columns 0-15");
+
+// Shared memory: [0, 16) s_fail, s_done, TMEM base; posteriors at kAp; then the shared
+// state words [sm_words][384]; then the extension channel words [ext_regs][384].
+constexpr int kAp = 16;
+template <int BG>
+__host__ __device__ constexpr int smem_bytes() {
+  return kAp + (Tab<BG>::KB + 4) * 384 * 4 + (sm_words<BG>() + ext_regs<BG>()) * 384 * 4;
+}
+
+// ---- tcgen05 storage primitives (sm_100a) ----
+__device__ __forceinline__ void ld2(uint32_t t, uint32_t (&v)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(v[0]), "=r"(v[1]) : "r"(t));
+}
+__device__ __forceinline__ void ld4(uint32_t t, uint32_t (&v)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "r"(t));
+}
+// Waits for this thread's TMEM loads; v passes through, so no use of the loaded
+// registers can move above the wait.
+__device__ __forceinline__ void wait_ld(uint32_t (&v)[4]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3])::"memory");
+}
+__device__ __forceinline__ uint32_t ld1_now(uint32_t t) {
+  uint32_t v;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(v) : "r"(t));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(v)::"memory");
+  return v;
+}
+__device__ __forceinline__ void st2(uint32_t t, uint32_t a, uint32_t b) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(t), "r"(a), "r"(b) : "memory");
+}
+__device__ __forceinline__ void st4(uint32_t t, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(t), "r"(a), "r"(b), "r"(c),
+               "r"(d)
+               : "memory");
+}
+__device__ __forceinline__ void st1(uint32_t t, uint32_t a) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(t), "r"(a) : "memory");
+}
+__device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Row context of the TMEM variant.  pf holds the next TMEM row while its load is in
+// flight; the cold paths (syndrome stages, outputs) run only while no load is in
+// flight, which is what lets them work on a copy of the context.
+template <int BG>
+struct TmCtx {
+  uint32_t tmb;  // TMEM address of this thread's slot: lane (32 * (warp % 4)) << 16 | column
+  int st;        // byte offset in pair_smem of this thread's first shared state word
+  int xo;        // byte offset in pair_smem of this thread's first extension channel word
+  int z4;
+  uint32_t sc, k7f;
+  uint32_t pf[4];
+
+  __device__ __forceinline__ uint32_t selc() const { return sc; }
+  __device__ __forceinline__ uint32_t c7f() const { return k7f; }
+  template <int GE>
+  __device__ __forceinline__ int vb() const {
+    // (z + shift) mod 384 in bytes: the add as a multiply-add (FMA pipe), the wrap as an
+    // unsigned min (below 384 the second candidate wraps high); the column base folds
+    // into the shared-memory instruction's immediate
+    int zl = z4;
+    asm volatile("" : "+r"(zl));
+    const unsigned r = mad_k((uint32_t)zl, 0, (uint32_t)(Tab<BG>::z384_shift(GE) * 4));
+    const unsigned rr = min(r, r - 384u * 4u);
+    return (int)rr + Tab<BG>::col(GE) * 384 * 4;
+  }
+  __device__ __forceinline__ uint32_t ld_ap(int b) const {
+    return *reinterpret_cast<const uint32_t*>(pair_smem + kAp + b);
+  }
+  __device__ __forceinline__ void st_ap(int b, uint32_t v) { *reinterpret_cast<uint32_t*>(pair_smem + kAp + b) = v; }
+  __device__ __forceinline__ uint32_t xr(int i) const {
+    return *reinterpret_cast<const uint32_t*>(pair_smem + xo + 4 * 384 * i);
+  }
+  __device__ __forceinline__ uint32_t sm_ld(int w) const {
+    return *reinterpret_cast<const uint32_t*>(pair_smem + st + 4 * 384 * w);
+  }
+  __device__ __forceinline__ void sm_st(int w, uint32_t v) {
+    *reinterpret_cast<uint32_t*>(pair_smem + st + 4 * 384 * w) = v;
+  }
+  // Issues the load of the TMEM row at column col (row_pad words) into pf.
+  template <int PAD>
+  __device__ __forceinline__ void fetch(int col) {
+    if constexpr (PAD == 4)
+      ld4(tmb + (uint32_t)col, pf);
+    else
+      ld2(tmb + (uint32_t)col, pf);
+  }
+  template <int N>
+  __device__ __forceinline__ void take(uint32_t (&w)[N]) {
+    wait_ld(pf);
+    static_for<0, N>([&](auto ii) { w[decltype(ii)::value] = pf[decltype(ii)::value]; });
+  }
+  template <int N>
+  __device__ __forceinline__ void put(int col, const uint32_t (&w)[N]) {
+    static_assert(N >= 2 && N <= 4, "row length");
+    if constexpr (N == 2)
+      st2(tmb + (uint32_t)col, w[0], w[1]);
+    else if constexpr (N == 3)
+      st4(tmb + (uint32_t)col, w[0], w[1], w[2], w[2]);  // the padding word takes a copy
+    else
+      st4(tmb + (uint32_t)col, w[0], w[1], w[2], w[3]);
+  }
+
+  template <int L, int N>
+  __device__ __forceinline__ void row_load(uint32_t (&w)[N]) {
+    if constexpr (in_tm<BG>(L)) {
+      take(w);
+    } else {
+      static_for<0, N>([&](auto ii) { w[decltype(ii)::value] = sm_ld(sm_word<BG>(L) + decltype(ii)::value); });
+    }
+  }
+  template <int L>
+  __device__ __forceinline__ void row_next() {
+    if constexpr (L + 1 < Tab<BG>::MB) {
+      if constexpr (in_tm<BG>(L + 1)) fetch<row_pad<BG>(L + 1)>(tm_col<BG>(L + 1));
+    }
+  }
+  template <int L, int N>
+  __device__ __forceinline__ void row_store(const uint32_t (&w)[N]) {
+    if constexpr (in_tm<BG>(L)) {
+      put(tm_col<BG>(L), w);
+    } else {
+      static_for<0, N>([&](auto ii) { sm_st(sm_word<BG>(L) + decltype(ii)::value, w[decltype(ii)::value]); });
+    }
+  }
+  template <int L>
+  __device__ __forceinline__ uint32_t row_word(int i) const {
+    if constexpr (in_tm<BG>(L))
+      return ld1_now(tmb + (uint32_t)(tm_col<BG>(L) + i));
+    else
+      return sm_ld(sm_word<BG>(L) + i);
+  }
+  // Starts the load of the first row of an iteration.
+  __device__ __forceinline__ void first_row() {
+    if constexpr (in_tm<BG>(0)) fetch<row_pad<BG>(0)>(tm_col<BG>(0));
+  }
+};
+
+// BG1 head layer l (0..3) over a TmCtx<0>: layer 0's compile-time structure with
+// layer l's addresses and TMEM row (columns 4l .. 4l + 3).
+struct TmHeadCtx {
+  TmCtx<0>& b;
+  int l;
+  __device__ TmHeadCtx(TmCtx<0>& base, int layer) : b(base), l(layer) {}
+  __device__ __forceinline__ uint32_t selc() const { return b.selc(); }
+  __device__ __forceinline__ uint32_t c7f() const { return b.c7f(); }
+  template <int GE>
+  __device__ __forceinline__ int vb() const {
+    const uint32_t t = kHeadTab.v[l * 19 + GE];
+    int zl = b.z4;
+    asm volatile("" : "+r"(zl));
+    const unsigned r = (unsigned)zl + (t & 0xFFFFu);
+    const unsigned rr = min(r, r - 384u * 4u);
+    return (int)rr + (int)(t >> 16);
+  }
+  __device__ __forceinline__ uint32_t ld_ap(int o) const { return b.ld_ap(o); }
+  __device__ __forceinline__ void st_ap(int o, uint32_t v) { b.st_ap(o, v); }
+  __device__ __forceinline__ uint32_t xr(int i) const { return b.xr(i); }
+  template <int L, int N>
+  __device__ __forceinline__ void row_load(uint32_t (&w)[N]) {
+    static_assert(L == 0 && N == 4, "head rows");
+    b.take(w);
+  }
+  template <int L>
+  __device__ __forceinline__ void row_next() {
+    if (l < 3)
+      b.fetch<4>(4 * (l + 1));
+    else if constexpr (in_tm<0>(4))
+      b.fetch<row_pad<0>(4)>(tm_col<0>(4));
+  }
+  template <int L, int N>
+  __device__ __forceinline__ void row_store(const uint32_t (&w)[N]) {
+    b.put(4 * l, w);
+  }
+};
+
+template <int BG, bool FILL>
+__global__ void __launch_bounds__(kPairThreads, 2) nr_pair_tm_kernel(const __grid_constant__ PairArgs<BG> a) {
+  using T = Tab<BG>;
+  constexpr int Z = 384, CORE = T::KB + 4, NEXT = T::MB - 4, NX = ext_regs<BG>(), NSW = sm_words<BG>();
+  unsigned char* smem = pair_smem;
+  const NrCommon& c = a.c;
+  int* s_fail = reinterpret_cast<int*>(smem);
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + 8);
+  const int tid = threadIdx.x, z = tid, lane = tid & 31, warp = tid >> 5;
+  const int sw_off = kAp + CORE * Z * 4, x_off = sw_off + NSW * Z * 4;
+
+  // TMEM: warp 0 allocates the CTA's columns and hands the address over shared memory.
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(s_tmem)),
+                 "r"(kCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  TmCtx<BG> cx;
+  cx.tmb = *s_tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(kSlot * (warp >> 2));
+  cx.st = sw_off + 4 * tid;
+  cx.xo = x_off + 4 * tid;
+  cx.z4 = z * 4;
+  cx.sc = 0xC480u;
+  cx.k7f = 0x7F7F7F7Fu;
+  asm volatile("" : "+r"(cx.sc), "+r"(cx.k7f));
+  const uint32_t bq2 = pair_beta(c.beta_q);
+  const int core_n = CORE * Z, K = T::KB * Z;
+  const long long npairs = (c.batch + 1) / 2;
+
+  for (long long g = blockIdx.x; g < npairs; g += gridDim.x) {
+    const bool va = 2 * g < c.batch, vbv = 2 * g + 1 < c.batch;
+    __syncthreads();
+    // ---- load: this thread's variables (col, z) of both codewords
+    {
+      const int8_t* sa = va ? c.llr + 2 * g * c.llr_stride - c.llr_offset : nullptr;
+      const int8_t* sb = vbv ? c.llr + (2 * g + 1) * c.llr_stride - c.llr_offset : nullptr;
+      auto fetch = [&](const int8_t* src, int j) -> int { return (src && j >= c.llr_offset) ? (int)src[j] : 0; };
+      uint32_t* apw = reinterpret_cast<uint32_t*>(smem + kAp);
+      for (int col = 0; col < CORE; ++col) {
+        const int j = col * Z + z;
+        uint32_t l0 = kAB + (uint32_t)fetch(sa, j), l1 = kAB + (uint32_t)fetch(sb, j);
+        if (c.prologue) {
+          if (j < 2 * Z) {
+            l0 = l1 = kAB;
+          } else if (FILL && j >= c.k_prime && j < K) {
+            l0 = l1 = kAB + kCapV;
+          }
+        }
+        apw[j] = (l0 & 0xFFFFu) | (l1 << 16);
+      }
+      uint32_t* xw = reinterpret_cast<uint32_t*>(smem + x_off);
+#pragma unroll 1
+      for (int r = 0; r < NX; ++r) {
+        uint32_t w = 0u;
+        for (int h = 0; h < 2; ++h) {
+          const int xi = 2 * r + h;
+          if (xi < NEXT) {
+            const int j = (CORE + xi) * Z + z;
+            const uint32_t b0 = (uint32_t)(fetch(sa, j) + 128) & 0xFFu, b1 = (uint32_t)(fetch(sb, j) + 128) & 0xFFu;
+            w |= (b0 | (b1 << 8)) << (16 * h);
+          }
+        }
+        xw[r * Z + tid] = w;
+      }
+      uint32_t* sw = reinterpret_cast<uint32_t*>(smem + sw_off);
+#pragma unroll 1
+      for (int w = 0; w < NSW; ++w) sw[w * Z + tid] = 0u;
+#pragma unroll 1
+      for (int col = 0; col + 4 <= kSlot; col += 4) st4(cx.tmb + (uint32_t)col, 0u, 0u, 0u, 0u);
+      st1(cx.tmb + (uint32_t)(kSlot - 1), 0u);
+      wait_st();
+      const long long gn = g + gridDim.x;  // this CTA's next codeword pair
+      const long long row_bytes = (long long)T::NB * Z - c.llr_offset;
+      if (2 * gn < c.batch) prefetch_row_l2(c.llr + 2 * gn * c.llr_stride, row_bytes, z, Z);
+      if (2 * gn + 1 < c.batch) prefetch_row_l2(c.llr + (2 * gn + 1) * c.llr_stride, row_bytes, z, Z);
+    }
+    __syncthreads();
+
+    // ---- layered iterations with per-lane early stop (as the kernel above)
+    uint32_t act = (va ? 1u : 0u) | (vbv ? 2u : 0u);
+    uint32_t done = c.iterations <= 0 ? act : 0u;
+    int it = 0;
+    for (;;) {
+#pragma unroll 1
+      for (int X = 0; X < 2; ++X) {
+        if (!((done >> X) & 1u)) continue;  // the same for the whole CTA
+        const long long cw = 2 * g + X;
+        if (z == 0 && c.iters) c.iters[cw] = it;
+        {
+          const TmCtx<BG> copy = cx;
+          write_rows<BG>(&copy, &c, X, cw, Z, z, -1);
+        }
+        const uint32_t* apq = reinterpret_cast<const uint32_t*>(smem + kAp);
+        if (c.app_out || c.hard_out) {
+          for (int j = tid; j < core_n; j += Z) {
+            int v = lane_of(apq[j], X, kAB);
+            if (FILL && j >= c.k_prime && j < K) v += c.app_clamp - kCapV;
+            if (c.app_out) c.app_out[cw * c.app_stride + j] = (int16_t)v;
+            if (c.hard_out) c.hard_out[cw * c.hard_stride + j] = v < 0 ? 1 : 0;
+          }
+        }
+        if (c.hard_packed) {
+          uint32_t* dst = c.hard_packed + cw * c.hard_words_stride;
+          const int nwords = (c.hard_bits + 31) >> 5, ncore = core_n >> 5;
+          for (int w = warp; w < min(nwords, ncore); w += Z / 32) {
+            const int j = (w << 5) + lane;
+            const bool bit = j < c.hard_bits && lane_of(apq[j], X, kAB) < 0;
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+            if (lane == 0) dst[w] = m;
+          }
+          if (nwords > ncore) {  // extension columns: word ncore + 12 (L - 4) + warp holds (L, 32 warp ..)
+            const TmCtx<BG> copy = cx;
+            static_for<4, T::MB>([&](auto li) {
+              constexpr int L = decltype(li)::value;
+              const int w = ncore + (Z / 32) * (L - 4) + warp;
+              const int j = (w << 5) + lane;
+              const bool bit = j < c.hard_bits && lane_of(pair_ext_app<BG, L>(copy), X) < 0;
+              const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+              if (lane == 0 && w < nwords) dst[w] = m;
+            });
+          }
+        }
+      }
+      act &= ~done;
+      if (!act) break;  // the same for the whole CTA
+      ++it;
+      __syncthreads();
+      cx.first_row();
+      if constexpr (BG == 0) {
+#pragma unroll 1
+        for (int l = 0; l < 4; ++l) {
+          TmHeadCtx h(cx, l);
+          pair_row<0, 0, FILL>(h, bq2);
+          __syncthreads();
+        }
+      }
+      static_for<BG == 0 ? 4 : 0, T::MB>([&](auto li) {
+        constexpr int L = decltype(li)::value;
+        pair_row<BG, L, FILL>(cx, bq2);
+        if constexpr (nr::barrier_after<BG>(L)) __syncthreads();
+      });
+      wait_st();  // this iteration's TMEM rows before the syndrome stages read them
+      // syndrome: the quick-stage layers first, the others only for lanes that pass them
+      if (z == 0) *s_fail = 0;
+      __syncthreads();
+      {
+        const uint32_t odd = quick_parity<BG>(cx) & act;
+        if (odd) atomicOr(s_fail, (int)odd);
+      }
+      __syncthreads();
+      const uint32_t pass = act & ~(uint32_t)*s_fail;
+      if (pass) {  // the same for the whole CTA
+        const TmCtx<BG> copy = cx;
+        const uint32_t odd = full_parity<BG>(&copy) & pass;
+        if (odd) atomicOr(s_fail, (int)odd);
+      }
+      __syncthreads();
+      done = it >= c.iterations ? act : act & ~(uint32_t)*s_fail;
+    }
+  }
+  // Every TMEM access of this CTA completes before warp 0 frees the columns.
+  wait_st();
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*s_tmem), "r"(kCols) : "memory");
+  }
+}
+
+template <int BG, bool FILL>
+cudaError_t launch_tm(const NrCommon& c0, int sms, cudaStream_t stream) {
+  PairArgs<BG> a;
+  a.c = c0;
+  for (int e = 0; e < Tab<BG>::E; ++e) {
+    a.sh4[e] = 0;
+    a.cz4[e] = 0;
+  }
+  a.c.cpb = 1;
+  const long long npairs = (c0.batch + 1) / 2;
+  auto fn = nr_pair_tm_kernel<BG, FILL>;
+  constexpr int smem = smem_bytes<BG>();
+  cudaError_t e = allow_max_dynamic_smem((const void*)fn);
+  if (e != cudaSuccess) return e;
+  // The whole unified L1 / shared array as shared memory, so that two CTAs (2 x 107 KB
+  // with the per-CTA reserve) fit an SM.
+  e = cudaFuncSetAttribute((const void*)fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  // The grid is sized for two CTAs per SM, the kernel's design point (80 registers x 384
+  // threads: at most two are ever resident on an SM, so their 2 x 256 TMEM columns
+  // never exceed the SM's 512 and no tcgen05.alloc waits on a CTA that is not running).
+  // The occupancy calculator reported one CTA per SM here while the launch itself runs
+  // two (ncu: register and shared-memory limits of two blocks each).
+  const long long ctas = std::min<long long>(npairs, 2LL * sms);
+  if (ctas <= 0) return cudaSuccess;
+  fn<<<(unsigned)ctas, kPairThreads, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace tm
 
 // ------------------------------------------------------------ mixed shapes --
 //
@@ -523,7 +1008,7 @@ __device__ __noinline__ void pair_mixed_item(const MixArgs& m, const MixItem& it
       if (mine) {
         if (z == 0 && m.iters) m.iters[m.cws[it.first + 2 * p + X].index] = itn;
         const Ctx copy = cx;
-        write_rows(&copy, &none, X, 0, Z, z, eh_off);
+        write_rows<BG>(&copy, &none, X, 0, Z, z, eh_off);
       }
       __syncthreads();
       for (int q = 0; q < P; ++q) {
@@ -561,7 +1046,7 @@ __device__ __noinline__ void pair_mixed_item(const MixArgs& m, const MixItem& it
     const uint32_t pass = act & ~(uint32_t)(lane_ok ? s_fail[p] : 0);
     if (pass) {
       const Ctx copy = cx;
-      const uint32_t odd = full_parity(&copy) & pass;
+      const uint32_t odd = full_parity<BG>(&copy) & pass;
       if (odd) atomicOr(&s_fail[p], (int)odd);
     }
     __syncthreads();
@@ -599,8 +1084,13 @@ bool nr_pair_applies(const NrCommon& c) {
   return c.app_clamp >= (fill ? nrp::kMinFillerClamp : nrp::kMaxReach) && c.z >= 1 && c.z <= 384;
 }
 
-cudaError_t nr_pair_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream) {
+cudaError_t nr_pair_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream,
+                              bool tmem) {
   const bool fill = c.prologue && c.k_prime < c.k;
+  if (tmem && c.z == 384) {
+    if (bg == 0) return fill ? nrp::tm::launch_tm<0, true>(c, sms, stream) : nrp::tm::launch_tm<0, false>(c, sms, stream);
+    return fill ? nrp::tm::launch_tm<1, true>(c, sms, stream) : nrp::tm::launch_tm<1, false>(c, sms, stream);
+  }
   if (bg == 0) return nrp::launch_bg<0>(c, shifts, fill, sms, stream);
   return nrp::launch_bg<1>(c, shifts, fill, sms, stream);
 }

@@ -200,13 +200,15 @@ class QcLdpcDecoder:
         return used.value
 
     # ---- batched GPU API (no reference counterpart) ----
-    KERNELS = {"auto": 0, "generic": 1, "nr": 2, "pair": 3, "generic_global": 4}
+    KERNELS = {"auto": 0, "generic": 1, "nr": 2, "pair": 3, "generic_global": 4, "pair_smem": 5}
 
     def set_kernel(self, kernel):
         """Kernel used by batch decodes: "auto", "generic" (layered, any graph; messages
         compressed in shared memory where they fit), "generic_global" (the same with its
-        messages in global memory), "nr" (5G NR specialised, one codeword per thread) or
-        "pair" (5G NR, two codewords per 32-bit word)."""
+        messages in global memory), "nr" (5G NR specialised, one codeword per thread),
+        "pair" (5G NR, two codewords per 32-bit word; at Z = 384 most check-row state in
+        tensor memory, two codeword pairs per SM) or "pair_smem" (the paired kernel with
+        all its state in shared memory, one pair per SM)."""
         _lib.check(_lib.load().syndrome_ldpc_decoder_set_kernel(self._h, self.KERNELS[kernel]))
         return self
 

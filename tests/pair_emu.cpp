@@ -16,7 +16,9 @@ using namespace syn::nrp;
 namespace {
 
 template <int BG>
-struct EmuCtx {
+struct EmuCtx : WordRows<BG, EmuCtx<BG>> {
+  EmuCtx(uint32_t* ap_, uint32_t* st_, const uint32_t* x_, int z_, int Z_, const int* sh_)
+      : ap(ap_), st(st_), x(x_), z(z_), Z(Z_), sh(sh_) {}
   uint32_t* ap;
   uint32_t* st;
   const uint32_t* x;
@@ -66,7 +68,7 @@ int run(int Z, const int* shifts, int beta_q, int app_clamp, int prologue, int n
   }
   const uint32_t bq2 = pair_beta(beta_q);
   auto ctx = [&](int z) {
-    return EmuCtx<BG>{ap.data(), st.data() + (size_t)z * NW, xr.data() + (size_t)z * NX, z, Z, shifts};
+    return EmuCtx<BG>(ap.data(), st.data() + (size_t)z * NW, xr.data() + (size_t)z * NX, z, Z, shifts);
   };
   auto snapshot = [&](int lane, int used) {
     iters_out[lane] = used;

@@ -49,7 +49,7 @@ def gpu_i8(dec, llr_i8, iters, quant, kernel="auto", **kw):
     return r
 
 
-KERNELS = ["generic", "generic_global", "nr", "pair"]
+KERNELS = ["generic", "generic_global", "nr", "pair", "pair_smem"]
 
 
 def assert_i8_equal(label, ref, r):
@@ -103,7 +103,7 @@ def test_int8_nr_punctured_filler_and_clamps(kernel):
         code = O.Code.nr(bg, z)
         dec = S.QcLdpcDecoder.with_lifting_size(bg, z, 0.5)
         info_len = code.k - n_filler
-        if kernel == "pair":  # the paired kernel needs app_clamp >= 3938 (7874 with filler bits)
+        if kernel in ("pair", "pair_smem"):  # the paired kernel needs app_clamp >= 3938 (7874 with filler bits)
             clamps = (32767, 7874 if n_filler else 3938)
         else:
             clamps = (32767, 1000, 255)
@@ -151,8 +151,9 @@ def test_int8_pair_kernel_rejects_small_clamps():
 def test_int8_pair_kernel_lanes_finish_apart(count):
     """Codewords of one pair converge at different iterations (SNR spread over the batch),
     odd batch sizes leave a lane without a codeword; BG1 Z=384 takes the compile-time-Z
-    instantiation, Z=192 the run-time one with two pairs per CTA."""
-    for z in (384, 192):
+    instantiations (state in tensor memory, and all in shared memory), Z=192 the
+    run-time one with two pairs per CTA."""
+    for z, kernel in ((384, "pair"), (384, "pair_smem"), (192, "pair")):
         code = O.Code.nr(0, z)
         dec = S.QcLdpcDecoder.with_lifting_size(0, z, 0.5)
         rows, refs = [], []
@@ -163,9 +164,9 @@ def test_int8_pair_kernel_lanes_finish_apart(count):
             rows.append(app[2 * z:].astype(np.int8))
             full = np.concatenate([np.zeros(2 * z, np.int16), app[2 * z:]])
             refs.append(code.decode_i8(code.prologue_5g_i8(full, 0), 4, 8))
-        r = gpu_i8(dec, np.stack(rows), 8, S.QuantParams(), "pair", llr_offset=2 * z, nr_prologue=True,
+        r = gpu_i8(dec, np.stack(rows), 8, S.QuantParams(), kernel, llr_offset=2 * z, nr_prologue=True,
                    hard_bits=code.k)
-        assert_i8_equal(f"pair z{z} count{count}", refs, r)
+        assert_i8_equal(f"{kernel} z{z} count{count}", refs, r)
 
 
 @pytest.mark.parametrize("kernel", ["auto", "generic_global"])

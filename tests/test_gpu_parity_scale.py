@@ -11,7 +11,8 @@ and compare every codeword with the oracle:
 * int8, 5G NR BG1 Z=384 at Eb/N0 = 1.0 dB, <= 8 iterations, the default kernel
   choice (the benchmark's workload): iteration counts and packed information bits
   of every codeword bit-identical; posteriors and messages bit-identical on a
-  subset that spans first, second and later groups of the CTAs;
+  subset that spans first, second and later groups of the CTAs; the paired kernel's
+  one-pair-per-SM variant gives the same on the same batch;
 * the same for BG2 Z=384 and for BG1 at a run-time lifting size (Z = 192, two
   codeword pairs per CTA);
 * f32, 5G NR BG1 Z=384: iteration counts and hard decisions bit-identical,
@@ -78,6 +79,14 @@ def test_int8_batch_matches_oracle_at_scale(bg, z, count, ebno):
     assert bad.size == 0, f"packed information bits differ on {bad.size} of {B} codewords, first {bad[:8]}"
     # the decode is not trivial: some codewords fail, some stop early
     assert 0 < (unpack(got, code.k) == info).all(axis=1).sum() < B or ebno > 1.0
+    if z == 384:  # the one-pair-per-SM variant of the paired kernel on the same batch
+        dec.set_kernel("pair_smem")
+        p2, i2 = torch.zeros_like(packed), torch.zeros_like(iters)
+        dec.decode_batch_i8(d_llr, 8, llr_offset=punct, nr_prologue=True, quant=quant, hard_bits=code.k,
+                            workspace=ws, out={"hard_packed": p2, "iters": i2})
+        torch.cuda.synchronize()
+        dec.set_kernel("auto")
+        assert torch.equal(i2, iters) and torch.equal(p2, packed), "pair_smem differs from the default kernel"
     # posteriors and messages on a subset spanning several groups per CTA
     r = dec.decode_batch_i8(d_llr, 8, llr_offset=punct, nr_prologue=True, quant=quant, hard_bits=code.k,
                             want_app=True, want_edge_r=True)
