@@ -348,6 +348,42 @@ int32_t syndrome_mixed_decode(SyndromeMixedPlan* plan, const int8_t* d_llr, size
                               uint32_t* d_hard_packed, size_t out_words, int32_t* d_iters, size_t iters_len,
                               int32_t use_graph, void* stream);
 
+/* One codeword of a mixed batch of 802.11 codewords (f32).  No counterpart in the
+ * reference, which decodes one codeword per call (decode_layered_offset_min_sum,
+ * src/qc_ldpc.rs:962, on the matrices of src/wifi_ldpc_tables.rs:339-453).  Its N f32
+ * channel LLRs start llr_offset elements into the batch's LLR buffer; its hard
+ * decisions of variables 0..hard_bits-1 are written LSB-first from word out_offset. */
+typedef struct {
+  int32_t z;         /* 27, 54 or 81 (n = 648, 1296, 1944) */
+  int32_t rate_num;  /* rate 1/2, 2/3, 3/4 or 5/6 */
+  int32_t rate_den;
+  int32_t hard_bits; /* leading variables reported, e.g. the K information bits */
+  int64_t llr_offset;
+  int64_t out_offset;
+} SyndromeWifiMixedCodeword;
+
+typedef struct SyndromeWifiMixedPlan SyndromeWifiMixedPlan;
+
+/* Plans a batch of codewords of any mix of the twelve 802.11 matrices for one
+ * persistent f32 launch: codewords grouped by matrix into chunks of `chunk` codewords
+ * (0: four CTAs' worth of codeword slots) on a device queue, the costliest matrices
+ * first; every codeword slot of a CTA takes the next codeword as soon as its own
+ * stops (zero syndrome or `iterations`), so skewed iteration counts keep the slots
+ * busy.  f32 layered offset min-sum with offset_beta. */
+int32_t syndrome_wifi_mixed_plan_create(const SyndromeWifiMixedCodeword* codewords, size_t count, float offset_beta,
+                                        size_t iterations, size_t chunk, SyndromeWifiMixedPlan** out_plan);
+void syndrome_wifi_mixed_plan_destroy(SyndromeWifiMixedPlan* plan);
+/* Chunks on the plan's queue and CTAs of its launch (ctas nullable). */
+int32_t syndrome_wifi_mixed_plan_chunks(const SyndromeWifiMixedPlan* plan, size_t* n_chunks, size_t* ctas);
+/* Decodes the planned batch from device LLRs (llr_len floats) into d_hard_packed
+ * (out_words long); d_iters (nullable, iters_len entries) receives the iterations of
+ * codeword i at index i.  Buffers shorter than the plan's offsets need give
+ * SYNDROME_BUFFER_TOO_SMALL.  use_graph != 0 captures the launch into a CUDA graph on
+ * first use (per buffer set) and replays it afterwards. */
+int32_t syndrome_wifi_mixed_decode(SyndromeWifiMixedPlan* plan, const float* d_llr, size_t llr_len,
+                                   uint32_t* d_hard_packed, size_t out_words, int32_t* d_iters, size_t iters_len,
+                                   int32_t use_graph, void* stream);
+
 /* ===================================== 4. transport blocks (DL-SCH) ===== */
 
 /* src/segmentation.rs:265 compute_segmentation.  out10 = {base graph (0 = BG1),

@@ -26,6 +26,7 @@ from .qc_ldpc import (  # noqa: F401
 )
 
 from .mixed import CODEWORD_DTYPE, LIFTING_SIZES, MixedBatch, code_dims, tile_capacity  # noqa: F401,E402
+from .mixed import WIFI_CODEWORD_DTYPE, WIFI_SHAPES, WifiMixedBatch, wifi_dims  # noqa: F401,E402
 
 __version__ = "0.1.0"
 from .dlsch import DecodeReport, DlSchDecoder, DlSchEncoder, SegmentationParams, compute_segmentation, crc24  # noqa: F401,E402

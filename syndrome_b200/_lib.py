@@ -68,6 +68,10 @@ PROTOTYPES = {
     "syndrome_mixed_plan_items": (_i32, [_vp, _vp, _sz, ctypes.POINTER(_sz)]),
     "syndrome_mixed_tile_capacity": (_i32, [_i32, _i32]),
     "syndrome_mixed_decode": (_i32, [_vp, _vp, _sz, _vp, _sz, _vp, _sz, _i32, _vp]),
+    "syndrome_wifi_mixed_plan_create": (_i32, [_vp, _sz, _f32, _sz, _sz, ctypes.POINTER(_vp)]),
+    "syndrome_wifi_mixed_plan_destroy": (None, [_vp]),
+    "syndrome_wifi_mixed_plan_chunks": (_i32, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
+    "syndrome_wifi_mixed_decode": (_i32, [_vp, _vp, _sz, _vp, _sz, _vp, _sz, _i32, _vp]),
     "syndrome_tb_segmentation": (_i32, [_sz, _f32, _vp]),
     "syndrome_crc24": (ctypes.c_uint32, [_vp, _sz, _i32]),
     "syndrome_dlsch_encoder_create": (_i32, [_sz, _f32, _sz, _sz, ctypes.POINTER(_vp)]),

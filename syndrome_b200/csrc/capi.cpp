@@ -22,6 +22,7 @@
 #include "frames.h"
 #include "graph.h"
 #include "mixed.h"
+#include "wifi_mixed.h"
 #include "serve.h"
 #include "tb.h"
 
@@ -43,6 +44,10 @@ struct SyndromeLdpcEncoder {
 
 struct SyndromeMixedPlan {
   syn::MixedPlan plan;
+};
+
+struct SyndromeWifiMixedPlan {
+  syn::WifiMixedPlan plan;
 };
 
 struct SyndromeServer {
@@ -771,6 +776,60 @@ int32_t syndrome_mixed_decode(SyndromeMixedPlan* plan, const int8_t* d_llr, size
   return guard([&]() -> int32_t {
     if (!plan || !d_llr || !d_hard_packed) return SYNDROME_NULL_POINTER;
     if ((long long)llr_bytes < plan->plan.llr_bytes_needed())
+      return fail(SYNDROME_BUFFER_TOO_SMALL, "LLR buffer shorter than the planned offsets");
+    if ((long long)out_words < plan->plan.out_words_needed())
+      return fail(SYNDROME_BUFFER_TOO_SMALL, "output buffer shorter than the planned offsets");
+    if (d_iters && iters_len < (size_t)plan->plan.codewords())
+      return fail(SYNDROME_BUFFER_TOO_SMALL, "iteration buffer shorter than the codeword count");
+    return from_cuda(plan->plan.decode(d_llr, d_hard_packed, d_iters, use_graph != 0,
+                                       static_cast<cudaStream_t>(stream)),
+                     "");
+  });
+}
+
+int32_t syndrome_wifi_mixed_plan_create(const SyndromeWifiMixedCodeword* codewords, size_t count, float offset_beta,
+                                        size_t iterations, size_t chunk, SyndromeWifiMixedPlan** out_plan) {
+  return guard([&]() -> int32_t {
+    if (!out_plan || (!codewords && count)) return SYNDROME_NULL_POINTER;
+    *out_plan = nullptr;
+    if (iterations > (size_t)INT_MAX || chunk > (size_t)INT_MAX || count > (size_t)INT_MAX / 2)
+      return fail(SYNDROME_INVALID_PARAM, "size out of range");
+    std::vector<syn::WifiMixedCodeword> cws(count);
+    for (size_t i = 0; i < count; ++i) {
+      const SyndromeWifiMixedCodeword& c = codewords[i];
+      cws[i] = syn::WifiMixedCodeword{c.z, c.rate_num, c.rate_den, c.hard_bits, (long long)c.llr_offset,
+                                      (long long)c.out_offset};
+    }
+    auto* p = new SyndromeWifiMixedPlan();
+    std::string err;
+    if (!p->plan.init(cws, offset_beta, (int)iterations, (int)chunk, &err)) {
+      delete p;
+      cudaGetLastError();
+      return fail(err.find("CUDA") != std::string::npos || err.find("cuda") != std::string::npos
+                      ? SYNDROME_CUDA_ERROR
+                      : SYNDROME_INVALID_PARAM,
+                  err);
+    }
+    *out_plan = p;
+    return SYNDROME_OK;
+  });
+}
+
+void syndrome_wifi_mixed_plan_destroy(SyndromeWifiMixedPlan* plan) { delete plan; }
+
+int32_t syndrome_wifi_mixed_plan_chunks(const SyndromeWifiMixedPlan* plan, size_t* n_chunks, size_t* ctas) {
+  if (!plan || !n_chunks) return SYNDROME_NULL_POINTER;
+  *n_chunks = (size_t)plan->plan.chunks();
+  if (ctas) *ctas = (size_t)plan->plan.ctas();
+  return SYNDROME_OK;
+}
+
+int32_t syndrome_wifi_mixed_decode(SyndromeWifiMixedPlan* plan, const float* d_llr, size_t llr_len,
+                                   uint32_t* d_hard_packed, size_t out_words, int32_t* d_iters, size_t iters_len,
+                                   int32_t use_graph, void* stream) {
+  return guard([&]() -> int32_t {
+    if (!plan || !d_llr || !d_hard_packed) return SYNDROME_NULL_POINTER;
+    if ((long long)llr_len < plan->plan.llr_needed())
       return fail(SYNDROME_BUFFER_TOO_SMALL, "LLR buffer shorter than the planned offsets");
     if ((long long)out_words < plan->plan.out_words_needed())
       return fail(SYNDROME_BUFFER_TOO_SMALL, "output buffer shorter than the planned offsets");

@@ -32,6 +32,7 @@
 #include "decoder.h"
 #include "smem_limit.h"
 #include "nr_kernels.h"
+#include "wifi_mixed.h"
 
 namespace syn {
 
@@ -74,7 +75,7 @@ struct KArgs {
   int st_off;             // byte offset of the state words in shared memory
 };
 
-__host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
+__host__ __device__ constexpr int align16(int x) { return (x + 15) & ~15; }
 
 __host__ __device__ inline int table_bytes(int n_edges, int mb, int cpb) {
   return align16(n_edges * 4) + align16((mb + 1) * 4) + align16(cpb * 4);
@@ -802,6 +803,198 @@ KernelFn kernel_for(Precision p, int tmpl, bool compressed = false) {
   return nullptr;
 }
 
+// ------------------------------------------- 802.11 mixed batches (f32) --
+//
+// One persistent launch over codewords of all twelve 802.11 matrices
+// (wifi_mixed.h).  A CTA takes a chunk (a run of codewords of one matrix) from the
+// device queue and runs a session of that matrix: the matrix's tables go to shared
+// memory, and each of its floor(384 / Z) codeword slots (Z threads each) decodes one
+// codeword at a time with the compressed-message row update of loms_f32c_kernel.  All
+// slots take the layers together (a barrier per layer), each on its own iteration:
+// after every iteration a slot whose codeword reached a zero syndrome or the iteration
+// limit writes its results and takes the next codeword of the chunk, and when the chunk
+// runs out the CTA takes the next chunk from the queue.  If that chunk is of another
+// matrix, the slots drain and the session ends; the CTA then starts a session of the
+// new matrix.  Codewords that converge in one iteration and codewords that run all of
+// them thus keep every slot busy (the batch's iteration counts are heavily skewed).
+
+extern __shared__ __align__(16) unsigned char wm_smem[];
+
+// The row update of layer_f32c with nothing per edge kept between its two passes:
+// the second pass reads each posterior again (still the old value: a row touches each
+// of its variables once, and only the second pass writes them) and rebuilds the old
+// message from the stored bits, so the subtraction, the sign and the minimum test see
+// exactly the values of the first pass.  Row minima by the reference's sequential
+// rule (qc_ldpc.rs:1100-1113).  Same results as layer_f32c in a fraction of its
+// registers, for a kernel that runs every matrix under one register budget.
+__device__ __forceinline__ void layer_f32c_lean(const uint32_t* __restrict__ s_edge, int lb, int deg, int Z, int zi,
+                                                float* __restrict__ A, uint32_t* __restrict__ st, int ns, int mw,
+                                                int cwo, float beta) {
+  const float magA = __uint_as_float(st[mw * ns]), magB = __uint_as_float(st[(mw + 1) * ns]);
+  const uint32_t lo = st[cwo * ns];
+  const uint32_t hi = deg > 16 ? st[(cwo + 1) * ns] : 0u;
+  const unsigned long long bits = ((unsigned long long)hi << 32) | lo;
+  float m1 = FLT_MAX, m2 = FLT_MAX;
+  unsigned sx = 0;
+#pragma unroll 4
+  for (int e = 0; e < deg; ++e) {
+    const float av = A[var_index(s_edge[lb + e], zi, Z)];
+    const float ro = f32c_message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u);
+    const unsigned b = __float_as_uint(__fsub_rn(av, ro));
+    const float aq = __uint_as_float(b & 0x7FFFFFFFu);
+    sx ^= b & 0x80000000u;
+    if (aq <= m1) {
+      m2 = m1;
+      m1 = aq;
+    } else if (aq < m2) {
+      m2 = aq;
+    }
+  }
+  if (m1 == FLT_MAX) m1 = 0.0f;
+  if (m2 == FLT_MAX) m2 = m1;
+  float nA = __fsub_rn(m1, beta), nB = __fsub_rn(m2, beta);
+  if (nA < 0.0f) nA = 0.0f;
+  if (nB < 0.0f) nB = 0.0f;
+  unsigned long long nbits = 0ull;
+#pragma unroll 4
+  for (int e = 0; e < deg; ++e) {
+    const int v = var_index(s_edge[lb + e], zi, Z);
+    const float av = A[v];
+    const float ro = f32c_message(magA, magB, (unsigned)(bits >> (2 * e)) & 3u);
+    const unsigned b = __float_as_uint(__fsub_rn(av, ro));
+    const float aq = __uint_as_float(b & 0x7FFFFFFFu);
+    const unsigned sgn = sx ^ (b & 0x80000000u);
+    const bool is_min = aq == m1;
+    const float nr = __uint_as_float(__float_as_uint(is_min ? nB : nA) | sgn);
+    A[v] = __fadd_rn(av, __fsub_rn(nr, ro));
+    nbits |= (unsigned long long)((is_min ? 1u : 0u) | (sgn >> 30)) << (2 * e);
+  }
+  st[mw * ns] = __float_as_uint(nA);
+  st[(mw + 1) * ns] = __float_as_uint(nB);
+  st[cwo * ns] = (uint32_t)nbits;
+  if (deg > 16) st[(cwo + 1) * ns] = (uint32_t)(nbits >> 32);
+}
+
+struct WmHdr {
+  int chunk, pending, cur, end, shape, pad[3];
+  int slot_cw[kWmMaxSlots], slot_used[kWmMaxSlots], slot_fail[kWmMaxSlots], slot_new[kWmMaxSlots];
+};
+constexpr int kWmHdr = (int)((sizeof(WmHdr) + 15) / 16 * 16);
+constexpr int kWmTab = kWmMaxEdges * 4 + align16((kWmMaxLayers + 1) * 4);
+
+__device__ __forceinline__ void wm_session(const WmArgs& a, const WmShape& sh) {
+  WmHdr* h = reinterpret_cast<WmHdr*>(wm_smem);
+  uint32_t* s_edge = reinterpret_cast<uint32_t*>(wm_smem + kWmHdr);
+  int32_t* s_loff = reinterpret_cast<int32_t*>(wm_smem + kWmHdr + kWmMaxEdges * 4);
+  float* app = reinterpret_cast<float*>(wm_smem + kWmHdr + kWmTab);
+  const int Z = sh.z, N = sh.n, cpb = sh.cpb, ns = (int)blockDim.x, tid = (int)threadIdx.x;
+  uint32_t* st = reinterpret_cast<uint32_t*>(wm_smem + kWmHdr + kWmTab + align16(cpb * N * 4)) + tid;
+  const int slot = tid / Z, zi = tid - slot * Z;
+  const bool lane_ok = slot < cpb;
+  for (int i = tid; i < sh.n_edges; i += ns) s_edge[i] = a.edges[sh.edge_off + i];
+  for (int i = tid; i <= sh.mb; i += ns) s_loff[i] = a.loffs[sh.loff_off + i];
+  if (tid < kWmMaxSlots) {
+    h->slot_cw[tid] = -1;
+    h->slot_used[tid] = 0;
+    h->slot_fail[tid] = 0;
+    h->slot_new[tid] = 0;
+  }
+  if (tid == 0) {
+    const WmChunk ch = a.chunks[h->chunk];
+    h->cur = ch.first;
+    h->end = ch.first + ch.count;
+    h->shape = ch.shape;
+    h->pending = -1;
+  }
+  __syncthreads();
+  for (;;) {
+    // every idle slot takes the next codeword of this matrix (thread 0 hands them out)
+    if (tid == 0) {
+      for (int s = 0; s < cpb; ++s) {
+        if (h->slot_cw[s] >= 0) continue;
+        while (h->cur >= h->end && h->pending < 0) {
+          const int nc = (int)atomicAdd(a.queue, 1u);
+          if (nc < a.n_chunks && a.chunks[nc].shape == h->shape) {
+            h->cur = a.chunks[nc].first;
+            h->end = h->cur + a.chunks[nc].count;
+          } else {
+            h->pending = nc;  // another matrix, or the end of the queue: after this session
+          }
+        }
+        if (h->cur >= h->end) break;
+        h->slot_cw[s] = h->cur++;
+        h->slot_used[s] = 0;
+        h->slot_new[s] = 1;
+      }
+    }
+    __syncthreads();
+    const int my = lane_ok ? h->slot_cw[slot] : -1;
+    if (my >= 0 && h->slot_new[slot]) {  // a new codeword: channel LLRs in, messages R = +0
+      const float* src = a.llr + a.cws[my].llr_off;
+      float* A = app + slot * N;
+      for (int j = zi; j < N; j += Z) A[j] = src[j];
+      for (int w = 0; w < sh.st_words; ++w) st[w * ns] = 0u;
+    }
+    int n_act = 0;
+    for (int s = 0; s < cpb; ++s) n_act += h->slot_cw[s] >= 0 ? 1 : 0;
+    __syncthreads();
+    if (tid < cpb) h->slot_new[tid] = 0;
+    if (n_act == 0) break;  // the same for the whole CTA: the chunk is drained
+    const bool active = my >= 0;
+    float* A = app + (lane_ok ? slot : 0) * N;
+    if (a.iterations > 0) {
+      int cwo = 2 * sh.mb;
+      for (int l = 0; l < sh.mb; ++l) {
+        const int lb = s_loff[l], deg = s_loff[l + 1] - lb;
+        if (active) layer_f32c_lean(s_edge, lb, deg, Z, zi, A, st, ns, 2 * l, cwo, a.beta);
+        cwo += max(1, (deg + 15) >> 4);
+        __syncthreads();
+      }
+      if (lane_ok && zi == 0) h->slot_fail[slot] = 0;
+      __syncthreads();
+      if (active && syndrome_fails(s_edge, s_loff, sh.mb, Z, zi, A)) h->slot_fail[slot] = 1;
+      __syncthreads();
+      if (tid < cpb && h->slot_cw[tid] >= 0) ++h->slot_used[tid];
+      __syncthreads();
+    }
+    // results of the codewords that stop here: zero syndrome, or the iteration limit
+    const bool fin = active && (a.iterations == 0 || h->slot_fail[slot] == 0 || h->slot_used[slot] >= a.iterations);
+    if (fin) {
+      const WmCodeword rec = a.cws[my];
+      if (zi == 0 && a.iters) a.iters[rec.index] = h->slot_used[slot];
+      const int nwords = (rec.hard_bits + 31) >> 5;
+      for (int w = zi; w < nwords; w += Z) {
+        uint32_t m = 0u;
+        for (int b = 0; b < 32; ++b) {
+          const int j = 32 * w + b;
+          if (j < rec.hard_bits && A[j] < 0.0f) m |= 1u << b;
+        }
+        a.out[rec.out_off + w] = m;
+      }
+    }
+    __syncthreads();
+    if (fin && zi == 0) h->slot_cw[slot] = -1;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kWmThreads, 2) wifi_mixed_f32_kernel(const __grid_constant__ WmArgs a) {
+  WmHdr* h = reinterpret_cast<WmHdr*>(wm_smem);
+  if (threadIdx.x == 0) h->pending = -1;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int c = h->pending;  // the chunk that ended the previous session, if any
+      if (c < 0) c = (int)atomicAdd(a.queue, 1u);
+      h->chunk = c;
+    }
+    __syncthreads();
+    const int c = h->chunk;
+    if (c >= a.n_chunks) break;
+    wm_session(a, a.shapes[a.chunks[c].shape]);
+  }
+}
+
 }  // namespace
 
 Decoder::~Decoder() {
@@ -1151,6 +1344,28 @@ cudaError_t Decoder::decode_i8_noalloc(const BatchRequest& req, cudaStream_t str
   a.hard_stride = req.hard_stride;
   KernelFn fn = kernel_for(Precision::kInt8, geo.maxdeg_tmpl);
   fn<<<(unsigned)ctas, geo.threads, geo.smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+int wifi_mixed_smem_bytes(const WmShape& s) {
+  return kWmHdr + kWmTab + align16(s.cpb * s.n * 4) + s.st_words * kWmThreads * 4;
+}
+
+cudaError_t wifi_mixed_prepare(int smem, int* ctas_per_sm) {
+  cudaError_t e = allow_max_dynamic_smem((const void*)wifi_mixed_f32_kernel);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wifi_mixed_f32_kernel, kWmThreads, smem);
+  if (e != cudaSuccess) return e;
+  *ctas_per_sm = std::max(per_sm, 1);
+  return cudaSuccess;
+}
+
+cudaError_t wifi_mixed_launch(const WmArgs& a, int ctas, int smem, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(unsigned), stream);
+  if (e != cudaSuccess) return e;
+  if (a.n_chunks <= 0) return cudaSuccess;
+  wifi_mixed_f32_kernel<<<std::max(1, std::min(ctas, a.n_chunks)), kWmThreads, smem, stream>>>(a);
   return cudaGetLastError();
 }
 

@@ -86,3 +86,69 @@ class MixedBatch:
             self._h, llr.data_ptr(), llr.numel(), out.data_ptr(), out.numel(),
             iters.data_ptr() if iters is not None else None, iters.numel() if iters is not None else 0,
             int(bool(use_graph)), ctypes.c_void_p(sp)))
+
+
+WIFI_CODEWORD_DTYPE = np.dtype([("z", "<i4"), ("rate_num", "<i4"), ("rate_den", "<i4"), ("hard_bits", "<i4"),
+                                ("llr_offset", "<i8"), ("out_offset", "<i8")])
+
+WIFI_SHAPES = tuple((z, rn, rd) for z in (27, 54, 81) for rn, rd in ((1, 2), (2, 3), (3, 4), (5, 6)))
+
+
+def wifi_dims(z, rate_num, rate_den):
+    """(N, K) of the 802.11 matrix at lifting size z (24 block columns) and rate."""
+    n = 24 * z
+    return n, n * rate_num // rate_den
+
+
+class WifiMixedBatch:
+    """A planned batch of 802.11 codewords of any mix of the twelve matrices, decoded
+    by one persistent f32 launch.  `codewords` is a structured array of
+    WIFI_CODEWORD_DTYPE: per codeword its lifting size, rate, number of leading hard
+    decisions to report, element offset of its N f32 channel LLRs in the LLR buffer
+    and word offset of its packed hard decisions.  No counterpart in the reference,
+    which decodes one codeword per call (decode_layered_offset_min_sum,
+    src/qc_ldpc.rs:962)."""
+
+    def __init__(self, codewords, offset_beta=0.5, iterations=20, chunk=0):
+        cw = np.ascontiguousarray(np.asarray(codewords, dtype=WIFI_CODEWORD_DTYPE))
+        self.codewords = cw
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().syndrome_wifi_mixed_plan_create(cw.ctypes.data, len(cw), offset_beta, iterations,
+                                                               chunk, ctypes.byref(h)))
+        self._h = h.value
+        self.iterations = iterations
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            try:
+                _lib.load().syndrome_wifi_mixed_plan_destroy(h)
+            except Exception:
+                pass
+
+    def chunks(self):
+        """(chunks on the device queue, CTAs of the launch)."""
+        n, c = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        _lib.check(_lib.load().syndrome_wifi_mixed_plan_chunks(self._h, ctypes.byref(n), ctypes.byref(c)))
+        return n.value, c.value
+
+    def decode(self, llr, out, iters=None, use_graph=False, stream=None):
+        """llr: float32 CUDA tensor holding every codeword's LLRs at its offset; out:
+        int32 CUDA tensor of packed hard-decision words; iters: optional int32 CUDA
+        tensor with one entry per codeword."""
+        import torch
+
+        for t, name in ((llr, "llr"), (out, "out")):
+            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.is_contiguous()):
+                raise TypeError(f"{name} must be a contiguous CUDA tensor")
+        if llr.dtype != torch.float32 or out.dtype != torch.int32:
+            raise TypeError("llr must be float32 and out int32")
+        if iters is not None and not (iters.is_cuda and iters.dtype == torch.int32 and iters.is_contiguous()):
+            raise TypeError("iters must be a contiguous int32 CUDA tensor")
+        if stream is None:
+            stream = torch.cuda.current_stream(llr.device)
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        _lib.check(_lib.load().syndrome_wifi_mixed_decode(
+            self._h, llr.data_ptr(), llr.numel(), out.data_ptr(), out.numel(),
+            iters.data_ptr() if iters is not None else None, iters.numel() if iters is not None else 0,
+            int(bool(use_graph)), ctypes.c_void_p(sp)))

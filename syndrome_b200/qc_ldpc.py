@@ -168,15 +168,17 @@ class QcLdpcDecoder:
         return used.value
 
     def decode_with_workspace(self, llr, workspace, iterations):
-        it = self.decode_layered_offset_min_sum(llr, workspace.edge_r, workspace.layer_scratch,
-                                                workspace.hard, iterations)
-        workspace.codeword_llr[:] = llr
-        return it
+        """src/qc_ldpc.rs:1851-1862: the posterior stays in the caller's llr, the hard
+        decisions land in workspace.hard_output(); workspace.codeword_llr is left
+        untouched (it is the staging buffer of reconstruction-style decodes,
+        :1951-1954).  A workspace built for a different code fails the decode's size
+        checks (BUFFER_TOO_SMALL or INVALID_PARAM), as in :2765-2783."""
+        return self.decode_layered_offset_min_sum(llr, workspace.edge_r, workspace.layer_scratch, workspace.hard,
+                                                  iterations)
 
     def decode_5g_with_workspace(self, llr, n_filler, workspace, iterations):
-        it = self.decode_5g(llr, n_filler, workspace.edge_r, workspace.layer_scratch, workspace.hard, iterations)
-        workspace.codeword_llr[:] = llr
-        return it
+        """src/qc_ldpc.rs:1887-1903 (decode_5g over the workspace's buffers)."""
+        return self.decode_5g(llr, n_filler, workspace.edge_r, workspace.layer_scratch, workspace.hard, iterations)
 
     # ---- int8 decode (src/qc_ldpc.rs:1345-1524) ----
     def decode_layered_offset_min_sum_i8(self, app, edge_r, layer_scratch, hard_output, iterations,

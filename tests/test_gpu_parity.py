@@ -399,3 +399,43 @@ def test_f32_nr_compressed_kernel_matches_oracle_and_generic(bg, z, count):
             a, b = getattr(fast, name).cpu().numpy(), getattr(slow, name).cpu().numpy()
             assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), name
     dec.set_kernel("auto")
+
+
+def test_workspace_decode_matches_raw_buffer_decode():
+    """src/qc_ldpc.rs:2785-2816: the workspace path and the raw-buffer path are the same
+    decode (BG2 Z=3, weak structured LLRs, 8 iterations); the workspace's posterior
+    staging buffer stays untouched by a plain decode (:1951-1954)."""
+    for bg, z, five_g in ((1, 3, False), (0, 24, True)):
+        dec = S.QcLdpcDecoder.with_lifting_size(bg, z, 0.25)
+        n = dec.variable_node_count()
+        llr_in = np.where(np.arange(n) % 7 == 0, -0.5, 1.5).astype(np.float32)
+        llr_raw = llr_in.copy()
+        edge_r = np.zeros(dec.required_edge_buffer(), np.float32)
+        scratch = np.zeros(dec.required_layer_buffer(), np.float32)
+        hard_raw = np.zeros(n, np.uint8)
+        llr_ws = llr_in.copy()
+        ws = dec.workspace()
+        if five_g:
+            it_raw = dec.decode_5g(llr_raw, 5, edge_r, scratch, hard_raw, 8)
+            it_ws = dec.decode_5g_with_workspace(llr_ws, 5, ws, 8)
+        else:
+            it_raw = dec.decode_layered_offset_min_sum(llr_raw, edge_r, scratch, hard_raw, 8)
+            it_ws = dec.decode_with_workspace(llr_ws, ws, 8)
+        assert it_raw == it_ws
+        assert np.array_equal(hard_raw, ws.hard_output())
+        assert np.array_equal(llr_raw.view(np.uint32), llr_ws.view(np.uint32))
+        assert not ws.posterior_llr().any(), "a plain decode wrote the workspace's staging buffer"
+
+
+def test_workspace_from_wrong_decoder_is_rejected():
+    """src/qc_ldpc.rs:2765-2783: a workspace sized for another code is rejected by the
+    decode's size checks instead of being silently misused."""
+    small = S.QcLdpcDecoder.with_lifting_size(1, 2, 0.25)
+    large = S.QcLdpcDecoder.with_lifting_size(0, 2, 0.25)
+    ws_small = small.workspace()
+    llr = np.full(large.variable_node_count(), 5.0, np.float32)
+    with pytest.raises(S.FecError) as e:
+        large.decode_with_workspace(llr, ws_small, 5)
+    assert e.value.status in (_lib.BUFFER_TOO_SMALL, _lib.INVALID_PARAM)
+    with pytest.raises(S.FecError):
+        large.decode_5g_with_workspace(llr, 0, ws_small, 5)
