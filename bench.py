@@ -69,6 +69,8 @@ def parse_args():
                    help="waiting code blocks that allow more steps in flight (0: the engine's default)")
     p.add_argument("--serve-loads", type=float, nargs="+", default=[0.1, 0.25, 0.5, 0.75],
                    help="offered loads as fractions of the measured serving capacity")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the other workloads (Wi-Fi single shape, mixed 5G NR, mixed Wi-Fi)")
     return p.parse_args()
 
 
@@ -412,6 +414,83 @@ def serve_section(batch_gbps, dev, args):
             "steps": st["steps"], "mean_code_blocks_per_step": st["code_blocks"] / max(st["steps"], 1)}
 
 
+def time_decodes(fn, reps, stream):
+    """Average ms of `reps` calls of fn() between CUDA events on `stream`, after two
+    warm-up calls."""
+    import torch
+
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def configs_section(dev):
+    """The benchmark's other workloads, each device-resident, information Gbit/s:
+    802.11 Z=27 R=1/2 (1024 codewords, f32, <= 10 iterations, 1.5 dB), mixed 5G NR code
+    blocks (65536, rate-matched, int8, <= 8 iterations, one persistent launch from a CUDA
+    graph) and mixed 802.11 codewords (32768 over all twelve matrices, f32, <= 20
+    iterations, one persistent launch from a CUDA graph)."""
+    import torch
+
+    import syndrome_b200 as S
+    from syndrome_b200 import workloads as W
+
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    # 802.11 n = 648, R = 1/2
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(11)
+    enc, dec = S.wifi_ldpc_encoder(27, 1, 2), S.wifi_ldpc_decoder(27, 1, 2, 0.5)
+    n, k = 648, 324
+    info = torch.randint(0, 2, (1024, k), generator=gen, device=dev, dtype=torch.uint8)
+    llr = W.awgn_llr(enc.encode_batch_device(info), k / n, 1.5, gen).contiguous()
+    ms = time_decodes(lambda: dec.decode_batch_f32(llr, 10, hard_bits=k), 20, stream)
+    r = dec.decode_batch_f32(llr, 10, hard_bits=k)
+    torch.cuda.synchronize()
+    got = np.unpackbits(r.hard_packed.cpu().numpy().view(np.uint8), axis=1, bitorder="little")[:, :k]
+    out["wifi_648_r12"] = {
+        "workload": "802.11 n=648 Z=27 R=1/2, 1024 codewords, every bit sent, BPSK/AWGN 1.5 dB, f32 LOMS beta 0.5, "
+                    "<= 10 iterations with early stop, one batched launch (decode_batch_f32)",
+        "gbps": 1024 * k / (ms * 1e-3) / 1e9, "ms_per_launch": ms, "mean_iterations": float(r.iters.float().mean()),
+        "frames_correct": int((got == info.cpu().numpy()).all(axis=1).sum()), "codewords": 1024}
+    # mixed 5G NR, rate-matched
+    recs, llr8, words, bits = W.nr_rate_matched(65536, 33, device=dev)
+    batch = S.MixedBatch(recs, 0.5, S.QuantParams(), ITERS)
+    o = torch.zeros(max(words, 1), dtype=torch.int32, device=dev)
+    it = torch.zeros(len(recs), dtype=torch.int32, device=dev)
+    ms = time_decodes(lambda: batch.decode(llr8, o, it, use_graph=True), 5, stream)
+    out["nr_mixed_rate_matched"] = {
+        "workload": "65536 5G NR code blocks: BG1 with Z in {64,128,256,384} or BG2 with Z any lifting size <= 384 "
+                    "(1/2 each), filler uniform in [0, K/5], target rate uniform in [1/5, 8/9] by RV0 bit selection "
+                    "(puncturing or repetition), Eb/N0 uniform in [0, 3] dB, int8 at scale 8, <= 8 iterations; one "
+                    "persistent launch replayed from a CUDA graph (MixedBatch)",
+        "gbps": bits / (ms * 1e-3) / 1e9, "ms_per_launch": ms, "mean_iterations": float(it.float().mean()),
+        "codewords": len(recs), "work_items": len(batch.items()), "info_bits": bits}
+    del llr8, o, it, batch
+    # mixed 802.11
+    recs, llrf, words, bits = W.wifi_mixed(32768, 44, device=dev)
+    wb = S.WifiMixedBatch(recs, 0.5, 20)
+    o = torch.zeros(max(words, 1), dtype=torch.int32, device=dev)
+    it = torch.zeros(len(recs), dtype=torch.int32, device=dev)
+    ms = time_decodes(lambda: wb.decode(llrf, o, it, use_graph=True), 5, stream)
+    n_chunks, ctas = wb.chunks()
+    out["wifi_mixed"] = {
+        "workload": "32768 802.11 codewords uniform over the twelve matrices (n 648/1296/1944 x R 1/2, 2/3, 3/4, 5/6), "
+                    "every bit sent, Eb/N0 uniform in [0.5, 4] dB per codeword, f32 LOMS beta 0.5, <= 20 iterations "
+                    "with early stop; one persistent launch replayed from a CUDA graph (WifiMixedBatch)",
+        "gbps": bits / (ms * 1e-3) / 1e9, "ms_per_launch": ms, "mean_iterations": float(it.float().mean()),
+        "iterations_at_limit": int((it == 20).sum()), "codewords": len(recs), "chunks": n_chunks, "ctas": ctas,
+        "info_bits": bits}
+    return out
+
+
 def max_over_ranks(ms, world, dist=None, device=None):
     """The slowest rank's time (every rank takes part in the same collective)."""
     if world <= 1:
@@ -601,6 +680,8 @@ def main():
         line["parity_vs_cpu"] = {"mismatches": bad, "of": m,
                                  "compared": "iteration count and packed information bits of each codeword of the "
                                              "CPU sample, GPU output of the timed launches vs the CPU pipeline"}
+    if rank == 0 and world == 1 and not args.no_configs:
+        line["configs"] = configs_section(dev)
     if rank == 0 and world == 1 and not args.no_serve:
         line["serve"] = serve_section(value, dev, args)
     if rank == 0:

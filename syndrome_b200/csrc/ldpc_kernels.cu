@@ -1061,7 +1061,11 @@ Decoder::Geometry Decoder::geometry(Precision p, long long batch, bool compress)
   const long long N = g_.n();
   int cpb = std::max(1, std::min(64, kMaxThreads / Z));
   while (cpb > 1 && table_bytes(g_.edges(), g_.mb, cpb) + (long long)cpb * N * elem > 100 * 1024) --cpb;
-  if (batch > 0) cpb = (int)std::min<long long>(cpb, batch);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ < 0 ? 0 : device_);
+  // a batch too small to give every SM a full group spreads over the SMs in smaller
+  // groups (the kernels are latency-bound: fewer codewords per CTA finish sooner)
+  if (batch > 0) cpb = (int)std::min<long long>(cpb, std::max<long long>(1, (batch + sms - 1) / std::max(sms, 1)));
   geo.cpb = cpb;
   geo.threads = ((cpb * Z + 31) / 32) * 32;
   geo.smem = table_bytes(g_.edges(), g_.mb, cpb) + (int)(cpb * N * elem);
@@ -1083,9 +1087,8 @@ Decoder::Geometry Decoder::geometry(Precision p, long long batch, bool compress)
   }
   KernelFn fn = kernel_for(p, geo.maxdeg_tmpl, geo.st_words > 0);
   allow_max_dynamic_smem((const void*)fn);
-  int per_sm = 0, sms = 0;
+  int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, geo.threads, geo.smem);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ < 0 ? 0 : device_);
   geo.max_ctas = std::max(1, per_sm) * std::max(1, sms);
   return geo;
 }

@@ -571,12 +571,12 @@ struct TmCtx {
   __device__ __forceinline__ uint32_t c7f() const { return k7f; }
   template <int GE>
   __device__ __forceinline__ int vb() const {
-    // (z + shift) mod 384 in bytes: the add as a multiply-add (FMA pipe), the wrap as an
-    // unsigned min (below 384 the second candidate wraps high); the column base folds
-    // into the shared-memory instruction's immediate
+    // (z + shift) mod 384 in bytes, the wrap as an unsigned min (below 384 the second
+    // candidate wraps high; add and min fuse); the column base folds into the
+    // shared-memory instruction's immediate
     int zl = z4;
     asm volatile("" : "+r"(zl));
-    const unsigned r = mad_k((uint32_t)zl, 0, (uint32_t)(Tab<BG>::z384_shift(GE) * 4));
+    const unsigned r = (unsigned)(zl + Tab<BG>::z384_shift(GE) * 4);
     const unsigned rr = min(r, r - 384u * 4u);
     return (int)rr + Tab<BG>::col(GE) * 384 * 4;
   }
