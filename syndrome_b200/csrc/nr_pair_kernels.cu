@@ -723,41 +723,114 @@ __global__ void __launch_bounds__(kPairThreads, 2) nr_pair_tm_kernel(const __gri
   const uint32_t bq2 = pair_beta(c.beta_q);
   const int core_n = CORE * Z, K = T::KB * Z;
   const long long npairs = (c.batch + 1) / 2;
+  // 128-bit loads when every codeword row starts on a 16-byte boundary
+  const bool vec = ((reinterpret_cast<uintptr_t>(c.llr) | (uintptr_t)c.llr_stride | (uintptr_t)c.llr_offset) & 15u) == 0;
 
   for (long long g = blockIdx.x; g < npairs; g += gridDim.x) {
     const bool va = 2 * g < c.batch, vbv = 2 * g + 1 < c.batch;
     __syncthreads();
-    // ---- load: this thread's variables (col, z) of both codewords
+    // ---- load: both codewords' channel LLRs into the posteriors and extension words
     {
       const int8_t* sa = va ? c.llr + 2 * g * c.llr_stride - c.llr_offset : nullptr;
       const int8_t* sb = vbv ? c.llr + (2 * g + 1) * c.llr_stride - c.llr_offset : nullptr;
       auto fetch = [&](const int8_t* src, int j) -> int { return (src && j >= c.llr_offset) ? (int)src[j] : 0; };
       uint32_t* apw = reinterpret_cast<uint32_t*>(smem + kAp);
-      for (int col = 0; col < CORE; ++col) {
-        const int j = col * Z + z;
-        uint32_t l0 = kAB + (uint32_t)fetch(sa, j), l1 = kAB + (uint32_t)fetch(sb, j);
-        if (c.prologue) {
-          if (j < 2 * Z) {
-            l0 = l1 = kAB;
-          } else if (FILL && j >= c.k_prime && j < K) {
-            l0 = l1 = kAB + kCapV;
+      if (vec) {
+        // 128-bit loads: chunk q holds variables 16q .. 16q + 15 of one column (Z and
+        // llr_offset are multiples of 16, so a chunk never straddles a column or the
+        // transmitted boundary), turned into 16 posterior words of the pair and
+        // stored as four 128-bit words at the same place in the variable-indexed array
+        for (int q = tid; q < core_n / 16; q += Z) {
+          const int j0 = 16 * q;
+          uint4 ra = make_uint4(0u, 0u, 0u, 0u), rb = ra;
+          if (j0 >= c.llr_offset) {
+            if (sa) ra = *reinterpret_cast<const uint4*>(sa + j0);
+            if (sb) rb = *reinterpret_cast<const uint4*>(sb + j0);
           }
+          const uint32_t av[4] = {ra.x ^ 0x80808080u, ra.y ^ 0x80808080u, ra.z ^ 0x80808080u, ra.w ^ 0x80808080u};
+          const uint32_t bv[4] = {rb.x ^ 0x80808080u, rb.y ^ 0x80808080u, rb.z ^ 0x80808080u, rb.w ^ 0x80808080u};
+          uint32_t wv[16];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            // offset-binary bytes a + 128, b + 128 interleaved, then spread to 16-bit
+            // lanes: (a + 128) + (PB + 127 - 128) = PB + 127 + a, no carry between lanes
+            const uint32_t lo = prmt(av[k], bv[k], 0x5140u), hi = prmt(av[k], bv[k], 0x7362u);
+            wv[4 * k] = prmt(lo, 0u, 0x4140u) + (kAB2 - 0x00800080u);
+            wv[4 * k + 1] = prmt(lo, 0u, 0x4342u) + (kAB2 - 0x00800080u);
+            wv[4 * k + 2] = prmt(hi, 0u, 0x4140u) + (kAB2 - 0x00800080u);
+            wv[4 * k + 3] = prmt(hi, 0u, 0x4342u) + (kAB2 - 0x00800080u);
+          }
+          if (c.prologue) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int j = j0 + i;
+              if (j < 2 * Z)
+                wv[i] = kAB2;
+              else if (FILL && j >= c.k_prime && j < K)
+                wv[i] = kCapS2;
+            }
+          }
+          uint4* dst = reinterpret_cast<uint4*>(apw + j0);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) dst[k] = make_uint4(wv[4 * k], wv[4 * k + 1], wv[4 * k + 2], wv[4 * k + 3]);
         }
-        apw[j] = (l0 & 0xFFFFu) | (l1 << 16);
+      } else {
+        for (int col = 0; col < CORE; ++col) {
+          const int j = col * Z + z;
+          uint32_t l0 = kAB + (uint32_t)fetch(sa, j), l1 = kAB + (uint32_t)fetch(sb, j);
+          if (c.prologue) {
+            if (j < 2 * Z) {
+              l0 = l1 = kAB;
+            } else if (FILL && j >= c.k_prime && j < K) {
+              l0 = l1 = kAB + kCapV;
+            }
+          }
+          apw[j] = (l0 & 0xFFFFu) | (l1 << 16);
+        }
       }
       uint32_t* xw = reinterpret_cast<uint32_t*>(smem + x_off);
-#pragma unroll 1
-      for (int r = 0; r < NX; ++r) {
-        uint32_t w = 0u;
-        for (int h = 0; h < 2; ++h) {
-          const int xi = 2 * r + h;
-          if (xi < NEXT) {
-            const int j = (CORE + xi) * Z + z;
-            const uint32_t b0 = (uint32_t)(fetch(sa, j) + 128) & 0xFFu, b1 = (uint32_t)(fetch(sb, j) + 128) & 0xFFu;
-            w |= (b0 | (b1 << 8)) << (16 * h);
-          }
+      // BG1's shared state area holds both codewords' extension bytes (2 x 42 x 384 B):
+      // with 128-bit rows they are staged there in memory order, then each thread
+      // gathers its own (layer, z) bytes; the area is cleared afterwards
+      constexpr bool kStage = NSW * 4 >= 2 * NEXT;
+      if (kStage && vec) {
+        unsigned char* stage = smem + sw_off;
+        constexpr int QC = NEXT * 384 / 16;  // chunks per codeword
+        for (int q = tid; q < 2 * QC; q += Z) {
+          const int8_t* src = q < QC ? sa : sb;
+          const int qq = q < QC ? q : q - QC;
+          uint4 v = make_uint4(0u, 0u, 0u, 0u);  // absent codeword or erased variables: LLR 0
+          if (src && core_n + 16 * qq >= c.llr_offset) v = *reinterpret_cast<const uint4*>(src + core_n + 16 * qq);
+          *reinterpret_cast<uint4*>(stage + 16 * q) = v;
         }
-        xw[r * Z + tid] = w;
+        __syncthreads();
+#pragma unroll 1
+        for (int r = 0; r < NX; ++r) {
+          uint32_t w = 0u;
+          for (int h = 0; h < 2; ++h) {
+            const int xi = 2 * r + h;
+            if (xi < NEXT) {
+              const uint32_t b0 = (uint32_t)(stage[xi * 384 + z] ^ 0x80u), b1 = (uint32_t)(stage[(NEXT + xi) * 384 + z] ^ 0x80u);
+              w |= (b0 | (b1 << 8)) << (16 * h);
+            }
+          }
+          xw[r * Z + tid] = w;
+        }
+        __syncthreads();
+      } else {
+#pragma unroll 1
+        for (int r = 0; r < NX; ++r) {
+          uint32_t w = 0u;
+          for (int h = 0; h < 2; ++h) {
+            const int xi = 2 * r + h;
+            if (xi < NEXT) {
+              const int j = (CORE + xi) * Z + z;
+              const uint32_t b0 = (uint32_t)(fetch(sa, j) + 128) & 0xFFu, b1 = (uint32_t)(fetch(sb, j) + 128) & 0xFFu;
+              w |= (b0 | (b1 << 8)) << (16 * h);
+            }
+          }
+          xw[r * Z + tid] = w;
+        }
       }
       uint32_t* sw = reinterpret_cast<uint32_t*>(smem + sw_off);
 #pragma unroll 1

@@ -439,3 +439,30 @@ def test_workspace_from_wrong_decoder_is_rejected():
     assert e.value.status in (_lib.BUFFER_TOO_SMALL, _lib.INVALID_PARAM)
     with pytest.raises(S.FecError):
         large.decode_5g_with_workspace(llr, 0, ws_small, 5)
+
+
+@pytest.mark.parametrize("llr_offset,pad,prologue", [(768, 3, True), (776, 0, True), (10064, 0, False), (0, 0, False)])
+def test_int8_pair_tm_load_paths(llr_offset, pad, prologue):
+    """The Z = 384 paired kernel loads rows with 128-bit loads when every row starts on a
+    16-byte boundary (row pointer, stride and llr_offset multiples of 16) and byte by byte
+    otherwise; an llr_offset past the core columns erases extension variables too.  Both
+    paths, against the oracle (BG1 Z=384, 3 codewords)."""
+    code = O.Code.nr(0, 384)
+    dec = S.QcLdpcDecoder.with_lifting_size(0, 384, 0.5)
+    _, llr = codewords(code, 3, 1.5, 0x7E57 + llr_offset)
+    rows = np.stack([O.quantize_i16(x)[llr_offset:] for x in llr]).astype(np.int8)
+    width = rows.shape[1]
+    big = torch.zeros((3, width + pad), dtype=torch.int8, device="cuda")
+    big[:, :width] = torch.from_numpy(rows).cuda()
+    t = big[:, :width]
+    dec.set_kernel("pair")
+    r = dec.decode_batch_i8(t, 8, llr_offset=llr_offset, nr_prologue=prologue, quant=S.QuantParams(),
+                            want_app=True, want_edge_r=True, want_hard=True)
+    torch.cuda.synchronize()
+    dec.set_kernel("auto")
+    ref = O.decode_i8_batch(code, rows, O.beta_q(0.5), 8, llr_offset=llr_offset, nr_prologue=prologue,
+                            hard_bits=code.n, detail=3)
+    assert np.array_equal(r.iters.cpu().numpy(), ref["iters"])
+    assert np.array_equal(r.app.cpu().numpy(), ref["app"])
+    assert np.array_equal(r.edge_r.cpu().numpy(), ref["edge_r"])
+    assert np.array_equal(r.hard_packed.cpu().numpy().view(np.uint32), ref["packed"])
