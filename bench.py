@@ -58,6 +58,8 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=8.0, help="target CPU work of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--kernel", choices=["auto", "generic", "nr", "pair", "pair_smem"], default="auto")
+    p.add_argument("--mixed-kernel", choices=["auto", "pair_smem"], default="auto",
+                   help="mixed-shape and serving decode: tensor-memory paired kernel (auto) or shared-memory one")
     p.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     p.add_argument("--serve-pool", type=int, default=48)
     p.add_argument("--serve-seconds", type=float, default=1.0)
@@ -373,7 +375,7 @@ def serve_section(batch_gbps, dev, args):
     mean_bits = float(np.mean([p["tb_size"] for p in pool]))
     server = S.Server(max_step_code_blocks=args.serve_step_cbs, steps_in_flight=args.serve_slots, iterations=ITERS,
                       offset_beta=BETA, scale=SCALE, latency_steps=args.serve_latency_steps,
-                      backlog_code_blocks=args.serve_backlog)
+                      backlog_code_blocks=args.serve_backlog, kernel=args.mixed_kernel)
     server.run_load(pool, offered_tb_per_s=200.0, duration_s=0.05, seed=1)  # warm-up
     # capacity: offered load well above what the engine sustains, blocks per second served
     st0 = server.stats()
@@ -407,7 +409,7 @@ def serve_section(batch_gbps, dev, args):
     return {"workload": SERVE_WORKLOAD, "pool_tbs": len(pool), "mean_tb_bits": mean_bits,
             "step_code_blocks": args.serve_step_cbs, "steps_in_flight": args.serve_slots or 6,
             "latency_steps": args.serve_latency_steps or 3,
-            "backlog_code_blocks": args.serve_backlog or 128, "points": points,
+            "backlog_code_blocks": args.serve_backlog or 128, "decode_kernel": args.mixed_kernel, "points": points,
             "capacity_tb_per_s": capacity, "saturated_decoded_gbps": sat_gbps,
             "saturated_goodput_gbps": sat["info_bits_ok"] / sat["wall_s"] / 1e9,
             "saturated_decoded_vs_batch": sat_gbps / batch_gbps, "saturation_diag": sat_diag,
@@ -431,7 +433,7 @@ def time_decodes(fn, reps, stream):
     return e0.elapsed_time(e1) / reps
 
 
-def configs_section(dev):
+def configs_section(dev, mixed_kernel="auto"):
     """The benchmark's other workloads, each device-resident, information Gbit/s:
     802.11 Z=27 R=1/2 (1024 codewords, f32, <= 10 iterations, 1.5 dB), mixed 5G NR code
     blocks (65536, rate-matched, int8, <= 8 iterations, one persistent launch from a CUDA
@@ -463,6 +465,7 @@ def configs_section(dev):
     # mixed 5G NR, rate-matched
     recs, llr8, words, bits = W.nr_rate_matched(65536, 33, device=dev)
     batch = S.MixedBatch(recs, 0.5, S.QuantParams(), ITERS)
+    tmem = batch.set_kernel(mixed_kernel)
     o = torch.zeros(max(words, 1), dtype=torch.int32, device=dev)
     it = torch.zeros(len(recs), dtype=torch.int32, device=dev)
     ms = time_decodes(lambda: batch.decode(llr8, o, it, use_graph=True), 5, stream)
@@ -472,7 +475,8 @@ def configs_section(dev):
                     "(puncturing or repetition), Eb/N0 uniform in [0, 3] dB, int8 at scale 8, <= 8 iterations; one "
                     "persistent launch replayed from a CUDA graph (MixedBatch)",
         "gbps": bits / (ms * 1e-3) / 1e9, "ms_per_launch": ms, "mean_iterations": float(it.float().mean()),
-        "codewords": len(recs), "work_items": len(batch.items()), "info_bits": bits}
+        "codewords": len(recs), "work_items": len(batch.items()), "info_bits": bits,
+        "kernel": "paired, check-row state in tensor memory, 2 CTAs/SM" if tmem else "paired, shared memory, 1 CTA/SM"}
     del llr8, o, it, batch
     # mixed 802.11
     recs, llrf, words, bits = W.wifi_mixed(32768, 44, device=dev)
@@ -681,7 +685,7 @@ def main():
                                  "compared": "iteration count and packed information bits of each codeword of the "
                                              "CPU sample, GPU output of the timed launches vs the CPU pipeline"}
     if rank == 0 and world == 1 and not args.no_configs:
-        line["configs"] = configs_section(dev)
+        line["configs"] = configs_section(dev, args.mixed_kernel)
     if rank == 0 and world == 1 and not args.no_serve:
         line["serve"] = serve_section(value, dev, args)
     if rank == 0:

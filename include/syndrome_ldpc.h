@@ -336,6 +336,13 @@ void syndrome_mixed_plan_destroy(SyndromeMixedPlan* plan);
 /* Number of work items; out_items (nullable, room for `cap` items) receives
  * (base_graph, z, codewords) per item in launch order. */
 int32_t syndrome_mixed_plan_items(const SyndromeMixedPlan* plan, int32_t* out_items, size_t cap, size_t* n_items);
+/* Kernel of the plan's decode: 0 = automatic (the default; the paired kernel keeps
+ * most of its check-row state in tensor memory, two CTAs per SM, when app_clamp >=
+ * 7874 and no codeword reports hard decisions past its core columns, 26Z for BG1 and
+ * 14Z for BG2), 5 = the paired kernel with all check-row state in shared memory, one
+ * CTA per SM.  Other values give SYNDROME_INVALID_PARAM.  Both produce identical
+ * results.  *is_tmem (nullable) receives 1 when decode runs the tensor-memory form. */
+int32_t syndrome_mixed_plan_set_kernel(SyndromeMixedPlan* plan, int32_t kernel, int32_t* is_tmem);
 /* Most codewords one work item of this shape can hold with the default app_clamp
  * (paired kernel; plans with app_clamp below 7874 use smaller items). */
 int32_t syndrome_mixed_tile_capacity(int32_t base_graph, int32_t z);
@@ -467,6 +474,9 @@ typedef struct {
                                     steps_in_flight): fewer steps share the SMs, each ends sooner */
   uint32_t backlog_code_blocks;  /* waiting code blocks from which up to steps_in_flight steps
                                     run (0 = 128) */
+  int32_t decode_kernel;         /* 0 = the paired kernel with its check-row state mostly in
+                                    tensor memory (two CTAs per SM), 5 = all of it in shared
+                                    memory (one CTA per SM); identical results */
 } SyndromeServeConfig;
 typedef struct {
   uint64_t tb_id;

@@ -66,6 +66,7 @@ PROTOTYPES = {
     "syndrome_mixed_plan_create": (_i32, [_vp, _sz, _f32, _f32, ctypes.c_int16, _sz, _vp, _sz, ctypes.POINTER(_vp)]),
     "syndrome_mixed_plan_destroy": (None, [_vp]),
     "syndrome_mixed_plan_items": (_i32, [_vp, _vp, _sz, ctypes.POINTER(_sz)]),
+    "syndrome_mixed_plan_set_kernel": (_i32, [_vp, _i32, ctypes.POINTER(_i32)]),
     "syndrome_mixed_tile_capacity": (_i32, [_i32, _i32]),
     "syndrome_mixed_decode": (_i32, [_vp, _vp, _sz, _vp, _sz, _vp, _sz, _i32, _vp]),
     "syndrome_wifi_mixed_plan_create": (_i32, [_vp, _sz, _f32, _sz, _sz, ctypes.POINTER(_vp)]),

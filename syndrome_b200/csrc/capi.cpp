@@ -765,6 +765,13 @@ int32_t syndrome_mixed_plan_items(const SyndromeMixedPlan* plan, int32_t* out_it
   return SYNDROME_OK;
 }
 
+int32_t syndrome_mixed_plan_set_kernel(SyndromeMixedPlan* plan, int32_t kernel, int32_t* is_tmem) {
+  if (!plan) return SYNDROME_NULL_POINTER;
+  if (!plan->plan.set_kernel(kernel)) return fail(SYNDROME_INVALID_PARAM, "mixed-plan kernel must be 0 or 5");
+  if (is_tmem) *is_tmem = plan->plan.tmem() && kernel != 5;
+  return SYNDROME_OK;
+}
+
 int32_t syndrome_mixed_tile_capacity(int32_t base_graph, int32_t z) {
   if ((base_graph != 0 && base_graph != 1) || syn::lifting_set_index(z) < 0) return 0;
   return syn::pair_mixed_capacity(base_graph, z);
@@ -1050,6 +1057,9 @@ int32_t syndrome_serve_create(const SyndromeServeConfig* config, SyndromeServer*
       if (config->latency_steps) c.latency_slots = (int)std::min<uint32_t>(config->latency_steps, 16);
       if (config->backlog_code_blocks)
         c.backlog_cbs = (int)std::min<uint32_t>(config->backlog_code_blocks, 1u << 30);
+      if (config->decode_kernel != 0 && config->decode_kernel != 5)
+        return fail(SYNDROME_INVALID_PARAM, "decode_kernel must be 0 or 5");
+      c.decode_kernel = config->decode_kernel;
     }
     auto* s = new SyndromeServer();
     std::string err;

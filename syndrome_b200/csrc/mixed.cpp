@@ -7,7 +7,9 @@
 // decreasing work so the longest start first, and uploads the items, the per-codeword
 // records and the shift / column-base tables of every (BG, Z) used.  With app_clamp
 // >= 7874 the items go to the paired kernel (two codewords per 32-bit word,
-// nr_pair_kernels.cu), otherwise to the one-codeword-per-thread kernel (nr_kernels.cu).  decode() zeroes
+// nr_pair_kernels.cu: its tensor-memory form, two CTAs per SM, when no codeword reports
+// hard decisions past its core columns), otherwise to the one-codeword-per-thread
+// kernel (nr_kernels.cu).  decode() zeroes
 // the device work counter and launches one CTA per SM; with use_graph the two
 // operations are captured once into a CUDA graph and replayed.
 #include "mixed.h"
@@ -79,6 +81,9 @@ bool MixedPlan::init(const std::vector<MixedCodeword>& cws, int beta_q, int app_
   }
   // two codewords per 32-bit word when no non-filler posterior can reach the clamp
   const bool paired = app_clamp >= 7874;
+  bool core_only = true;  // every codeword's reported bits lie in its core columns
+  for (const MixedCodeword& c : cws)
+    if (c.hard_bits > (long long)pair_mixed_core_columns(c.bg) * c.z) core_only = false;
   std::vector<MixItem> items;
   std::vector<MixCodeword> recs;
   recs.reserve(cws.size());
@@ -136,7 +141,9 @@ bool MixedPlan::init(const std::vector<MixedCodeword>& cws, int beta_q, int app_
   if (cudaGetDevice(&device_) != cudaSuccess) return fail("no CUDA device");
   cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
   paired_ = paired;
-  if ((paired ? pair_mixed_prepare() : mixed_kernel_prepare()) != cudaSuccess)
+  tmem_ = paired && core_only;
+  if ((paired ? pair_mixed_prepare() : mixed_kernel_prepare()) != cudaSuccess ||
+      (tmem_ && pair_tm_mixed_prepare() != cudaSuccess))
     return fail("cannot configure the mixed-batch kernel");
   if (cudaMalloc(&d_items_, sizeof(MixItem) * std::max<size_t>(items.size(), 1)) != cudaSuccess ||
       cudaMalloc(&d_cws_, sizeof(MixCodeword) * std::max<size_t>(recs.size(), 1)) != cudaSuccess ||
@@ -152,6 +159,16 @@ bool MixedPlan::init(const std::vector<MixedCodeword>& cws, int beta_q, int app_
   cudaMemcpy(d_colz_, colz.data(), sizeof(int) * colz.size(), cudaMemcpyHostToDevice);
   items_ = items;
   if (cudaGetLastError() != cudaSuccess) return fail("copying the plan tables failed");
+  return true;
+}
+
+bool MixedPlan::set_kernel(int kernel) {
+  if (kernel != 0 && kernel != 5) return false;
+  if (kernel != kernel_ && exec_) {  // a captured graph holds the other kernel
+    cudaGraphExecDestroy(exec_);
+    exec_ = nullptr;
+  }
+  kernel_ = kernel;
   return true;
 }
 
@@ -178,7 +195,10 @@ cudaError_t MixedPlan::decode(const int8_t* d_llr, uint32_t* d_out, int32_t* d_i
                               cudaStream_t stream) {
   if (n_items_ == 0) return cudaSuccess;
   const MixArgs m = args(d_llr, d_out, d_iters);
-  auto launch = [&](cudaStream_t st) { return paired_ ? pair_mixed_launch(m, sms_, st) : mixed_decode_launch(m, sms_, st); };
+  auto launch = [&](cudaStream_t st) {
+    if (tmem_ && kernel_ != 5) return pair_tm_mixed_launch(m, sms_, st);
+    return paired_ ? pair_mixed_launch(m, sms_, st) : mixed_decode_launch(m, sms_, st);
+  };
   if (!use_graph) return launch(stream);
   if (!exec_ || g_llr_ != d_llr || g_out_ != d_out || g_iters_ != d_iters) {
     if (exec_) cudaGraphExecDestroy(exec_);

@@ -37,6 +37,11 @@ class MixedPlan {
   long long llr_bytes_needed() const { return need_llr_; }
   long long out_words_needed() const { return need_out_; }
   int items() const { return n_items_; }
+  // 0: automatic (the tensor-memory paired kernel when every codeword reports at most
+  // its core columns' hard decisions), 5: the shared-memory paired kernel.  Returns
+  // false for other values.
+  bool set_kernel(int kernel);
+  bool tmem() const { return tmem_; }
   int codewords() const { return n_codewords_; }
   const std::vector<MixItem>& item_list() const { return items_; }
 
@@ -45,6 +50,8 @@ class MixedPlan {
   MixArgs args(const int8_t* d_llr, uint32_t* d_out, int32_t* d_iters) const;
   int device_ = -1, sms_ = 0, n_items_ = 0, n_codewords_ = 0;
   bool paired_ = false;  // paired kernel (app_clamp >= 7874) or one codeword per thread
+  bool tmem_ = false;    // paired, and no codeword reports hard decisions past its core columns
+  int kernel_ = 0;
   int beta_q_ = 0, app_clamp_ = 32767, iterations_ = 0;
   long long need_llr_ = 0, need_out_ = 0;
   MixItem* d_items_ = nullptr;

@@ -128,6 +128,12 @@ cudaError_t nr_f32_decode(int bg, const NrF32Common& c, int z, const int* shifts
 int pair_mixed_capacity(int bg, int z);
 cudaError_t pair_mixed_prepare();
 cudaError_t pair_mixed_launch(const MixArgs& m, int sms, cudaStream_t stream);
+// The same decode with the check-row state mostly in tensor memory, two CTAs per SM
+// (same items and results); for batches whose codewords report hard decisions of at
+// most their pair_mixed_core_columns(bg) * z core variables.
+cudaError_t pair_tm_mixed_prepare();
+cudaError_t pair_tm_mixed_launch(const MixArgs& m, int sms, cudaStream_t stream);
+int pair_mixed_core_columns(int bg);
 // tmem: at Z = 384, the variant that keeps most check-row state in tensor memory (two
 // codeword pairs per SM) instead of the one that keeps it all in shared memory.
 cudaError_t nr_pair_decode_i8(int bg, const NrCommon& c, const int* shifts, int sms, cudaStream_t stream,

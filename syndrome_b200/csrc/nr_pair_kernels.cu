@@ -519,6 +519,15 @@ template <int BG>
 __host__ __device__ constexpr int smem_bytes() {
   return kAp + (Tab<BG>::KB + 4) * 384 * 4 + (sm_words<BG>() + ext_regs<BG>()) * 384 * 4;
 }
+// Dynamic shared memory a TMEM-kernel CTA is launched with: at least a third of the
+// SM's 228 KB, so that no SM ever holds three CTAs of the TMEM kernels (each takes 256
+// of the SM's 512 TMEM columns; a third would wait in tcgen05.alloc), whatever the
+// register count.
+constexpr int kTwoPerSm = 233472 / 3 + 16;
+template <int BG>
+__host__ __device__ constexpr int launch_smem() {
+  return smem_bytes<BG>() > kTwoPerSm ? smem_bytes<BG>() : kTwoPerSm;
+}
 
 // ---- tcgen05 storage primitives (sm_100a) ----
 __device__ __forceinline__ void ld2(uint32_t t, uint32_t (&v)[4]) {
@@ -557,33 +566,52 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 
 // Row context of the TMEM variant.  pf holds the next TMEM row while its load is in
 // flight; the cold paths (syndrome stages, outputs) run only while no load is in
-// flight, which is what lets them work on a copy of the context.
-template <int BG>
+// flight, which is what lets them work on a copy of the context.  State and extension
+// words are laid out for 384 threads.  ZT = 384: one codeword pair at Z = 384, its
+// posteriors at byte APC of pair_smem, compile-time shifts.  ZT = -1 (mixed-shape
+// kernel): any Z, the thread's pair's posteriors at byte `ap`, shifts and column bases
+// from the item's table at byte `tab` (4 * shift [E], then 4 * col * Z [E]); a thread
+// past the item's pairs runs the row updates on pair 0's posteriors without storing
+// them (`live` false), so that every TMEM access stays warp-wide.
+template <int BG, int ZT = 384, int APC = kAp>
 struct TmCtx {
+  static_assert(ZT == 384 || ZT == -1, "TMEM context: Z = 384 or run-time Z");
   uint32_t tmb;  // TMEM address of this thread's slot: lane (32 * (warp % 4)) << 16 | column
   int st;        // byte offset in pair_smem of this thread's first shared state word
   int xo;        // byte offset in pair_smem of this thread's first extension channel word
   int z4;
   uint32_t sc, k7f;
+  int ap, tab, Z4;  // ZT = -1 only
+  bool live;        // ZT = -1 only
   uint32_t pf[4];
 
   __device__ __forceinline__ uint32_t selc() const { return sc; }
   __device__ __forceinline__ uint32_t c7f() const { return k7f; }
   template <int GE>
   __device__ __forceinline__ int vb() const {
-    // (z + shift) mod 384 in bytes, the wrap as an unsigned min (below 384 the second
-    // candidate wraps high; add and min fuse); the column base folds into the
-    // shared-memory instruction's immediate
+    // (z + shift) mod Z in bytes, the wrap as an unsigned min (below Z the second
+    // candidate wraps high; add and min fuse); at Z = 384 the column base folds into
+    // the shared-memory instruction's immediate
     int zl = z4;
     asm volatile("" : "+r"(zl));
-    const unsigned r = (unsigned)(zl + Tab<BG>::z384_shift(GE) * 4);
-    const unsigned rr = min(r, r - 384u * 4u);
-    return (int)rr + Tab<BG>::col(GE) * 384 * 4;
+    if constexpr (ZT > 0) {
+      const unsigned r = (unsigned)(zl + Tab<BG>::z384_shift(GE) * 4);
+      const unsigned rr = min(r, r - 384u * 4u);
+      return (int)rr + Tab<BG>::col(GE) * 384 * 4;
+    } else {
+      const int* t = reinterpret_cast<const int*>(pair_smem + tab);
+      const unsigned r = (unsigned)(zl + t[GE]);
+      const unsigned rr = min(r, r - (unsigned)Z4);
+      return (int)rr + t[Tab<BG>::E + GE];
+    }
   }
+  __device__ __forceinline__ int apb() const { return ZT > 0 ? APC : ap; }
   __device__ __forceinline__ uint32_t ld_ap(int b) const {
-    return *reinterpret_cast<const uint32_t*>(pair_smem + kAp + b);
+    return *reinterpret_cast<const uint32_t*>(pair_smem + apb() + b);
   }
-  __device__ __forceinline__ void st_ap(int b, uint32_t v) { *reinterpret_cast<uint32_t*>(pair_smem + kAp + b) = v; }
+  __device__ __forceinline__ void st_ap(int b, uint32_t v) {
+    if (ZT > 0 || live) *reinterpret_cast<uint32_t*>(pair_smem + apb() + b) = v;
+  }
   __device__ __forceinline__ uint32_t xr(int i) const {
     return *reinterpret_cast<const uint32_t*>(pair_smem + xo + 4 * 384 * i);
   }
@@ -652,12 +680,13 @@ struct TmCtx {
   }
 };
 
-// BG1 head layer l (0..3) over a TmCtx<0>: layer 0's compile-time structure with
-// layer l's addresses and TMEM row (columns 4l .. 4l + 3).
-struct TmHeadCtx {
-  TmCtx<0>& b;
+// BG1 head layer l (0..3) over a TmCtx<0, 384, APC>: layer 0's compile-time structure
+// with layer l's addresses and TMEM row (columns 4l .. 4l + 3).
+template <int APC>
+struct TmHeadCtxT {
+  TmCtx<0, 384, APC>& b;
   int l;
-  __device__ TmHeadCtx(TmCtx<0>& base, int layer) : b(base), l(layer) {}
+  __device__ TmHeadCtxT(TmCtx<0, 384, APC>& base, int layer) : b(base), l(layer) {}
   __device__ __forceinline__ uint32_t selc() const { return b.selc(); }
   __device__ __forceinline__ uint32_t c7f() const { return b.c7f(); }
   template <int GE>
@@ -899,7 +928,7 @@ __global__ void __launch_bounds__(kPairThreads, 2) nr_pair_tm_kernel(const __gri
       if constexpr (BG == 0) {
 #pragma unroll 1
         for (int l = 0; l < 4; ++l) {
-          TmHeadCtx h(cx, l);
+          TmHeadCtxT<kAp> h(cx, l);
           pair_row<0, 0, FILL>(h, bq2);
           __syncthreads();
         }
@@ -949,7 +978,7 @@ cudaError_t launch_tm(const NrCommon& c0, int sms, cudaStream_t stream) {
   a.c.cpb = 1;
   const long long npairs = (c0.batch + 1) / 2;
   auto fn = nr_pair_tm_kernel<BG, FILL>;
-  constexpr int smem = smem_bytes<BG>();
+  constexpr int smem = launch_smem<BG>();
   cudaError_t e = allow_max_dynamic_smem((const void*)fn);
   if (e != cudaSuccess) return e;
   // The whole unified L1 / shared array as shared memory, so that two CTAs (2 x 107 KB
@@ -1150,6 +1179,224 @@ __global__ void __launch_bounds__(kPairThreads, 1) nr_pair_mixed_kernel(const __
   }
 }
 
+// ------------------------------------------------- mixed shapes, TMEM state --
+//
+// The mixed-shape decode with the state layout of nr_pair_tm_kernel: two CTAs per SM,
+// each with 256 TMEM columns for the CTA's life, taking work items from the device
+// queue (an item: up to 2 * floor(384 / Z) codewords of one (BG, Z) as consecutive
+// pairs).  Every thread runs every row update, syndrome stage and TMEM access of an
+// item -- threads past the item's pairs on pair 0's posteriors without storing them,
+// and the full syndrome stage for all threads whenever any pair passed the quick one --
+// so that the warp-wide tcgen05 instructions never diverge (a warp can hold the rows
+// of two pairs, which stop at different iterations).  The only per-pair work is the
+// output: iterations and the packed hard decisions of the core columns, read from
+// shared memory; a batch in which some codeword reports hard decisions beyond its
+// core columns (the extension columns' decisions live in TMEM rows) goes to
+// nr_pair_mixed_kernel instead.
+
+constexpr int kTmMixTab = 16;                                    // 4 * shift [316], 4 * col * z [316]
+constexpr int kTmMixFlags = kTmMixTab + 2 * 316 * 4;             // s_fail [192], s_done [192]
+constexpr int kTmMixAp = kTmMixFlags + 2 * 192 * 4;              // posteriors, <= 26 * 384 words
+constexpr int kTmMixSt = kTmMixAp + 26 * 384 * 4;                // shared state words [sm_words][384]
+constexpr int kTmMixX = kTmMixSt + tm::sm_words<0>() * 384 * 4;  // extension words [ext_regs][384]
+constexpr int kTmMixSmem = kTmMixX + ext_regs<0>() * 384 * 4;
+static_assert(kTmMixAp % 16 == 0 && kTmMixSt % 16 == 0 && kTmMixX % 16 == 0, "alignment");
+static_assert(tm::sm_words<1>() <= tm::sm_words<0>() && ext_regs<1>() <= ext_regs<0>() && 14 <= 26, "BG2 fits BG1's layout");
+static_assert(kTmMixSmem + 1024 <= 233472 / 2, "two CTAs per SM");
+// ... and never three of the two TMEM kernels on one SM (each holds 256 of the SM's
+// 512 TMEM columns, so a third would wait in tcgen05.alloc)
+static_assert(kTmMixSmem >= tm::kTwoPerSm, "at most two TMEM CTAs per SM");
+
+template <int BG, int ZT>
+__device__ __noinline__ void tm_mixed_item(const MixArgs& m, const MixItem& it, uint32_t tmb) {
+  using T = Tab<BG>;
+  using Ctx = tm::TmCtx<BG, ZT, kTmMixAp>;
+  constexpr int CORE = T::KB + 4, NEXT = T::MB - 4, NX = ext_regs<BG>(), NSW = tm::sm_words<BG>();
+  constexpr int NS = kPairThreads;
+  unsigned char* smem = pair_smem;
+  const int tid = (int)threadIdx.x;
+  const int Z = ZT > 0 ? ZT : it.z;
+  const int P = ZT > 0 ? 1 : (it.count + 1) / 2;
+  if (ZT < 0) {
+    int* t = reinterpret_cast<int*>(smem + kTmMixTab);
+    const short* sh = m.shift_tab + (long long)(BG * kMixLiftSizes + it.zi) * kMixEdges;
+    const int* cz = m.colz_tab + (long long)(BG * kMixLiftSizes + it.zi) * kMixEdges;
+    for (int e = tid; e < T::E; e += NS) {
+      t[e] = 4 * (int)sh[e];
+      t[T::E + e] = 4 * cz[e];
+    }
+  }
+  int* s_fail = reinterpret_cast<int*>(smem + kTmMixFlags);
+  int* s_done = s_fail + 192;
+  const int ap_pair = CORE * Z * 4;
+  const int p = tid / Z, z = tid - p * Z;
+  const bool lane_ok = p < P;
+  const int pq = lane_ok ? p : 0, zq = lane_ok ? z : 0;
+  Ctx cx;
+  cx.tmb = tmb;
+  cx.st = kTmMixSt + 4 * tid;
+  cx.xo = kTmMixX + 4 * tid;
+  cx.z4 = zq * 4;
+  cx.sc = 0xC480u;
+  cx.k7f = 0x7F7F7F7Fu;
+  asm volatile("" : "+r"(cx.sc), "+r"(cx.k7f));
+  cx.ap = kTmMixAp + pq * ap_pair;
+  cx.tab = kTmMixTab;
+  cx.Z4 = Z * 4;
+  cx.live = lane_ok;
+  const uint32_t bq2 = pair_beta(m.beta_q);
+  const int K = T::KB * Z;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = NS >> 5;
+  const bool va = lane_ok && 2 * p < it.count, vbv = lane_ok && 2 * p + 1 < it.count;
+  // ---- load: channel LLRs of variables 2Z..N (the punctured 2Z are erasures), the
+  // filler proxy for every codeword's filler bits, cleared state
+  {
+    const MixCodeword ca = m.cws[it.first + 2 * pq];
+    const MixCodeword cb = vbv ? m.cws[it.first + 2 * p + 1] : ca;
+    const int8_t* sa = va ? m.llr + ca.llr_off - 2 * Z : nullptr;
+    const int8_t* sb = vbv ? m.llr + cb.llr_off - 2 * Z : nullptr;
+    auto fetch = [&](const int8_t* src, int j) -> int { return (src && j >= 2 * Z) ? (int)src[j] : 0; };
+    if (lane_ok) {
+      const int kpa = ca.n_filler > K ? 0 : K - ca.n_filler, kpb = cb.n_filler > K ? 0 : K - cb.n_filler;
+      uint32_t* apw = reinterpret_cast<uint32_t*>(smem + cx.ap);
+      for (int col = 0; col < CORE; ++col) {
+        const int j = col * Z + z;
+        uint32_t l0 = kAB + (uint32_t)fetch(sa, j), l1 = kAB + (uint32_t)fetch(sb, j);
+        if (j >= kpa && j < K) l0 = kAB + kCapV;
+        if (j >= kpb && j < K) l1 = kAB + kCapV;
+        apw[j] = (l0 & 0xFFFFu) | (l1 << 16);
+      }
+    }
+    uint32_t* xw = reinterpret_cast<uint32_t*>(smem + kTmMixX);
+#pragma unroll 1
+    for (int r = 0; r < NX; ++r) {
+      uint32_t w = 0u;
+      for (int h = 0; h < 2; ++h) {
+        const int xi = 2 * r + h;
+        if (xi < NEXT) {
+          const int j = (CORE + xi) * Z + z;
+          const uint32_t b0 = (uint32_t)(fetch(sa, j) + 128) & 0xFFu, b1 = (uint32_t)(fetch(sb, j) + 128) & 0xFFu;
+          w |= (b0 | (b1 << 8)) << (16 * h);
+        }
+      }
+      xw[r * NS + tid] = w;
+    }
+    uint32_t* sw = reinterpret_cast<uint32_t*>(smem + kTmMixSt);
+#pragma unroll 1
+    for (int w = 0; w < NSW; ++w) sw[w * NS + tid] = 0u;
+#pragma unroll 1
+    for (int col = 0; col + 4 <= tm::kSlot; col += 4) tm::st4(tmb + (uint32_t)col, 0u, 0u, 0u, 0u);
+    tm::st1(tmb + (uint32_t)(tm::kSlot - 1), 0u);
+    tm::wait_st();
+  }
+  __syncthreads();
+  const int core_n = CORE * Z;
+  uint32_t act = (va ? 1u : 0u) | (vbv ? 2u : 0u);
+  uint32_t done = m.iterations <= 0 ? act : 0u;
+  int itn = 0;
+  for (;;) {
+#pragma unroll 1
+    for (int X = 0; X < 2; ++X) {
+      const bool mine = ((done >> X) & 1u) != 0u;
+      if (!__syncthreads_or(mine)) continue;
+      if (lane_ok && z == 0) s_done[p] = mine ? 1 : 0;
+      if (mine && z == 0 && m.iters) m.iters[m.cws[it.first + 2 * p + X].index] = itn;
+      __syncthreads();
+      for (int q = 0; q < P; ++q) {
+        if (!s_done[q]) continue;
+        const MixCodeword cw = m.cws[it.first + 2 * q + X];
+        const uint32_t* apq = reinterpret_cast<const uint32_t*>(smem + kTmMixAp + q * ap_pair);
+        uint32_t* dst = m.out + cw.out_off;
+        const int nwords = (cw.hard_bits + 31) >> 5;  // hard_bits <= core_n: the plan checks
+        for (int w = warp; w < nwords; w += nwarps) {
+          const int j = (w << 5) + lane;
+          const bool bit = j < cw.hard_bits && j < core_n && lane_of(apq[j], X, kAB) < 0;
+          const uint32_t mm = __ballot_sync(0xFFFFFFFFu, bit);
+          if (lane == 0) dst[w] = mm;
+        }
+      }
+      __syncthreads();
+    }
+    act &= ~done;
+    if (!__syncthreads_or(act != 0u)) break;
+    ++itn;
+    cx.first_row();
+    constexpr bool head_loop = BG == 0 && ZT > 0;
+    if constexpr (head_loop) {
+#pragma unroll 1
+      for (int l = 0; l < 4; ++l) {
+        tm::TmHeadCtxT<kTmMixAp> h(cx, l);
+        pair_row<0, 0, true>(h, bq2);
+        __syncthreads();
+      }
+    }
+    static_for<head_loop ? 4 : 0, T::MB>([&](auto li) {
+      constexpr int L = decltype(li)::value;
+      pair_row<BG, L, true>(cx, bq2);
+      if constexpr (nr::barrier_after<BG>(L)) __syncthreads();
+    });
+    tm::wait_st();  // this iteration's TMEM rows before the syndrome stages read them
+    if (lane_ok && z == 0) s_fail[p] = 0;
+    __syncthreads();
+    {
+      const uint32_t odd = quick_parity<BG>(cx) & act;
+      if (odd) atomicOr(&s_fail[pq], (int)odd);
+    }
+    __syncthreads();
+    const uint32_t pass = act & ~(uint32_t)(lane_ok ? s_fail[p] : 0);
+    if (__syncthreads_or(pass != 0u)) {  // every thread, so that the TMEM reads stay warp-wide
+      const Ctx copy = cx;
+      const uint32_t odd = full_parity<BG>(&copy) & pass;
+      if (odd) atomicOr(&s_fail[pq], (int)odd);
+    }
+    __syncthreads();
+    done = itn >= m.iterations ? act : act & ~(uint32_t)(lane_ok ? s_fail[p] : 0);
+  }
+}
+
+__global__ void __launch_bounds__(kPairThreads, 2) nr_pair_tm_mixed_kernel(const __grid_constant__ MixArgs m) {
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(pair_smem);
+  int* s_item = reinterpret_cast<int*>(pair_smem + 4);
+  const int warp = (int)threadIdx.x >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(s_tmem)),
+                 "r"(tm::kCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tm::fence_before();
+  __syncthreads();
+  tm::fence_after();
+  const uint32_t tmb = *s_tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(tm::kSlot * (warp >> 2));
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) *s_item = (int)atomicAdd(m.queue, 1u);
+    __syncthreads();
+    const int item = *s_item;
+    if (item >= m.n_items) break;
+    const MixItem it = m.items[item];
+    if (it.bg == 0) {
+      if (it.z == 384)
+        tm_mixed_item<0, 384>(m, it, tmb);
+      else
+        tm_mixed_item<0, -1>(m, it, tmb);
+    } else {
+      if (it.z == 384)
+        tm_mixed_item<1, 384>(m, it, tmb);
+      else
+        tm_mixed_item<1, -1>(m, it, tmb);
+    }
+  }
+  tm::wait_st();
+  tm::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tm::fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*s_tmem), "r"(tm::kCols) : "memory");
+  }
+}
+
 }  // namespace nrp
 
 bool nr_pair_applies(const NrCommon& c) {
@@ -1177,6 +1424,26 @@ cudaError_t pair_mixed_prepare() {
   return cudaFuncSetAttribute(nrp::nr_pair_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               nrp::kPairMixSmem);
 }
+
+cudaError_t pair_tm_mixed_prepare() {
+  cudaError_t e = cudaFuncSetAttribute(nrp::nr_pair_tm_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       nrp::kTmMixSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(nrp::nr_pair_tm_mixed_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              cudaSharedmemCarveoutMaxShared);
+}
+
+// Two CTAs per SM (80 registers x 384 threads: never more on one SM, so their 2 x 256
+// TMEM columns never exceed the SM's 512).
+cudaError_t pair_tm_mixed_launch(const MixArgs& m, int sms, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(m.queue, 0, sizeof(unsigned), stream);
+  if (e != cudaSuccess) return e;
+  const int ctas = std::max(1, std::min(2 * sms, m.n_items));
+  nrp::nr_pair_tm_mixed_kernel<<<ctas, nrp::kPairThreads, nrp::kTmMixSmem, stream>>>(m);
+  return cudaGetLastError();
+}
+
+int pair_mixed_core_columns(int bg) { return bg == 0 ? 26 : 14; }
 
 cudaError_t pair_mixed_launch(const MixArgs& m, int sms, cudaStream_t stream) {
   cudaError_t e = cudaMemsetAsync(m.queue, 0, sizeof(unsigned), stream);

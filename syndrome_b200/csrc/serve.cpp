@@ -106,7 +106,9 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
   if (cudaGetDevice(&device_) != cudaSuccess) return fail("no CUDA device");
   cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
   paired_ = cfg_.app_clamp >= 7874;
-  if ((paired_ ? pair_mixed_prepare() : mixed_kernel_prepare()) != cudaSuccess)
+  tmem_ = paired_ && cfg_.decode_kernel != 5;  // code blocks report their K' <= K bits
+  if ((paired_ ? pair_mixed_prepare() : mixed_kernel_prepare()) != cudaSuccess ||
+      (tmem_ && pair_tm_mixed_prepare() != cudaSuccess))
     return fail("cannot configure the decode kernel");
   // shift and column-base tables of every 5G NR shape
   std::vector<short> shift((size_t)2 * kMixLiftSizes * kMixEdges, 0);
@@ -404,7 +406,9 @@ bool ServeEngine::launch_step(Slot& s) {
   m.k32 = 32;
   m.two = 2;
   if (e == cudaSuccess) e = cudaEventRecord(s.t0, st);
-  if (e == cudaSuccess) e = paired_ ? pair_mixed_launch(m, sms_, st) : mixed_decode_launch(m, sms_, st);
+  if (e == cudaSuccess)
+    e = tmem_ ? pair_tm_mixed_launch(m, sms_, st)
+              : (paired_ ? pair_mixed_launch(m, sms_, st) : mixed_decode_launch(m, sms_, st));
   if (e == cudaSuccess) e = cudaEventRecord(s.t1, st);
   if (e == cudaSuccess) e = serve_cb_crc_launch(s.d_cbs, n_cbs, s.d_crc, st);
   if (e == cudaSuccess) e = serve_tb_finish_launch(s.d_tbs, n_tb, s.d_cbs, s.d_crc, s.d_iters, st);

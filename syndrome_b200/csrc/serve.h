@@ -41,6 +41,9 @@ struct ServeConfig {
   float beta = 0.5f;
   float scale = 8.0f;
   int app_clamp = 32767;
+  // Code-block decode: 0 = the paired kernel in its tensor-memory form (two CTAs per SM),
+  // 5 = the paired kernel with all state in shared memory (one CTA per SM).
+  int decode_kernel = 0;
 };
 
 struct ServeResult {
@@ -144,6 +147,7 @@ class ServeEngine {
   ServeConfig cfg_;
   int device_ = 0, sms_ = 0, max_words_ = 0, max_tb_words_ = 0, beta_q_ = 0;
   bool paired_ = false;  // paired mixed-shape decode (app_clamp >= 7874)
+  bool tmem_ = false;    // ... in its tensor-memory form
   char* d_harq_ = nullptr;
   short* d_shift_ = nullptr;
   int* d_colz_ = nullptr;

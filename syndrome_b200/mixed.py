@@ -57,6 +57,18 @@ class MixedBatch:
             except Exception:
                 pass
 
+    def set_kernel(self, kernel="auto"):
+        """"auto" (the paired kernel with most of its check-row state in tensor
+        memory, two CTAs per SM, when app_clamp >= 7874 and no codeword reports hard
+        decisions past its core columns) or "pair_smem" (all of it in shared memory,
+        one CTA per SM).  Returns True when decode runs the tensor-memory form."""
+        code = {"auto": 0, "pair_smem": 5}.get(kernel)
+        if code is None:
+            raise ValueError(f"unknown mixed-batch kernel {kernel!r}")
+        tm = ctypes.c_int32(0)
+        _lib.check(_lib.load().syndrome_mixed_plan_set_kernel(self._h, code, ctypes.byref(tm)))
+        return bool(tm.value)
+
     def items(self):
         """(base_graph, z, codewords) of each work item in launch order."""
         L = _lib.load()

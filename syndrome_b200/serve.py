@@ -16,7 +16,8 @@ class _Config(ctypes.Structure):
     _fields_ = [("max_step_code_blocks", ctypes.c_uint32), ("steps_in_flight", ctypes.c_uint32),
                 ("harq_bytes", ctypes.c_uint64), ("staging_bytes", ctypes.c_uint64), ("iterations", ctypes.c_int32),
                 ("offset_beta", ctypes.c_float), ("scale", ctypes.c_float), ("app_clamp", ctypes.c_int32),
-                ("latency_steps", ctypes.c_uint32), ("backlog_code_blocks", ctypes.c_uint32)]
+                ("latency_steps", ctypes.c_uint32), ("backlog_code_blocks", ctypes.c_uint32),
+                ("decode_kernel", ctypes.c_int32)]
 
 
 class _Result(ctypes.Structure):
@@ -50,9 +51,13 @@ class Server:
     accumulators, 256 MiB of staging for host-memory LLRs)."""
 
     def __init__(self, max_step_code_blocks=0, steps_in_flight=0, harq_bytes=0, staging_bytes=0, iterations=8,
-                 offset_beta=0.5, scale=8.0, app_clamp=32767, latency_steps=0, backlog_code_blocks=0):
+                 offset_beta=0.5, scale=8.0, app_clamp=32767, latency_steps=0, backlog_code_blocks=0,
+                 kernel="auto"):
+        code = {"auto": 0, "pair_smem": 5}.get(kernel)
+        if code is None:
+            raise ValueError(f"unknown serving kernel {kernel!r}")
         cfg = _Config(max_step_code_blocks, steps_in_flight, harq_bytes, staging_bytes, iterations, offset_beta,
-                      scale, app_clamp, latency_steps, backlog_code_blocks)
+                      scale, app_clamp, latency_steps, backlog_code_blocks, code)
         h = ctypes.c_void_p()
         _lib.check(_lib.load().syndrome_serve_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h.value

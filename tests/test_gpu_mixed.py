@@ -1,6 +1,8 @@
 """Mixed-shape persistent decode (one launch over codewords of any BG / Z mix)
 against the oracle's decode_5g_i8 path, codeword by codeword: iterations and hard
-decisions bit-identical."""
+decisions bit-identical.  The paired cases run both forms of the paired kernel: the
+default one with most check-row state in tensor memory (two CTAs per SM) and the
+shared-memory one ("pair_smem", one CTA per SM)."""
 import numpy as np
 import pytest
 
@@ -12,7 +14,7 @@ pytestmark = pytest.mark.gpu
 import syndrome_b200 as S  # noqa: E402
 
 
-def build_mix(shapes, seed, clamp=32767):
+def build_mix(shapes, seed, clamp=32767, report_all=False):
     rng = np.random.default_rng(seed)
     recs, rows, refs = [], [], []
     llr_off, out_off = 0, 0
@@ -26,7 +28,7 @@ def build_mix(shapes, seed, clamp=32767):
         app[: 2 * z] = 0
         row = app[2 * z:].astype(np.int8)
         ref = code.decode_i8(code.prologue_5g_i8(app, n_filler, clamp), O.beta_q(0.5), 8, clamp)
-        hard_bits = code.k - n_filler
+        hard_bits = code.n if report_all else code.k - n_filler
         recs.append((bg, z, n_filler, hard_bits, llr_off, out_off))
         rows.append(row)
         refs.append((ref, hard_bits))
@@ -56,7 +58,13 @@ def check(batch, buf, n_words, refs, use_graph=False, reps=1):
         assert np.array_equal(bits, ref["hard"][:hard_bits]), f"codeword {i} {tuple(rec)}: hard bits differ"
 
 
-def test_mixed_batch_matches_oracle():
+def use_kernel(batch, kernel):
+    tm = batch.set_kernel(kernel)
+    assert tm == (kernel == "auto"), f"{kernel}: tensor-memory form {tm}"
+
+
+@pytest.mark.parametrize("kernel", ["auto", "pair_smem"])
+def test_mixed_batch_matches_oracle(kernel):
     rng = np.random.default_rng(5)
     shapes = [(1, int(z)) for z in rng.choice([z for z in S.LIFTING_SIZES if z <= 64], 40)]
     shapes += [(0, int(z)) for z in rng.choice([2, 5, 13, 32, 64], 20)]
@@ -66,6 +74,17 @@ def test_mixed_batch_matches_oracle():
     recs, buf, n_words, refs = build_mix(shapes, 11)
     batch = S.MixedBatch(recs, 0.5, S.QuantParams(), 8)
     assert sum(c for _, _, c in batch.items()) == len(shapes)
+    use_kernel(batch, kernel)
+    check(batch, buf, n_words, refs)
+
+
+def test_mixed_batch_reporting_every_variable():
+    """Codewords reporting hard decisions past their core columns run the
+    shared-memory paired kernel, whose extension decisions are in shared memory."""
+    shapes = [(0, 384), (1, 384), (0, 64), (1, 26), (1, 2), (0, 160)] * 2
+    recs, buf, n_words, refs = build_mix(shapes, 61, report_all=True)
+    batch = S.MixedBatch(recs, 0.5, S.QuantParams(), 8)
+    assert not batch.set_kernel("auto")
     check(batch, buf, n_words, refs)
 
 
@@ -78,19 +97,34 @@ def test_mixed_batch_one_codeword_per_thread_kernel():
     check(batch, buf, n_words, refs)
 
 
-def test_mixed_batch_odd_counts_per_shape():
-    """Paired items with an odd codeword count leave one lane empty."""
-    shapes = [(0, 384)] * 3 + [(1, 384)] * 5 + [(0, 7)] * 9 + [(1, 2)] * 1
+@pytest.mark.parametrize("kernel", ["auto", "pair_smem"])
+def test_mixed_batch_odd_counts_per_shape(kernel):
+    """Paired items with an odd codeword count leave one lane empty; items of small Z
+    leave the threads past their pairs idle."""
+    shapes = [(0, 384)] * 3 + [(1, 384)] * 5 + [(0, 7)] * 9 + [(1, 2)] * 1 + [(0, 240)] * 3 + [(1, 176)] * 2
     recs, buf, n_words, refs = build_mix(shapes, 57)
     batch = S.MixedBatch(recs, 0.5, S.QuantParams(), 8)
+    use_kernel(batch, kernel)
     check(batch, buf, n_words, refs)
 
 
-def test_mixed_batch_graph_replay_and_tiles():
+@pytest.mark.parametrize("kernel", ["auto", "pair_smem"])
+def test_mixed_batch_graph_replay_and_tiles(kernel):
     shapes = [(1, 13)] * 30 + [(0, 16)] * 20 + [(1, 52)] * 7
     recs, buf, n_words, refs = build_mix(shapes, 23)
     batch = S.MixedBatch(recs, 0.5, S.QuantParams(), 8, tile_hints={(1, 13): 4, (0, 16): 1})
     items = batch.items()
     assert all(c <= 4 for bg, z, c in items if (bg, z) == (1, 13))
     assert all(c == 1 for bg, z, c in items if (bg, z) == (0, 16))
+    use_kernel(batch, kernel)
     check(batch, buf, n_words, refs, use_graph=True, reps=3)
+    # switching the kernel drops the captured graph; the other kernel replays the same
+    use_kernel(batch, "pair_smem" if kernel == "auto" else "auto")
+    check(batch, buf, n_words, refs, use_graph=True, reps=2)
+
+
+def test_mixed_batch_rejects_unknown_kernel():
+    recs, _, _, _ = build_mix([(1, 13)], 3)
+    batch = S.MixedBatch(recs)
+    with pytest.raises(ValueError):
+        batch.set_kernel("tmem")

@@ -17,7 +17,7 @@ and compare every codeword with the oracle:
   codeword pairs per CTA);
 * f32, 5G NR BG1 Z=384: iteration counts and hard decisions bit-identical,
   posteriors within 1e-5 relative (checked bit-identical as well);
-* the persistent mixed-shape kernel with more work items than SMs.
+* the persistent mixed-shape kernel, both forms, with more work items than CTAs.
 """
 import numpy as np
 import pytest
@@ -133,11 +133,14 @@ def test_f32_batch_matches_oracle_at_scale():
         assert np.array_equal(app[i].view(np.uint32), want.view(np.uint32)), f"codeword {b}: posteriors not exact"
 
 
-def test_mixed_kernel_with_more_items_than_sms():
-    """More work items than SMs, so persistent CTAs take several items from the device
-    queue; Z = 384 items (one codeword pair each) and small-Z items mixed."""
+@pytest.mark.parametrize("kernel", ["auto", "pair_smem"])
+def test_mixed_kernel_with_more_items_than_sms(kernel):
+    """More work items than CTAs, so persistent CTAs take several items from the
+    device queue (the tensor-memory form runs two CTAs per SM: 296 on 148 SMs, the
+    shared-memory one 148); Z = 384 items (one codeword pair each) and small-Z items
+    mixed."""
     rng = np.random.default_rng(77)
-    shapes = [(0, 384)] * 150 + [(1, 384)] * 150 + [(1, int(z)) for z in rng.choice([13, 26, 52, 104], 60)]
+    shapes = [(0, 384)] * 300 + [(1, 384)] * 300 + [(1, int(z)) for z in rng.choice([13, 26, 52, 104], 60)]
     shapes = [shapes[i] for i in rng.permutation(len(shapes))]
     recs, rows, refs = [], [], []
     llr_off, out_off = 0, 0
@@ -158,7 +161,8 @@ def test_mixed_kernel_with_more_items_than_sms():
     for (_, _, _, _, off, _), row in zip(recs, rows):
         buf[off: off + row.size] = row
     batch = S.MixedBatch(np.array(recs, dtype=S.CODEWORD_DTYPE), 0.5, S.QuantParams(), 8)
-    assert len(batch.items()) > 148
+    assert len(batch.items()) > 2 * 148
+    assert batch.set_kernel(kernel) == (kernel == "auto")
     llr = torch.from_numpy(buf).cuda()
     out = torch.zeros(max(out_off, 1), dtype=torch.int32, device="cuda")
     iters = torch.zeros(len(refs), dtype=torch.int32, device="cuda")

@@ -86,8 +86,9 @@ def check_against_oracle(data, reports, payloads, iterations=8):
                 assert np.array_equal(payloads[tid], tb), label + ": CRC passed on a wrong payload"
 
 
-def test_serve_matches_oracle_with_harq():
-    server = S.Server(iterations=8)
+@pytest.mark.parametrize("kernel", ["auto", "pair_smem"])
+def test_serve_matches_oracle_with_harq(kernel):
+    server = S.Server(iterations=8, kernel=kernel)
     data, reports, payloads = run_sequences(server, CASES)
     assert any(len(v) > 1 for v in reports.values()), "no retransmission happened: raise the noise"
     assert any(v[-1]["crc_ok"] for v in reports.values())
