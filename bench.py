@@ -60,6 +60,8 @@ def parse_args():
     p.add_argument("--kernel", choices=["auto", "generic", "nr", "pair", "pair_smem"], default="auto")
     p.add_argument("--mixed-kernel", choices=["auto", "pair_smem"], default="auto",
                    help="mixed-shape and serving decode: tensor-memory paired kernel (auto) or shared-memory one")
+    p.add_argument("--serve-engine", choices=["continuous", "steps"], default="continuous",
+                   help="serving engine: one persistent kernel fed per transmission, or steps of code blocks")
     p.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     p.add_argument("--serve-pool", type=int, default=48)
     p.add_argument("--serve-seconds", type=float, default=1.0)
@@ -375,7 +377,7 @@ def serve_section(batch_gbps, dev, args):
     mean_bits = float(np.mean([p["tb_size"] for p in pool]))
     server = S.Server(max_step_code_blocks=args.serve_step_cbs, steps_in_flight=args.serve_slots, iterations=ITERS,
                       offset_beta=BETA, scale=SCALE, latency_steps=args.serve_latency_steps,
-                      backlog_code_blocks=args.serve_backlog, kernel=args.mixed_kernel)
+                      backlog_code_blocks=args.serve_backlog, kernel=args.mixed_kernel, engine=args.serve_engine)
     server.run_load(pool, offered_tb_per_s=200.0, duration_s=0.05, seed=1)  # warm-up
     # capacity: offered load well above what the engine sustains, blocks per second served
     st0 = server.stats()
@@ -383,13 +385,19 @@ def serve_section(batch_gbps, dev, args):
     st1 = server.stats()
     capacity = sat["tbs"] / sat["wall_s"]
     sat_items = max(st1["items"] - st0["items"], 1)
-    sat_diag = {"steps": st1["steps"] - st0["steps"],
-                "code_blocks_per_step": (st1["code_blocks"] - st0["code_blocks"]) / max(st1["steps"] - st0["steps"], 1),
-                "item_thread_occupancy": (st1["item_threads"] - st0["item_threads"]) / (384.0 * sat_items),
-                "decode_gpu_s": (st1["decode_us"] - st0["decode_us"]) * 1e-6,
-                "step_gpu_s": (st1["step_us"] - st0["step_us"]) * 1e-6,
-                "host_launch_s": (st1["host_launch_us"] - st0["host_launch_us"]) * 1e-6,
-                "host_finish_s": (st1["host_finish_us"] - st0["host_finish_us"]) * 1e-6, "wall_s": sat["wall_s"]}
+    if args.serve_engine == "steps":
+        sat_diag = {"steps": st1["steps"] - st0["steps"],
+                    "code_blocks_per_step": (st1["code_blocks"] - st0["code_blocks"]) / max(st1["steps"] - st0["steps"], 1),
+                    "item_thread_occupancy": (st1["item_threads"] - st0["item_threads"]) / (384.0 * sat_items),
+                    "decode_gpu_s": (st1["decode_us"] - st0["decode_us"]) * 1e-6,
+                    "step_gpu_s": (st1["step_us"] - st0["step_us"]) * 1e-6,
+                    "host_launch_s": (st1["host_launch_us"] - st0["host_launch_us"]) * 1e-6,
+                    "host_finish_s": (st1["host_finish_us"] - st0["host_finish_us"]) * 1e-6, "wall_s": sat["wall_s"]}
+    else:  # one persistent kernel: launches only after idle periods
+        sat_diag = {"kernel_launches": st1["steps"] - st0["steps"], "work_items": st1["items"] - st0["items"],
+                    "code_blocks": st1["code_blocks"] - st0["code_blocks"],
+                    "item_thread_occupancy": (st1["item_threads"] - st0["item_threads"]) / (384.0 * sat_items),
+                    "wall_s": sat["wall_s"]}
     points = []
     for frac in args.serve_loads:
         lam = frac * capacity
@@ -409,11 +417,13 @@ def serve_section(batch_gbps, dev, args):
     return {"workload": SERVE_WORKLOAD, "pool_tbs": len(pool), "mean_tb_bits": mean_bits,
             "step_code_blocks": args.serve_step_cbs, "steps_in_flight": args.serve_slots or 6,
             "latency_steps": args.serve_latency_steps or 3,
-            "backlog_code_blocks": args.serve_backlog or 128, "decode_kernel": args.mixed_kernel, "points": points,
+            "backlog_code_blocks": args.serve_backlog or 128, "decode_kernel": args.mixed_kernel,
+            "engine": args.serve_engine, "points": points,
             "capacity_tb_per_s": capacity, "saturated_decoded_gbps": sat_gbps,
             "saturated_goodput_gbps": sat["info_bits_ok"] / sat["wall_s"] / 1e9,
             "saturated_decoded_vs_batch": sat_gbps / batch_gbps, "saturation_diag": sat_diag,
-            "steps": st["steps"], "mean_code_blocks_per_step": st["code_blocks"] / max(st["steps"], 1)}
+            "launches" if args.serve_engine == "continuous" else "steps": st["steps"],
+            "code_blocks": st["code_blocks"]}
 
 
 def time_decodes(fn, reps, stream):

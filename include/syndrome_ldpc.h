@@ -477,6 +477,14 @@ typedef struct {
   int32_t decode_kernel;         /* 0 = the paired kernel with its check-row state mostly in
                                     tensor memory (two CTAs per SM), 5 = all of it in shared
                                     memory (one CTA per SM); identical results */
+  int32_t engine;                /* 0 = continuous: one persistent kernel takes each
+                                    transmission's code blocks as they arrive (with
+                                    decode_kernel 0 and app_clamp >= 7874; otherwise steps),
+                                    1 = steps of up to max_step_code_blocks, up to
+                                    steps_in_flight at once; identical results */
+  uint32_t idle_us;              /* continuous engine: the kernel exits after this long
+                                    without work and is relaunched with the next
+                                    transmission (0 = 2000) */
 } SyndromeServeConfig;
 typedef struct {
   uint64_t tb_id;
@@ -513,6 +521,11 @@ int32_t syndrome_serve_release(SyndromeServer* server, uint64_t tb_id);
  * from each step's first copy to its last, worker microseconds building steps,
  * worker microseconds finishing steps}. */
 int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out14);
+/* Continuous engine (zeros for the step engine): out10 = {work items the persistent
+ * kernel finished, then microseconds summed over its CTAs: busy, HARQ combine, decode,
+ * code-block CRCs, transport-block finish; then the worker's iterations and its
+ * microseconds admitting, publishing and taking results}. */
+int32_t syndrome_serve_core_stats(SyndromeServer* server, double* out10);
 /* Work-item sizes per shape: n triples (base_graph, z, codewords per item; 0 = as many
  * as one CTA holds), as chosen by the autotuner (syndrome_b200/autotune.py).  Takes
  * effect from the next step; results do not depend on it.  INVALID_PARAM for a base

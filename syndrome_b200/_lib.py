@@ -87,6 +87,7 @@ PROTOTYPES = {
     "syndrome_serve_fetch": (_i32, [_vp, ctypes.c_uint64, _vp, _sz]),
     "syndrome_serve_release": (_i32, [_vp, ctypes.c_uint64]),
     "syndrome_serve_stats": (_i32, [_vp, _vp]),
+    "syndrome_serve_core_stats": (_i32, [_vp, _vp]),
     "syndrome_serve_run_load": (_i32, [_vp, _vp, _sz, _vp, _vp, _vp, _sz]),
     "syndrome_wifi_shortening_counts": (_i32, [_sz, _sz, _sz, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
     "syndrome_wifi_encode_shortened": (_i32, [_vp, _vp, _sz, _sz, _vp, _sz]),

@@ -26,8 +26,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
           "-I" + CSRC, "-I" + INCLUDE]
 DEVICE = ["-fmad=false", "-ftz=false", "-prec-div=true", "-prec-sqrt=true", "-Xptxas", "-O3"]
 
-SOURCES = ["graph.cpp", "encoder.cpp", "channel.cpp", "tb.cpp", "frames.cpp", "serve.cpp", "serve_load.cpp", "mixed.cpp", "wifi_mixed.cpp", "capi.cpp", "ldpc_kernels.cu", "nr_kernels.cu", "nr_pair_kernels.cu", "serve_kernels.cu", "encoder_kernels.cu", "nr_f32_kernels.cu"]
-HEADERS = ["smem_limit.h", "nr_graph.cuh", "nr_pair.cuh", "graph.h", "tb.h", "frames.h", "serve.h", "serve_kernels.h", "encoder.h", "channel.h", "decoder.h", "graph_tables.h", "base_graph_tables.inc",
+SOURCES = ["graph.cpp", "encoder.cpp", "channel.cpp", "tb.cpp", "frames.cpp", "serve.cpp", "serve_cont.cpp", "serve_load.cpp", "mixed.cpp", "wifi_mixed.cpp", "capi.cpp", "ldpc_kernels.cu", "nr_kernels.cu", "nr_pair_kernels.cu", "serve_kernels.cu", "encoder_kernels.cu", "nr_f32_kernels.cu"]
+HEADERS = ["smem_limit.h", "nr_graph.cuh", "nr_pair.cuh", "graph.h", "tb.h", "frames.h", "serve.h", "serve_kernels.h", "serve_device.cuh", "encoder.h", "channel.h", "decoder.h", "graph_tables.h", "base_graph_tables.inc",
            "nr_kernels.h", "nr_layered_tables.h", "mixed.h", "wifi_mixed.h"]
 
 

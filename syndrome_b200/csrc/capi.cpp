@@ -1060,6 +1060,9 @@ int32_t syndrome_serve_create(const SyndromeServeConfig* config, SyndromeServer*
       if (config->decode_kernel != 0 && config->decode_kernel != 5)
         return fail(SYNDROME_INVALID_PARAM, "decode_kernel must be 0 or 5");
       c.decode_kernel = config->decode_kernel;
+      if (config->engine != 0 && config->engine != 1) return fail(SYNDROME_INVALID_PARAM, "engine must be 0 or 1");
+      c.mode = config->engine;
+      if (config->idle_us) c.idle_us = (long long)std::min<uint32_t>(config->idle_us, 1000000u);
     }
     auto* s = new SyndromeServer();
     std::string err;
@@ -1153,6 +1156,17 @@ int32_t syndrome_serve_stats(SyndromeServer* server, int64_t* out14) {
                            (int64_t)(s.step_ms * 1000.0), (int64_t)(s.host_launch_ms * 1000.0),
                            (int64_t)(s.host_finish_ms * 1000.0)};
     for (int i = 0; i < 14; ++i) out14[i] = v[i];
+    return SYNDROME_OK;
+  });
+}
+
+int32_t syndrome_serve_core_stats(SyndromeServer* server, double* out10) {
+  return guard([&]() -> int32_t {
+    if (!server || !out10) return SYNDROME_NULL_POINTER;
+    const syn::ServeCoreStats s = server->engine.core_stats();
+    const double v[10] = {(double)s.items, s.busy_us,  s.combine_us, s.decode_us,  s.crc_us,
+                          s.finish_us,     (double)s.loops, s.admit_us, s.publish_us, s.complete_us};
+    for (int i = 0; i < 10; ++i) out10[i] = v[i];
     return SYNDROME_OK;
   });
 }

@@ -22,6 +22,7 @@
 #include "nr_kernels.h"
 #include "smem_limit.h"
 #include "nr_pair.cuh"
+#include "serve_device.cuh"
 
 namespace syn {
 namespace nrp {
@@ -1255,7 +1256,8 @@ __device__ __noinline__ void tm_mixed_item(const MixArgs& m, const MixItem& it, 
     const MixCodeword cb = vbv ? m.cws[it.first + 2 * p + 1] : ca;
     const int8_t* sa = va ? m.llr + ca.llr_off - 2 * Z : nullptr;
     const int8_t* sb = vbv ? m.llr + cb.llr_off - 2 * Z : nullptr;
-    auto fetch = [&](const int8_t* src, int j) -> int { return (src && j >= 2 * Z) ? (int)src[j] : 0; };
+    // through L2: the persistent serving kernel rewrites these bytes while it runs
+    auto fetch = [&](const int8_t* src, int j) -> int { return (src && j >= 2 * Z) ? (int)__ldcg(src + j) : 0; };
     if (lane_ok) {
       const int kpa = ca.n_filler > K ? 0 : K - ca.n_filler, kpb = cb.n_filler > K ? 0 : K - cb.n_filler;
       uint32_t* apw = reinterpret_cast<uint32_t*>(smem + cx.ap);
@@ -1397,7 +1399,393 @@ __global__ void __launch_bounds__(kPairThreads, 2) nr_pair_tm_mixed_kernel(const
   }
 }
 
+// ------------------------------------------------- persistent serving kernel --
+//
+// One kernel for the whole serving stream (serve_kernels.h, ServeContArgs): CTAs claim
+// work items from a ring the host publishes into host-mapped memory; per item a CTA
+// runs the HARQ combine of its code blocks into int8 decoder input, the decode of
+// tm_mixed_item, the code blocks' CRCs, and counts them done; the CTA that completes a
+// transmission's last code block folds the TB CRC, writes the report and the
+// desegmented bits to host-mapped memory and then the completion flag.
+//
+// Memory written while the kernel runs (decoder input, accumulators, staged LLRs, hard
+// decisions, CRC records) is read through L2 (ld.cg); host-mapped records through
+// ld.cv.  The only wait is the claim loop: bounded by idle_ns of the global timer and
+// by an iteration limit, after which the CTA exits (the host relaunches the kernel when
+// it publishes into a ring no kernel serves).
+
+constexpr int kSrvHdr = kTmMixSmem;  // SrvHdr
+constexpr int kSrvCws = kSrvHdr + 512;  // MixCodeword[kServeMaxItemCbs]
+constexpr int kSrvSmem = kSrvCws + kServeMaxItemCbs * (int)sizeof(MixCodeword);
+static_assert(kSrvSmem + 1024 <= 233472 / 2, "two CTAs per SM");
+
+struct SrvHdr {
+  long long item;  // claimed ring index, -1 = exit
+  int last;        // this CTA completed the transmission
+  int pad;
+  ServeJob job;
+  ServeTxRec rec;
+  uint32_t red[2 * 12];
+};
+static_assert(sizeof(SrvHdr) <= 512 && sizeof(ServeTxRec) % 4 == 0 && sizeof(ServeJob) == 16, "serving header");
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_gpu(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_sys64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_acquire_sys32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_sys32(unsigned* p, unsigned v) {
+  asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Thread 0: the next ring index, or -1 once this launch is closing.  The launch closes
+// when no CTA has claimed an item (or seen a new one) for idle_ns, counted from the
+// later of the last claim and this CTA's start, on the host's stop with the ring
+// drained, or at the iteration limit.  One CTA at a time reads the host tail and
+// mirrors it into device memory; the others poll the mirror.
+//
+// Placement: the two CTAs of an SM slow each other down (a lone BG1 Z=384 pair decodes
+// in ~180 us, two side by side in ~320 us), so a CTA whose SM sibling is busy leaves a
+// shallow queue (at most kShallow items) for up to kGraceNs to the CTAs of idle SMs.
+constexpr unsigned long long kShallow = 2, kGraceNs = 20000;
+__device__ __forceinline__ unsigned sm_id() {
+  unsigned v;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(v));
+  return v & 1023u;
+}
+__device__ long long srv_claim(const ServeContArgs& a, unsigned long long t_start) {
+  ServeCtl* ctl = a.ctl;
+  const unsigned sm = sm_id();
+  unsigned nap = 256;  // backoff of an idle CTA, up to 8 us, so pollers leave the claim line to the claimers
+  unsigned long long seen = 0;  // when this CTA first saw a claimable item it left to others
+  for (int spins = 0; spins < (1 << 22); ++spins) {
+    if (*reinterpret_cast<volatile unsigned*>(&ctl->closing) == a.epoch) return -1;
+    const unsigned long long h = ld_acquire_gpu(&ctl->head), t = ld_acquire_gpu(&ctl->tail);
+    if (h < t) {
+      if (t - h <= kShallow && *reinterpret_cast<volatile int*>(a.sm_busy + sm) > 0) {
+        const unsigned long long now = global_ns();
+        if (seen == 0) seen = now;
+        if (now - seen < kGraceNs) {
+          __nanosleep(1000);
+          continue;
+        }
+      }
+      if (atomicCAS(&ctl->head, h, h + 1) == h) {
+        atomicAdd(a.sm_busy + sm, 1);
+        atomicMax(&ctl->last_ns, global_ns());
+        __threadfence_system();  // the item's host-written records after the tail that covers it
+        return (long long)h;
+      }
+      continue;
+    }
+    if (atomicCAS(&ctl->watch, 0u, 1u) == 0u) {
+      const unsigned long long ht = ld_acquire_sys64(a.host_tail);
+      const unsigned stop = ld_acquire_sys32(a.host_stop);
+      if (ht > t) {
+        __threadfence();
+        atomicMax(&ctl->tail, ht);
+        atomicMax(&ctl->last_ns, global_ns());
+      }
+      atomicExch(&ctl->watch, 0u);
+      if (ht > h) continue;
+      if (stop) break;
+    }
+    // (another CTA may stamp last_ns after this CTA read the timer: no unsigned wrap)
+    const unsigned long long now = global_ns(), last = ld_acquire_gpu(&ctl->last_ns);
+    const unsigned long long ref = last > t_start ? last : t_start;
+    if (now > ref && now - ref > a.idle_ns) break;
+    __nanosleep(nap);
+    if (nap < 8192) nap *= 2;
+  }
+  atomicExch(&ctl->closing, a.epoch);
+  return -1;
+}
+
+// CRC-24A register of the code block's first crc_len bits and the CRC-24B check over
+// its K' bits, by the whole CTA: word w contributes (its bits * x^24 mod P) * x^(bits
+// after it) mod P, and the contributions add (XOR).
+__device__ void srv_cb_crc(const ServeContArgs& a, SrvHdr* hdr, const uint32_t* hard, int kp, int len, bool check_b,
+                           ServeCbCrc* out) {
+  const int tid = (int)threadIdx.x;
+  const uint32_t(*ta)[256] = reinterpret_cast<const uint32_t(*)[256]>(a.crc_tab);
+  const uint32_t(*tb)[256] = reinterpret_cast<const uint32_t(*)[256]>(a.crc_tab + 1024);
+  const uint32_t* xa = a.xpow;
+  const uint32_t* xb = a.xpow + kServeXpow;
+  uint32_t ra = 0u, rb = 0u;
+  for (int w = tid; 32 * w < kp; w += kPairThreads) {
+    const uint32_t v = __brev(__ldcg(hard + w));  // first stream bit in the MSB
+    const int nb = min(32, kp - 32 * w);
+    const uint32_t vb = nb < 32 ? v >> (32 - nb) : v;
+    rb ^= srv::crc_mulmod(srv::crc_step4(0u, vb, tb), __ldg(xb + (kp - 32 * w - nb)), srv::kPolyB);
+    if (32 * w < len) {
+      const int na = min(32, len - 32 * w);
+      const uint32_t va = na < 32 ? v >> (32 - na) : v;
+      ra ^= srv::crc_mulmod(srv::crc_step4(0u, va, ta), __ldg(xa + (len - 32 * w - na)), srv::kPolyA);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ra ^= __shfl_xor_sync(0xFFFFFFFFu, ra, o);
+    rb ^= __shfl_xor_sync(0xFFFFFFFFu, rb, o);
+  }
+  const int lane = tid & 31, warp = tid >> 5;
+  if (lane == 0) {
+    hdr->red[2 * warp] = ra;
+    hdr->red[2 * warp + 1] = rb;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t sa = 0u, sb = 0u;
+    for (int i = 0; i < kPairThreads / 32; ++i) {
+      sa ^= hdr->red[2 * i];
+      sb ^= hdr->red[2 * i + 1];
+    }
+    out->crc_a = sa;
+    out->ok_b = check_b ? (sb == 0u ? 1 : 0) : 1;
+  }
+  __syncthreads();
+}
+
+// The transmission's report and desegmented bits (transport_block.rs:1014-1050), by the
+// CTA that finished its last code block; then the completion flag.
+__device__ void srv_finish(const ServeContArgs& a, const ServeTxRec& rec, int tx) {
+  const int tid = (int)threadIdx.x;
+  unsigned char* sm = pair_smem + kTmMixAp;  // the decode's areas are free here
+  uint32_t(*my)[256] = reinterpret_cast<uint32_t(*)[256]>(sm);  // (v << 8k) * x^payload mod P_A
+  uint32_t* s_crc = reinterpret_cast<uint32_t*>(sm + 3 * 1024);
+  int* s_ok = reinterpret_cast<int*>(s_crc + 160);
+  int* s_it = s_ok + 160;
+  const int C = rec.n_cb, first = rec.slot_first;
+  for (int i = tid; i < 768; i += kPairThreads)
+    my[i >> 8][i & 255] = srv::crc_mulmod((uint32_t)(i & 255) << (8 * (i >> 8)), rec.x_payload, srv::kPolyA);
+  for (int i = tid; i < C; i += kPairThreads) {
+    s_crc[i] = __ldcg(&a.crc[first + i].crc_a);
+    s_ok[i] = __ldcg(&a.crc[first + i].ok_b);
+    s_it[i] = __ldcg(a.iters + first + i);
+  }
+  __syncthreads();
+  ServeTxOut* out = a.outs + tx;
+  if (tid == 0) {
+    uint32_t total = 0;
+    int all_cb = 1, max_it = 0;
+    for (int i = 0; i < C; ++i) {
+      const long long rest = rec.b - (long long)i * rec.payload;
+      const int len = (int)(rest < 0 ? 0 : (rest < rec.payload ? rest : rec.payload));
+      if (len == rec.payload)
+        total = srv::mul_fixed(total, my) ^ s_crc[i];
+      else if (len > 0)
+        total = srv::crc_mulmod(total, i == C - 1 ? rec.x_last : srv::crc_xpow(len, srv::kPolyA), srv::kPolyA) ^
+                s_crc[i];
+      all_cb &= s_ok[i];
+      max_it = max(max_it, s_it[i]);
+    }
+    out->result[0] = (all_cb && total == 0u) ? 1 : 0;
+    out->result[1] = max_it;
+  }
+  if (tid < 6) {
+    uint32_t bits = 0;
+    for (int t = 0; t < 32 && 32 * tid + t < C; ++t) bits |= (uint32_t)s_ok[32 * tid + t] << t;
+    out->result[2 + tid] = (int32_t)bits;
+  }
+  // TB bit i is bit i % payload of code block i / payload; a word spans at most two
+  // code blocks (with more than one block, payload > 32)
+  const int hw = (rec.k_prime + 31) >> 5;
+  auto bits_at = [&](int c, int j) -> uint32_t {  // 32 bits of block c from bit j on (0 past its words)
+    const uint32_t* h = a.hard + (long long)(first + c) * kServeHardWords;
+    const int w = j >> 5;
+    const uint32_t lo = w < hw ? __ldcg(h + w) : 0u, hi = w + 1 < hw ? __ldcg(h + w + 1) : 0u;
+    return __funnelshift_r(lo, hi, (unsigned)(j & 31));
+  };
+  const int nwords = (int)((rec.tb_size + 31) >> 5);
+  for (int w = tid; w < nwords; w += kPairThreads) {
+    const int i0 = 32 * w;
+    const int c = i0 / rec.payload, j = i0 - c * rec.payload;
+    uint32_t v = bits_at(c, j);
+    const int avail = rec.payload - j;
+    if (avail < 32) {
+      v &= (1u << avail) - 1u;
+      if (c + 1 < C) v |= bits_at(c + 1, 0) << avail;
+    }
+    const long long left = rec.tb_size - i0;
+    if (left < 32) v &= (1u << left) - 1u;
+    rec.bits[w] = v;
+  }
+  __threadfence_system();
+  __syncthreads();
+  if (tid == 0) {
+    a.tx_done[tx] = 0;  // ready for the slot's next transmission
+    __threadfence_system();
+    st_release_sys32(&out->flag, rec.seq);
+  }
+}
+
+__global__ void __launch_bounds__(kPairThreads, 2) serve_cont_kernel(const __grid_constant__ ServeContArgs a) {
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(pair_smem);
+  SrvHdr* hdr = reinterpret_cast<SrvHdr*>(pair_smem + kSrvHdr);
+  MixCodeword* cws = reinterpret_cast<MixCodeword*>(pair_smem + kSrvCws);
+  const int tid = (int)threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(s_tmem)),
+                 "r"(tm::kCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tm::fence_before();
+  __syncthreads();
+  tm::fence_after();
+  const uint32_t tmb = *s_tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(tm::kSlot * (warp >> 2));
+  const unsigned long long t_start = global_ns();
+  MixArgs m{};
+  m.cws = cws;
+  m.llr = a.llr;
+  m.out = a.hard;
+  m.iters = a.iters;
+  m.shift_tab = a.shift_tab;
+  m.colz_tab = a.colz_tab;
+  m.beta_q = a.beta_q;
+  m.app_clamp = a.app_clamp;
+  m.iterations = a.iterations;
+  m.k32 = 32;
+  m.two = 2;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) hdr->item = srv_claim(a, t_start);
+    __syncthreads();
+    const long long item = hdr->item;
+    if (item < 0) break;
+    unsigned long long tp[5];  // phase boundaries (thread 0)
+    if (tid == 0) tp[0] = global_ns();
+    // the job and its transmission's record, host-mapped
+    if (tid < 4)
+      reinterpret_cast<int*>(&hdr->job)[tid] =
+          __ldcv(reinterpret_cast<const int*>(a.ring + (unsigned long long)item % a.ring_cap) + tid);
+    __syncthreads();
+    const int tx = hdr->job.tx;
+    if (tid < (int)(sizeof(ServeTxRec) / 4))
+      reinterpret_cast<int*>(&hdr->rec)[tid] = __ldcv(reinterpret_cast<const int*>(a.recs + tx) + tid);
+    __syncthreads();
+    const ServeTxRec& rec = hdr->rec;
+    const int first_cb = hdr->job.first_cb, count = hdr->job.count;
+    if (tid < count) {
+      const int slot = rec.slot_first + first_cb + tid;
+      MixCodeword c{};
+      c.llr_off = (long long)slot * kServeLlrStride;
+      c.out_off = (long long)slot * kServeHardWords;
+      c.n_filler = rec.n_filler;
+      c.hard_bits = rec.k_prime;
+      c.index = slot;
+      cws[tid] = c;
+    }
+    // HARQ combine of the item's code blocks into their decoder input
+    {
+      srv::CombineWalk w;
+      w.ncb = rec.ncb;
+      w.fs = rec.fs;
+      w.fe = rec.fe;
+      w.m = rec.m;
+      w.c0 = rec.c0;
+      w.e_len = rec.e_len;
+      w.qm = rec.qm;
+      w.first = rec.first;
+      for (int j = 0; j < count; ++j) {
+        const int ci = first_cb + j;
+        float* acc = rec.acc + (long long)ci * rec.ncb;
+        const float* e = rec.e + (long long)ci * rec.e_len;
+        int8_t* llr = a.llr + (long long)(rec.slot_first + ci) * kServeLlrStride;
+        srv::combine_cb(w, acc, e, llr, a.scale, tid, kPairThreads);
+      }
+    }
+    __syncthreads();
+    if (tid == 0) tp[1] = global_ns();
+    MixItem it{};
+    it.bg = rec.bg;
+    it.z = rec.z;
+    it.zi = rec.zi;
+    it.count = count;
+    it.first = 0;
+    if (it.bg == 0) {
+      if (it.z == 384)
+        tm_mixed_item<0, 384>(m, it, tmb);
+      else
+        tm_mixed_item<0, -1>(m, it, tmb);
+    } else {
+      if (it.z == 384)
+        tm_mixed_item<1, 384>(m, it, tmb);
+      else
+        tm_mixed_item<1, -1>(m, it, tmb);
+    }
+    __syncthreads();
+    if (tid == 0) tp[2] = global_ns();
+    for (int j = 0; j < count; ++j) {
+      const int ci = first_cb + j, slot = rec.slot_first + ci;
+      const long long rest = rec.b - (long long)ci * rec.payload;
+      const int len = (int)(rest < 0 ? 0 : (rest < rec.payload ? rest : rec.payload));
+      srv_cb_crc(a, hdr, a.hard + (long long)slot * kServeHardWords, rec.k_prime, len, rec.has_cb_crc != 0,
+                 a.crc + slot);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+      tp[3] = global_ns();
+      hdr->last = atomicAdd(a.tx_done + tx, count) + count == rec.n_cb ? 1 : 0;
+    }
+    __syncthreads();
+    if (hdr->last) {
+      __threadfence();
+      srv_finish(a, rec, tx);
+    }
+    if (tid == 0) {
+      tp[4] = global_ns();
+      atomicSub(a.sm_busy + sm_id(), 1);
+      ServeCtl* c = a.ctl;
+      atomicAdd(&c->items, 1ull);
+      atomicAdd(&c->busy_ns, tp[4] - tp[0]);
+      atomicAdd(&c->combine_ns, tp[1] - tp[0]);
+      atomicAdd(&c->decode_ns, tp[2] - tp[1]);
+      atomicAdd(&c->crc_ns, tp[3] - tp[2]);
+      atomicAdd(&c->finish_ns, tp[4] - tp[3]);
+    }
+  }
+  tm::wait_st();
+  tm::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tm::fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*s_tmem), "r"(tm::kCols) : "memory");
+  }
+}
+
 }  // namespace nrp
+
+cudaError_t serve_cont_prepare() {
+  cudaError_t e = cudaFuncSetAttribute(nrp::serve_cont_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       nrp::kSrvSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(nrp::serve_cont_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              cudaSharedmemCarveoutMaxShared);
+}
+
+// Two CTAs per SM (see pair_tm_mixed_launch); every CTA stays until it finds no item.
+cudaError_t serve_cont_launch(const ServeContArgs& a, int sms, cudaStream_t stream) {
+  nrp::serve_cont_kernel<<<2 * std::max(sms, 1), nrp::kPairThreads, nrp::kSrvSmem, stream>>>(a);
+  return cudaGetLastError();
+}
 
 bool nr_pair_applies(const NrCommon& c) {
   const bool fill = c.prologue && c.k_prime < c.k;

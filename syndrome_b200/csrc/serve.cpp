@@ -57,6 +57,7 @@ ServeEngine::~ServeEngine() {
   cv_work_.notify_all();
   if (thread_.joinable()) thread_.join();
   cudaSetDevice(device_);
+  release_cont();
   for (Slot& s : slots_) {
     if (s.stream) cudaStreamSynchronize(s.stream);
     cudaFree(s.d_llr);
@@ -100,6 +101,8 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
   cfg_.latency_slots = std::max(1, std::min(cfg_.latency_slots, cfg_.slots));
   if (cfg_.backlog_cbs <= 0) cfg_.backlog_cbs = 128;
   if (cfg_.harq_bytes <= 0 || cfg_.staging_bytes < 0) return fail("negative memory budget");
+  if (cfg_.mode != 0 && cfg_.mode != 1) return fail("mode must be 0 (continuous) or 1 (steps)");
+  if (cfg_.idle_us < 10 || cfg_.idle_us > 1000000) return fail("idle_us must be in [10, 1e6]");
   if (cfg_.iterations < 0) return fail("iterations must be non-negative");
   if (cfg_.app_clamp < 255) return fail("app_clamp below 255 is not supported by the serving decoder");
   beta_q_ = syn::beta_q(cfg_.beta, cfg_.scale);
@@ -132,7 +135,17 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
     ok = cudaMemcpy(d_shift_, shift.data(), sizeof(short) * shift.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(d_colz_, colz.data(), sizeof(int) * colz.size(), cudaMemcpyHostToDevice) == cudaSuccess;
   }
-  free_[0] = cfg_.harq_bytes & ~255LL;
+  harq_.reset(cfg_.harq_bytes & ~255LL);
+  cont_ = tmem_ && cfg_.mode == 0;
+  if (cont_) {
+    if (!ok || !init_cont(err)) {
+      cudaGetLastError();
+      if (!ok) return fail("allocating the serving buffers failed (HBM budget too large?)");
+      return false;
+    }
+    thread_ = std::thread([this] { worker_cont(); });
+    return true;
+  }
   slots_.resize(cfg_.slots);
   for (Slot& s : slots_) {
     if (!ok) break;
@@ -166,26 +179,26 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
   return true;
 }
 
-long long ServeEngine::harq_alloc(long long bytes) {
-  bytes = al256(bytes);
+long long RangeAlloc::alloc(long long n) {
+  if (n <= 0) return -1;
   for (auto it = free_.begin(); it != free_.end(); ++it) {
-    if (it->second < bytes) continue;
-    const long long off = it->first, rest = it->second - bytes;
+    if (it->second < n) continue;
+    const long long off = it->first, rest = it->second - n;
     free_.erase(it);
-    if (rest > 0) free_[off + bytes] = rest;
-    used_[off] = bytes;
-    harq_used_ += bytes;
+    if (rest > 0) free_[off + n] = rest;
+    used_[off] = n;
+    used += n;
     return off;
   }
   return -1;
 }
 
-void ServeEngine::harq_free(long long off) {
+void RangeAlloc::release(long long off) {
   auto u = used_.find(off);
   if (u == used_.end()) return;
   long long size = u->second;
   used_.erase(u);
-  harq_used_ -= size;
+  used -= size;
   auto next = free_.lower_bound(off);
   if (next != free_.end() && off + size == next->first) {
     size += next->second;
@@ -201,6 +214,10 @@ void ServeEngine::harq_free(long long off) {
   }
   free_[off] = size;
 }
+
+long long ServeEngine::harq_alloc(long long bytes) { return harq_.alloc(al256(bytes)); }
+
+void ServeEngine::harq_free(long long off) { harq_.release(off); }
 
 int ServeEngine::submit(uint64_t id, long long tb_size, float rate, int qm, long long g, int rv, const float* llr,
                         long long llr_len, bool on_device, std::string* err) {
@@ -594,7 +611,7 @@ void ServeEngine::set_tile(int bg, int z, int tile) {
 ServeStats ServeEngine::stats() {
   std::lock_guard<std::mutex> lk(mu_);
   ServeStats s = stats_;
-  s.harq_bytes_used = harq_used_;
+  s.harq_bytes_used = harq_.used;
   s.pending = (long long)(pending_retx_.size() + pending_new_.size());
   s.in_flight = inflight_;
   s.tbs_held = (long long)tbs_.size();

@@ -44,6 +44,28 @@ struct ServeConfig {
   // Code-block decode: 0 = the paired kernel in its tensor-memory form (two CTAs per SM),
   // 5 = the paired kernel with all state in shared memory (one CTA per SM).
   int decode_kernel = 0;
+  // 0 = continuous: one persistent kernel takes each transmission's code blocks as soon
+  // as they are published (serve_cont.cpp; with the tensor-memory decode, else steps);
+  // 1 = steps of up to max_step_cbs code blocks, up to `slots` in flight.
+  int mode = 0;
+  // Continuous mode: the kernel exits once no CTA has found work for this long (it is
+  // relaunched with the next transmission).
+  long long idle_us = 2000;
+};
+
+// First-fit allocator of [0, size) in units (free list merged on release).
+struct RangeAlloc {
+  std::map<long long, long long> free_;  // offset -> length
+  std::unordered_map<long long, long long> used_;
+  long long used = 0;
+  void reset(long long size) {
+    free_.clear();
+    used_.clear();
+    used = 0;
+    if (size > 0) free_[0] = size;
+  }
+  long long alloc(long long n);  // offset, or -1
+  void release(long long off);
 };
 
 struct ServeResult {
@@ -67,6 +89,14 @@ struct ServeStats {
   double host_launch_ms = 0.0, host_finish_ms = 0.0;  // worker time building and finishing steps
 };
 
+// Continuous engine: what the persistent kernel and the worker spent their time on.
+struct ServeCoreStats {
+  long long items = 0;  // work items the kernel finished
+  double busy_us = 0, combine_us = 0, decode_us = 0, crc_us = 0, finish_us = 0;  // summed over CTAs
+  long long loops = 0;  // worker iterations
+  double admit_us = 0, publish_us = 0, complete_us = 0;
+};
+
 class ServeEngine {
  public:
   ~ServeEngine();
@@ -83,6 +113,8 @@ class ServeEngine {
   // Drops the state of id (HARQ accumulators included).  Not while a transmission is in flight.
   int release(uint64_t id, std::string* err);
   ServeStats stats();
+  // Zeros in the step engine.
+  ServeCoreStats core_stats();
   // Codewords per work item for one shape (0 = as many as a CTA holds); takes effect
   // from the next step.
   void set_tile(int bg, int z, int tile);
@@ -138,11 +170,32 @@ class ServeEngine {
     std::chrono::steady_clock::time_point launched;
   };
 
+  // A transmission of the continuous mode from admission to its result.
+  struct Flight {
+    Pending pd;
+    int tx = -1;              // transmission slot (record, report)
+    long long cb_first = -1;  // first code-block slot
+    int n_cb = 0;
+    long long bits_off = -1;  // words into the host-mapped bits arena
+    long long stage_off = -1; // floats into the device staging arena (host LLRs)
+    cudaEvent_t staged = nullptr;
+    uint32_t seq = 0;
+    bool published = false;
+    std::chrono::steady_clock::time_point t_pub;
+  };
+
   void worker();
   bool launch_step(Slot& s);
   void finish_step(Slot& s);
   long long harq_alloc(long long bytes);
   void harq_free(long long off);
+  bool init_cont(std::string* err);
+  void release_cont();
+  void worker_cont();
+  bool admit_cont();
+  bool publish_cont();
+  bool complete_cont();
+  void fail_all_cont();
 
   ServeConfig cfg_;
   int device_ = 0, sms_ = 0, max_words_ = 0, max_tb_words_ = 0, beta_q_ = 0;
@@ -151,9 +204,7 @@ class ServeEngine {
   char* d_harq_ = nullptr;
   short* d_shift_ = nullptr;
   int* d_colz_ = nullptr;
-  std::map<long long, long long> free_;       // HARQ arena free list: offset -> bytes
-  std::unordered_map<long long, long long> used_;
-  long long harq_used_ = 0;
+  RangeAlloc harq_;  // HARQ arena, bytes (256-byte units are rounded up by harq_alloc)
   std::vector<Slot> slots_;
   std::deque<int> order_;                    // busy slots (worker thread only)
   int inflight_ = 0;                         // order_.size(), readable under mu_
@@ -169,6 +220,39 @@ class ServeEngine {
   std::thread thread_;
   std::string fatal_;
   std::atomic<int> tiles_[2][385] = {};
+
+  // ---- continuous mode ----
+  bool cont_ = false;
+  cudaStream_t c_stream_ = nullptr, c_copy_ = nullptr;
+  cudaEvent_t c_kernel_done_ = nullptr;
+  bool c_running_ = false;
+  ServeContArgs c_args_{};
+  ServeJob* h_ring_ = nullptr;       // host-mapped
+  ServeTxRec* h_recs_ = nullptr;
+  ServeTxOut* h_outs_ = nullptr;
+  unsigned long long* h_tail_ = nullptr;
+  unsigned* h_stop_ = nullptr;
+  uint32_t* h_bits_ = nullptr;
+  uint32_t* d_bits_map_ = nullptr;   // device address of h_bits_
+  unsigned long long c_tail_ = 0;    // items published
+  int c_txs_ = 0;
+  long long c_cbs_ = 0, c_bits_words_ = 0, c_stage_floats_ = 0;
+  int8_t* d_c_llr_ = nullptr;
+  uint32_t* d_c_hard_ = nullptr;
+  int32_t* d_c_iters_ = nullptr;
+  ServeCbCrc* d_c_crc_ = nullptr;
+  int* d_c_done_ = nullptr;
+  int* d_c_smbusy_ = nullptr;
+  ServeCtl* d_c_ctl_ = nullptr;
+  uint32_t* d_c_tabs_ = nullptr;     // CRC slice tables, then x^n tables
+  float* d_c_stage_ = nullptr;
+  std::vector<int> c_free_tx_;
+  RangeAlloc c_cb_alloc_, c_bits_alloc_, c_stage_alloc_;
+  std::deque<Flight> c_flights_;     // admission order (worker thread only)
+  std::vector<cudaEvent_t> c_events_;  // free staging events
+  uint32_t c_seq_ = 0;
+  unsigned c_epoch_ = 0;  // launches of the persistent kernel
+  std::atomic<long long> c_loops_{0}, c_admit_ns_{0}, c_publish_ns_{0}, c_complete_ns_{0};
 };
 
 // Open-loop Poisson load against an engine (serve_load.cpp, syndrome_serve_run_load).

@@ -21,110 +21,42 @@
 
 #include <algorithm>
 
+#include "serve_device.cuh"
+
 namespace syn {
 
 namespace {
 
-constexpr uint32_t kPolyA = 0x864CFBu, kPolyB = 0x800063u;
-
-__host__ __device__ inline uint32_t crc_mulmod(uint32_t a, uint32_t b, uint32_t poly) {
-  uint32_t r = 0;
-  for (int i = 23; i >= 0; --i) {
-    r <<= 1;
-    if (r & 0x1000000u) r ^= 0x1000000u | poly;
-    if ((b >> i) & 1u) r ^= a;
-  }
-  return r;
-}
-
-__host__ __device__ inline uint32_t crc_xpow(long long n, uint32_t poly) {
-  uint32_t result = 1u, base = 2u;  // x^0, x^1
-  while (n > 0) {
-    if (n & 1) result = crc_mulmod(result, base, poly);
-    base = crc_mulmod(base, base, poly);
-    n >>= 1;
-  }
-  return result;
-}
-
-__device__ inline uint32_t crc_bit(uint32_t reg, uint32_t bit, uint32_t poly) {
-  const uint32_t fb = ((reg >> 23) ^ bit) & 1u;
-  reg = (reg << 1) & 0xFFFFFFu;
-  return fb ? reg ^ poly : reg;
-}
-
-// CRC register of bits [0, nbits) of LSB-first packed words (stream bit i is bit i % 32
-// of word i / 32), one thread, t = the four slice tables of the polynomial.
-__device__ uint32_t thread_crc(const uint32_t* words, int nbits, const uint32_t (*t)[256],
-                               uint32_t poly) {
-  const int full = nbits >> 5, rem = nbits & 31;
-  uint32_t reg = 0;
-  for (int w = 0; w < full; ++w) {
-    const uint32_t x = (reg << 8) ^ __brev(words[w]);  // first stream bit in the MSB
-    reg = t[3][x >> 24] ^ t[2][(x >> 16) & 0xFFu] ^ t[1][(x >> 8) & 0xFFu] ^ t[0][x & 0xFFu];
-  }
-  if (rem) {
-    const uint32_t w = words[full];
-    for (int i = 0; i < rem; ++i) reg = crc_bit(reg, (w >> i) & 1u, poly);
-  }
-  return reg;
-}
-
-// x * y mod P for a fixed y, from the tables m[k][v] = (v << 8k) * y mod P.
-__device__ __forceinline__ uint32_t mul_fixed(uint32_t x, const uint32_t (*m)[256]) {
-  return m[0][x & 0xFFu] ^ m[1][(x >> 8) & 0xFFu] ^ m[2][(x >> 16) & 0xFFu];
-}
+using srv::crc_mulmod;
+using srv::crc_xpow;
+using srv::kPolyA;
+using srv::kPolyB;
+using srv::mul_fixed;
+using srv::thread_crc;
 
 constexpr int kCombThreads = 256, kCombPer = 4;  // positions per thread (block-strided)
-constexpr int kCombMaxAdds = 16;  // contributions per position: E <= 8 * ncb and M >= ncb / 2
 
 __global__ void __launch_bounds__(kCombThreads) serve_combine_kernel(const ServeCb* __restrict__ cbs, float scale) {
   // Only the fields used, once per thread, and 32-bit index arithmetic throughout (the
   // kernel is otherwise bound by its integer instructions, not by memory).
   const ServeCb* cbp = cbs + blockIdx.y;
-  const int ncb = cbp->ncb, fs = cbp->fs, fe = cbp->fe, m = cbp->m, e_len = cbp->e_len, qm = cbp->qm;
-  const int first = cbp->first, c0 = cbp->c0 % m;
-  float* __restrict__ acc = cbp->acc;
-  const float* __restrict__ e = cbp->e;
-  int8_t* __restrict__ llr = cbp->llr;
-  const int rows = e_len / qm;
+  srv::CombineWalk w;
+  w.ncb = cbp->ncb;
+  w.fs = cbp->fs;
+  w.fe = cbp->fe;
+  w.m = cbp->m;
+  w.c0 = cbp->c0 % w.m;
+  w.e_len = cbp->e_len;
+  w.qm = cbp->qm;
+  w.first = cbp->first;
+  float* acc = cbp->acc;
+  const float* e = cbp->e;
+  int8_t* llr = cbp->llr;
 #pragma unroll
   for (int i = 0; i < kCombPer; ++i) {
     const int p = (blockIdx.x * kCombPer + i) * kCombThreads + threadIdx.x;
-    if (p >= ncb) break;
-    if (p >= fs && p < fe) {  // filler positions: never transmitted, decoder pins them
-      if (first) acc[p] = 0.0f;
-      if (llr) llr[p] = 0;
-      continue;
-    }
-    const int c = p < fs ? p : p - (fe - fs);
-    int k = c - c0;
-    if (k < 0) k += m;
-    float a = first ? 0.0f : acc[p];
-    if (qm == 1) {
-      for (int kk = k; kk < e_len; kk += m) a = __fadd_rn(a, e[kk]);
-    } else {
-      // received index of selection kk: q = (kk % qm) * rows + kk / qm; add in q order
-      int q[kCombMaxAdds];
-      int n = 0;
-      for (int kk = k; kk < e_len && n < kCombMaxAdds; kk += m) {
-        const int d = kk / qm;
-        const int v = (kk - d * qm) * rows + d;
-        int j = n++;
-        while (j > 0 && q[j - 1] > v) {
-          q[j] = q[j - 1];
-          --j;
-        }
-        q[j] = v;
-      }
-      for (int j = 0; j < n; ++j) a = __fadd_rn(a, e[q[j]]);
-    }
-    acc[p] = a;
-    if (!llr) continue;  // f32 decode: the accumulator is the decoder input
-    const float v = __fmul_rn(a, scale);
-    int qv = 0;
-    if (!isnan(v)) qv = (int)fminf(fmaxf(roundf(v), -127.0f), 127.0f);
-    llr[p] = (int8_t)qv;
+    if (p >= w.ncb) break;
+    srv::combine_position(p, w, acc, e, llr, scale);
   }
 }
 
@@ -210,6 +142,7 @@ __global__ void serve_tb_finish_kernel(const ServeTb* __restrict__ tbs, const Se
 }  // namespace
 
 uint32_t crc24_xpow_host(long long n, uint32_t poly) { return crc_xpow(n, poly); }
+uint32_t crc24_mulmod_host(uint32_t a, uint32_t b, uint32_t poly) { return crc_mulmod(a, b, poly); }
 
 cudaError_t serve_combine_launch(const ServeCb* d_cbs, int n_cbs, int max_ncb, float scale, cudaStream_t stream) {
   if (n_cbs <= 0) return cudaSuccess;

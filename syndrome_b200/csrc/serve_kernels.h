@@ -42,6 +42,92 @@ struct ServeCbCrc {
 
 // x^n mod P for the 24-bit generator poly (MSB-first register convention).
 uint32_t crc24_xpow_host(long long n, uint32_t poly);
+// a * b mod P.
+uint32_t crc24_mulmod_host(uint32_t a, uint32_t b, uint32_t poly);
+
+// ---- continuous serving: one persistent kernel over a ring of work items ----
+//
+// The host writes one record per transmission (ServeTxRec) and the transmission's work
+// items (ServeJob: up to a CTA's worth of its code blocks) into host-mapped memory and
+// publishes them by advancing a 64-bit tail.  The kernel's CTAs claim items in ring
+// order; per item a CTA combines the code blocks' HARQ buffers into int8 decoder input,
+// decodes them, checks their CRCs and counts them done; the CTA that completes a
+// transmission's last code block folds the TB CRC, writes the report and the
+// desegmented bits to host-mapped memory and then the completion flag.
+constexpr int kServeLlrStride = 25344;   // int8 LLR bytes per code-block slot (N - 2Z, BG1 Z=384)
+constexpr int kServeHardWords = 264;     // packed hard-decision words per code-block slot (K' <= 8448)
+constexpr int kServeMaxItemCbs = 32;     // code blocks per work item
+constexpr int kServeXpow = 8449;         // entries of each x^n mod P table (n = 0 .. 8448)
+
+struct ServeTxRec {
+  float* acc;          // HARQ accumulators of code block 0 (block i at acc + i * ncb)
+  const float* e;      // received LLRs of code block 0 (block i at e + i * e_len)
+  uint32_t* bits;      // host-mapped output: tb_size bits, LSB-first words
+  long long tb_size;   // A
+  long long b;         // A + 24
+  int ncb, fs, fe, m, c0, e_len, qm, first;  // rate-matching walk, c0 reduced mod m
+  int bg, z, zi, n_filler, k_prime, has_cb_crc;
+  int n_cb, payload, slot_first;
+  uint32_t x_payload;  // x^payload mod P_A
+  uint32_t x_last;     // x^(CRC-24A bits of the last code block) mod P_A
+  uint32_t seq;        // value of the completion flag
+};
+
+struct ServeTxOut {
+  int32_t result[8];   // [0] crc_ok, [1] max iterations, [2 + i/32] bit i%32 = code block i CRC ok
+  uint32_t flag;       // seq of the record once result and bits are written
+  uint32_t pad[7];
+};
+
+struct ServeJob {
+  int tx;              // transmission slot
+  int first_cb;        // first code block of the item within the transmission
+  int count;           // code blocks in the item
+  int pad;
+};
+
+struct ServeCtl {      // device memory
+  unsigned long long head;     // next item to claim
+  unsigned long long tail;     // items published (mirror of the host tail)
+  unsigned long long last_ns;  // global timer of the last claim or newly seen item
+  unsigned watch;              // 1 while a CTA reads the host tail
+  unsigned closing;            // = the launch's epoch once that launch is winding down
+  // telemetry: items done and global-timer nanoseconds per phase, summed over CTAs
+  unsigned long long items, busy_ns, combine_ns, decode_ns, crc_ns, finish_ns;
+  unsigned pad[12];
+};
+
+struct ServeContArgs {
+  const ServeJob* ring;            // host-mapped, ring_cap entries
+  unsigned long long ring_cap;
+  const ServeTxRec* recs;          // host-mapped, per transmission slot
+  ServeTxOut* outs;                // host-mapped, per transmission slot
+  const unsigned long long* host_tail;  // host-mapped
+  const unsigned* host_stop;       // host-mapped: 1 = exit once no item is left
+  ServeCtl* ctl;
+  int* sm_busy;                    // [1024] items in progress per SM id (0 between launches)
+  int* tx_done;                    // per transmission slot: code blocks finished (0 between uses)
+  int8_t* llr;                     // per code-block slot kServeLlrStride bytes
+  uint32_t* hard;                  // per code-block slot kServeHardWords words
+  int32_t* iters;                  // per code-block slot
+  ServeCbCrc* crc;                 // per code-block slot
+  const uint32_t* crc_tab;         // [2][4][256] slice tables, P_A then P_B
+  const uint32_t* xpow;            // [2][kServeXpow] x^n mod P, P_A then P_B
+  const short* shift_tab;          // as MixArgs
+  const int* colz_tab;
+  int beta_q, app_clamp, iterations;
+  float scale;
+  unsigned long long idle_ns;      // the kernel exits once no CTA has claimed an item for this long
+  unsigned epoch;                  // launch number (never 0)
+};
+
+// Raises the persistent kernel's shared-memory limit (once per device).
+cudaError_t serve_cont_prepare();
+// Launches the persistent kernel: two CTAs per SM, each holding 256 TMEM columns until
+// the kernel winds down as a whole (no claim for idle_ns, or host_stop with the ring
+// drained): the CTA that sees it marks the launch closing and every CTA leaves at its
+// next claim, so a kernel never runs on with a fraction of its CTAs.
+cudaError_t serve_cont_launch(const ServeContArgs& a, int sms, cudaStream_t stream);
 
 // HARQ soft combining + quantization: acc[p] (+)= the received LLRs rate-matched to
 // position p, in received order; llr[p] = quantize(acc[p] * scale).

@@ -17,7 +17,7 @@ class _Config(ctypes.Structure):
                 ("harq_bytes", ctypes.c_uint64), ("staging_bytes", ctypes.c_uint64), ("iterations", ctypes.c_int32),
                 ("offset_beta", ctypes.c_float), ("scale", ctypes.c_float), ("app_clamp", ctypes.c_int32),
                 ("latency_steps", ctypes.c_uint32), ("backlog_code_blocks", ctypes.c_uint32),
-                ("decode_kernel", ctypes.c_int32)]
+                ("decode_kernel", ctypes.c_int32), ("engine", ctypes.c_int32), ("idle_us", ctypes.c_uint32)]
 
 
 class _Result(ctypes.Structure):
@@ -52,12 +52,15 @@ class Server:
 
     def __init__(self, max_step_code_blocks=0, steps_in_flight=0, harq_bytes=0, staging_bytes=0, iterations=8,
                  offset_beta=0.5, scale=8.0, app_clamp=32767, latency_steps=0, backlog_code_blocks=0,
-                 kernel="auto"):
+                 kernel="auto", engine="continuous", idle_us=0):
         code = {"auto": 0, "pair_smem": 5}.get(kernel)
         if code is None:
             raise ValueError(f"unknown serving kernel {kernel!r}")
+        mode = {"continuous": 0, "steps": 1}.get(engine)
+        if mode is None:
+            raise ValueError(f"unknown serving engine {engine!r}")
         cfg = _Config(max_step_code_blocks, steps_in_flight, harq_bytes, staging_bytes, iterations, offset_beta,
-                      scale, app_clamp, latency_steps, backlog_code_blocks, code)
+                      scale, app_clamp, latency_steps, backlog_code_blocks, code, mode, idle_us)
         h = ctypes.c_void_p()
         _lib.check(_lib.load().syndrome_serve_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h.value
@@ -142,6 +145,16 @@ class Server:
         keys = ("steps", "code_blocks", "transmissions", "harq_bytes_used", "pending", "in_flight", "tbs_held",
                 "max_pending", "items", "item_threads", "decode_us", "step_us", "host_launch_us", "host_finish_us")
         return dict(zip(keys, (int(x) for x in v)))
+
+    def core_stats(self):
+        """Continuous engine: items the persistent kernel finished, microseconds its CTAs
+        spent (busy, combine, decode, crc, finish) and the worker's iterations and
+        microseconds (admit, publish, complete).  Zeros for the step engine."""
+        v = np.zeros(10, dtype=np.float64)
+        _lib.check(_lib.load().syndrome_serve_core_stats(self._h, v.ctypes.data))
+        keys = ("items", "busy_us", "combine_us", "decode_us", "crc_us", "finish_us", "loops", "admit_us",
+                "publish_us", "complete_us")
+        return dict(zip(keys, (float(x) for x in v)))
 
     def run_load(self, pool, offered_tb_per_s, duration_s, max_transmissions=4, seed=0, latencies=False):
         """Open-loop Poisson load (syndrome_serve_run_load).  pool: list of dicts with

@@ -6,7 +6,10 @@ the oracle's restatement of DlSchDecoder::decode (src/transport_block.rs:829) wi
 int8 code-block decode (HARQ f32 sum -> quantize_llr_i16 -> decode_5g_i8), over
 retransmission sequences that exercise HARQ soft combining (RV 0, 2, 3, 1), several
 modulation orders and sizes from one code block to many.  Also: a transport block
-gives the same result alone and in a mix, and admission by HBM budget completes."""
+gives the same result alone and in a mix, and admission by HBM budget completes.
+
+Both engines run the same checks: the continuous one (the default: one persistent
+kernel takes each transmission's code blocks as they arrive) and the step one."""
 import numpy as np
 import pytest
 
@@ -86,9 +89,12 @@ def check_against_oracle(data, reports, payloads, iterations=8):
                 assert np.array_equal(payloads[tid], tb), label + ": CRC passed on a wrong payload"
 
 
-@pytest.mark.parametrize("kernel", ["auto", "pair_smem"])
-def test_serve_matches_oracle_with_harq(kernel):
-    server = S.Server(iterations=8, kernel=kernel)
+ENGINES = [dict(), dict(engine="steps"), dict(engine="steps", kernel="pair_smem")]
+
+
+@pytest.mark.parametrize("cfg", ENGINES)
+def test_serve_matches_oracle_with_harq(cfg):
+    server = S.Server(iterations=8, **cfg)
     data, reports, payloads = run_sequences(server, CASES)
     assert any(len(v) > 1 for v in reports.values()), "no retransmission happened: raise the noise"
     assert any(v[-1]["crc_ok"] for v in reports.values())
@@ -97,8 +103,9 @@ def test_serve_matches_oracle_with_harq(kernel):
 
 
 @pytest.mark.parametrize("cfg", [dict(max_step_code_blocks=200),
-                                 dict(max_step_code_blocks=200, latency_steps=1, backlog_code_blocks=1),
-                                 dict(steps_in_flight=16, latency_steps=16)])
+                                 dict(max_step_code_blocks=200, engine="steps"),
+                                 dict(max_step_code_blocks=200, latency_steps=1, backlog_code_blocks=1, engine="steps"),
+                                 dict(steps_in_flight=16, latency_steps=16, engine="steps")])
 def test_serve_same_result_alone_and_in_a_mix(cfg):
     """A result does not depend on what else is in flight, nor on how many steps run
     at once (the backlog policy's settings)."""
@@ -180,23 +187,56 @@ def test_serve_open_loop_load():
     s.close()
 
 
-def test_serve_large_transport_blocks_match_oracle():
+@pytest.mark.parametrize("engine", ["continuous", "steps"])
+def test_serve_large_transport_blocks_match_oracle(engine):
     """Transport blocks of 36 and 152 code blocks (the largest TB size): the
     desegmented payload and the TB CRC folded over every block must match the oracle
     and the transmitted bits."""
     cases = [(300000, 0.75, 2, 400002, 4.0), (1277992, 0.9, 6, 1419996, 5.0), (300000, 0.75, 2, 400002, 1.2)]
-    server = S.Server(iterations=8)
+    server = S.Server(iterations=8, engine=engine)
     data, reports, payloads = run_sequences(server, cases, seed0=700)
     assert any(v[-1]["crc_ok"] for v in reports.values())
     check_against_oracle(data, reports, payloads)
     server.close()
 
 
-def test_serve_256qam_and_repetition_match_oracle():
+@pytest.mark.parametrize("engine", ["continuous", "steps"])
+def test_serve_256qam_and_repetition_match_oracle(engine):
     """Qm = 8 (the combine's interleaved gather) and a code block sent almost twice
     over (E close to 2 * ncb, up to three contributions per buffer position)."""
     cases = [(40000, 0.8, 8, 50000, 3.0), (200, 0.5, 2, 2600, -1.0), (200, 0.5, 2, 2600, 2.0)]
-    server = S.Server(iterations=8)
+    server = S.Server(iterations=8, engine=engine)
     data, reports, payloads = run_sequences(server, cases, seed0=800)
     check_against_oracle(data, reports, payloads)
     server.close()
+
+
+def test_serve_continuous_kernel_exits_when_idle_and_relaunches():
+    """With a short idle limit the persistent kernel exits between transmissions that
+    arrive far apart; the next transmission relaunches it, with the same results as a
+    server that stays up."""
+    import time
+
+    a, r, qm, g, eb = CASES[3]
+    tb, llrs = make_tb(a, r, qm, g, eb, 91)
+    outs = []
+    for idle in (50, 0):
+        s = S.Server(idle_us=idle)
+        got = []
+        for k in range(3):
+            s.submit(40 + k, a, r, qm, g, 0, llrs[0])
+            res = s.wait(1)[0]
+            res.pop("latency_us")
+            got.append((res["crc_ok"], res["max_iters_used"], tuple(res["cb_crc"]), s.fetch(40 + k, a).tobytes()))
+            s.release(40 + k)
+            time.sleep(0.02)  # well past the 50 us idle limit
+        if idle:
+            assert s.stats()["steps"] == 3, "the kernel should have exited and been relaunched per transmission"
+        outs.append(got)
+        s.close()
+    assert outs[0] == outs[1]
+
+
+def test_serve_rejects_unknown_engine():
+    with pytest.raises(ValueError):
+        S.Server(engine="batch")
