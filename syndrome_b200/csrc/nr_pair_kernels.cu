@@ -1570,13 +1570,16 @@ __device__ void srv_finish(const ServeContArgs& a, const ServeTxRec& rec, int tx
   uint32_t* s_crc = reinterpret_cast<uint32_t*>(sm + 3 * 1024);
   int* s_ok = reinterpret_cast<int*>(s_crc + 160);
   int* s_it = s_ok + 160;
-  const int C = rec.n_cb, first = rec.slot_first;
+  int* s_slot = s_it + 160;
+  const int C = rec.n_cb;
   for (int i = tid; i < 768; i += kPairThreads)
     my[i >> 8][i & 255] = srv::crc_mulmod((uint32_t)(i & 255) << (8 * (i >> 8)), rec.x_payload, srv::kPolyA);
   for (int i = tid; i < C; i += kPairThreads) {
-    s_crc[i] = __ldcg(&a.crc[first + i].crc_a);
-    s_ok[i] = __ldcg(&a.crc[first + i].ok_b);
-    s_it[i] = __ldcg(a.iters + first + i);
+    const int slot = __ldcv(a.slots + (long long)tx * kServeMaxCbs + i);
+    s_slot[i] = slot;
+    s_crc[i] = __ldcg(&a.crc[slot].crc_a);
+    s_ok[i] = __ldcg(&a.crc[slot].ok_b);
+    s_it[i] = __ldcg(a.iters + slot);
   }
   __syncthreads();
   ServeTxOut* out = a.outs + tx;
@@ -1606,7 +1609,7 @@ __device__ void srv_finish(const ServeContArgs& a, const ServeTxRec& rec, int tx
   // code blocks (with more than one block, payload > 32)
   const int hw = (rec.k_prime + 31) >> 5;
   auto bits_at = [&](int c, int j) -> uint32_t {  // 32 bits of block c from bit j on (0 past its words)
-    const uint32_t* h = a.hard + (long long)(first + c) * kServeHardWords;
+    const uint32_t* h = a.hard + (long long)s_slot[c] * kServeHardWords;
     const int w = j >> 5;
     const uint32_t lo = w < hw ? __ldcg(h + w) : 0u, hi = w + 1 < hw ? __ldcg(h + w + 1) : 0u;
     return __funnelshift_r(lo, hi, (unsigned)(j & 31));
@@ -1683,7 +1686,7 @@ __global__ void __launch_bounds__(kPairThreads, 2) serve_cont_kernel(const __gri
     const ServeTxRec& rec = hdr->rec;
     const int first_cb = hdr->job.first_cb, count = hdr->job.count;
     if (tid < count) {
-      const int slot = rec.slot_first + first_cb + tid;
+      const int slot = __ldcv(a.slots + (long long)tx * kServeMaxCbs + first_cb + tid);
       MixCodeword c{};
       c.llr_off = (long long)slot * kServeLlrStride;
       c.out_off = (long long)slot * kServeHardWords;
@@ -1692,6 +1695,7 @@ __global__ void __launch_bounds__(kPairThreads, 2) serve_cont_kernel(const __gri
       c.index = slot;
       cws[tid] = c;
     }
+    __syncthreads();
     // HARQ combine of the item's code blocks into their decoder input
     {
       srv::CombineWalk w;
@@ -1707,7 +1711,7 @@ __global__ void __launch_bounds__(kPairThreads, 2) serve_cont_kernel(const __gri
         const int ci = first_cb + j;
         float* acc = rec.acc + (long long)ci * rec.ncb;
         const float* e = rec.e + (long long)ci * rec.e_len;
-        int8_t* llr = a.llr + (long long)(rec.slot_first + ci) * kServeLlrStride;
+        int8_t* llr = a.llr + cws[j].llr_off;
         srv::combine_cb(w, acc, e, llr, a.scale, tid, kPairThreads);
       }
     }
@@ -1733,7 +1737,7 @@ __global__ void __launch_bounds__(kPairThreads, 2) serve_cont_kernel(const __gri
     __syncthreads();
     if (tid == 0) tp[2] = global_ns();
     for (int j = 0; j < count; ++j) {
-      const int ci = first_cb + j, slot = rec.slot_first + ci;
+      const int ci = first_cb + j, slot = cws[j].index;
       const long long rest = rec.b - (long long)ci * rec.payload;
       const int len = (int)(rest < 0 ? 0 : (rest < rec.payload ? rest : rec.payload));
       srv_cb_crc(a, hdr, a.hard + (long long)slot * kServeHardWords, rec.k_prime, len, rec.has_cb_crc != 0,

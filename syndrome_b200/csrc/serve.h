@@ -173,8 +173,7 @@ class ServeEngine {
   // A transmission of the continuous mode from admission to its result.
   struct Flight {
     Pending pd;
-    int tx = -1;              // transmission slot (record, report)
-    long long cb_first = -1;  // first code-block slot
+    int tx = -1;              // transmission slot (record, code-block slots, report)
     int n_cb = 0;
     long long bits_off = -1;  // words into the host-mapped bits arena
     long long stage_off = -1; // floats into the device staging arena (host LLRs)
@@ -247,7 +246,9 @@ class ServeEngine {
   uint32_t* d_c_tabs_ = nullptr;     // CRC slice tables, then x^n tables
   float* d_c_stage_ = nullptr;
   std::vector<int> c_free_tx_;
-  RangeAlloc c_cb_alloc_, c_bits_alloc_, c_stage_alloc_;
+  std::vector<int> c_free_cb_;  // free code-block slots
+  int* h_slots_ = nullptr;       // host-mapped [c_txs_][kServeMaxCbs] code-block slots per transmission
+  RangeAlloc c_bits_alloc_, c_stage_alloc_;
   std::deque<Flight> c_flights_;     // admission order (worker thread only)
   std::vector<cudaEvent_t> c_events_;  // free staging events
   uint32_t c_seq_ = 0;

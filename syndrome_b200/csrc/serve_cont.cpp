@@ -3,8 +3,9 @@
 // No steps: one persistent kernel (serve_cont_kernel, nr_pair_kernels.cu) serves the
 // whole stream.  The worker thread admits transmissions in the step engine's order
 // (retransmissions first, then new blocks while their HARQ accumulators fit the HBM
-// budget), gives each a transmission slot, a contiguous range of code-block slots
-// (decoder input, hard decisions, CRC record) and a range of the host-mapped bits
+// budget), gives each a transmission slot, a code-block slot per code block (decoder
+// input, hard decisions, CRC record; any free ones, listed in host-mapped memory, so
+// that no fragmentation holds up a large block) and a range of the host-mapped bits
 // arena, writes its record and work items (code blocks of the transmission, up to a
 // CTA's worth each) into host-mapped memory and publishes them by advancing the ring's
 // tail.  The kernel's CTAs claim items as they come; a transmission's result is
@@ -63,10 +64,11 @@ bool ServeEngine::init_cont(std::string* err) {
   };
   c_cbs_ = std::max<long long>(2LL * 160, (long long)cfg_.max_step_cbs * cfg_.slots);
   c_txs_ = (int)std::min<long long>(c_cbs_, 8192);
-  c_bits_words_ = 16LL << 20;  // 64 MiB of decoded payload in flight
+  c_bits_words_ = 48LL << 20;  // 192 MiB of decoded payload in flight
   c_stage_floats_ = cfg_.staging_bytes / 4;
   bool ok = host_mapped(&h_ring_, (size_t)c_cbs_) && host_mapped(&h_recs_, (size_t)c_txs_) &&
             host_mapped(&h_outs_, (size_t)c_txs_) && host_mapped(&h_tail_, 1) && host_mapped(&h_stop_, 1) &&
+            host_mapped(&h_slots_, (size_t)c_txs_ * kServeMaxCbs) &&
             host_mapped(&h_bits_, (size_t)c_bits_words_);
   if (!ok) return fail("allocating host-mapped serving memory failed");
   ok = cudaMalloc(&d_c_llr_, (size_t)c_cbs_ * kServeLlrStride) == cudaSuccess &&
@@ -107,10 +109,11 @@ bool ServeEngine::init_cont(std::string* err) {
   a.ring = device_view(h_ring_);
   a.ring_cap = (unsigned long long)c_cbs_;  // items in flight <= code blocks in flight
   a.recs = device_view(h_recs_);
+  a.slots = device_view(h_slots_);
   a.outs = device_view(h_outs_);
   a.host_tail = device_view(h_tail_);
   a.host_stop = device_view(h_stop_);
-  if (!d_bits_map_ || !a.ring || !a.recs || !a.outs || !a.host_tail || !a.host_stop)
+  if (!d_bits_map_ || !a.ring || !a.recs || !a.slots || !a.outs || !a.host_tail || !a.host_stop)
     return fail("no device address for host-mapped memory");
   a.ctl = d_c_ctl_;
   a.tx_done = d_c_done_;
@@ -130,7 +133,8 @@ bool ServeEngine::init_cont(std::string* err) {
   a.idle_ns = (unsigned long long)cfg_.idle_us * 1000ULL;
   c_free_tx_.clear();
   for (int i = c_txs_ - 1; i >= 0; --i) c_free_tx_.push_back(i);
-  c_cb_alloc_.reset(c_cbs_);
+  c_free_cb_.clear();
+  for (long long i = c_cbs_ - 1; i >= 0; --i) c_free_cb_.push_back((int)i);
   c_bits_alloc_.reset(c_bits_words_);
   c_stage_alloc_.reset(c_stage_floats_);
   return true;
@@ -170,7 +174,8 @@ void ServeEngine::release_cont() {
   d_c_ctl_ = nullptr;
   d_c_tabs_ = nullptr;
   d_c_stage_ = nullptr;
-  for (void* p : {(void*)h_ring_, (void*)h_recs_, (void*)h_outs_, (void*)h_tail_, (void*)h_stop_, (void*)h_bits_})
+  for (void* p : {(void*)h_ring_, (void*)h_recs_, (void*)h_outs_, (void*)h_tail_, (void*)h_stop_, (void*)h_bits_,
+                  (void*)h_slots_})
     if (p) cudaFreeHost(p);
   h_ring_ = nullptr;
   h_recs_ = nullptr;
@@ -178,6 +183,7 @@ void ServeEngine::release_cont() {
   h_tail_ = nullptr;
   h_stop_ = nullptr;
   h_bits_ = nullptr;
+  h_slots_ = nullptr;
 }
 
 // Moves queued transmissions into flights while every resource they need is free:
@@ -195,23 +201,17 @@ bool ServeEngine::admit_cont() {
         const TbParams& p = t.p;
         if (c_free_tx_.empty()) return;
         const long long stage_n = pd.on_device ? 0 : (long long)p.c * t.e;
-        const long long cb = c_cb_alloc_.alloc(p.c);
-        if (cb < 0) return;
+        if ((long long)c_free_cb_.size() < p.c) return;
         const long long bits = c_bits_alloc_.alloc((t.tb_size + 31) / 32);
-        if (bits < 0) {
-          c_cb_alloc_.release(cb);
-          return;
-        }
+        if (bits < 0) return;
         long long st = -1;
         if (stage_n > 0 && (st = c_stage_alloc_.alloc(stage_n)) < 0) {
-          c_cb_alloc_.release(cb);
           c_bits_alloc_.release(bits);
           return;
         }
         if (need_harq && t.harq_off < 0) {
           t.harq_off = harq_alloc((long long)p.c * p.ncb * 4);
           if (t.harq_off < 0) {  // HBM budget full: wait for accumulators to free
-            c_cb_alloc_.release(cb);
             c_bits_alloc_.release(bits);
             if (st >= 0) c_stage_alloc_.release(st);
             return;
@@ -222,7 +222,11 @@ bool ServeEngine::admit_cont() {
         f.pd = pd;
         f.tx = c_free_tx_.back();
         c_free_tx_.pop_back();
-        f.cb_first = cb;
+        int* slots = h_slots_ + (long long)f.tx * kServeMaxCbs;
+        for (int i = 0; i < p.c; ++i) {
+          slots[i] = c_free_cb_.back();
+          c_free_cb_.pop_back();
+        }
         f.n_cb = p.c;
         f.bits_off = bits;
         f.stage_off = st;
@@ -251,7 +255,7 @@ bool ServeEngine::admit_cont() {
         r.has_cb_crc = p.has_cb_crc ? 1 : 0;
         r.n_cb = p.c;
         r.payload = p.payload;
-        r.slot_first = (int)cb;
+        r.pad = 0;
         r.x_payload = crc24_xpow_host(p.payload, kCrc24A);
         r.x_last = crc24_xpow_host(
             std::max<long long>(0, std::min<long long>(p.payload, p.b - (long long)(p.c - 1) * p.payload)), kCrc24A);
@@ -368,7 +372,8 @@ bool ServeEngine::complete_cont() {
       t.busy = false;
       done_.push_back(res);
       stats_.step_ms += res.step_us * 1e-3;
-      c_cb_alloc_.release(f.cb_first);
+      const int* slots = h_slots_ + (long long)f.tx * kServeMaxCbs;
+      for (int i = 0; i < f.n_cb; ++i) c_free_cb_.push_back(slots[i]);
       c_bits_alloc_.release(f.bits_off);
       if (f.stage_off >= 0) c_stage_alloc_.release(f.stage_off);
       c_free_tx_.push_back(f.tx);

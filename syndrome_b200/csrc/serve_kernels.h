@@ -47,8 +47,8 @@ uint32_t crc24_mulmod_host(uint32_t a, uint32_t b, uint32_t poly);
 
 // ---- continuous serving: one persistent kernel over a ring of work items ----
 //
-// The host writes one record per transmission (ServeTxRec) and the transmission's work
-// items (ServeJob: up to a CTA's worth of its code blocks) into host-mapped memory and
+// The host writes one record per transmission (ServeTxRec), the slots of its code blocks
+// and its work items (ServeJob: up to a CTA's worth of its code blocks) into host-mapped memory and
 // publishes them by advancing a 64-bit tail.  The kernel's CTAs claim items in ring
 // order; per item a CTA combines the code blocks' HARQ buffers into int8 decoder input,
 // decodes them, checks their CRCs and counts them done; the CTA that completes a
@@ -58,6 +58,7 @@ constexpr int kServeLlrStride = 25344;   // int8 LLR bytes per code-block slot (
 constexpr int kServeHardWords = 264;     // packed hard-decision words per code-block slot (K' <= 8448)
 constexpr int kServeMaxItemCbs = 32;     // code blocks per work item
 constexpr int kServeXpow = 8449;         // entries of each x^n mod P table (n = 0 .. 8448)
+constexpr int kServeMaxCbs = 160;        // code blocks per transport block (code-block slot list length)
 
 struct ServeTxRec {
   float* acc;          // HARQ accumulators of code block 0 (block i at acc + i * ncb)
@@ -67,7 +68,7 @@ struct ServeTxRec {
   long long b;         // A + 24
   int ncb, fs, fe, m, c0, e_len, qm, first;  // rate-matching walk, c0 reduced mod m
   int bg, z, zi, n_filler, k_prime, has_cb_crc;
-  int n_cb, payload, slot_first;
+  int n_cb, payload, pad;
   uint32_t x_payload;  // x^payload mod P_A
   uint32_t x_last;     // x^(CRC-24A bits of the last code block) mod P_A
   uint32_t seq;        // value of the completion flag
@@ -101,6 +102,7 @@ struct ServeContArgs {
   const ServeJob* ring;            // host-mapped, ring_cap entries
   unsigned long long ring_cap;
   const ServeTxRec* recs;          // host-mapped, per transmission slot
+  const int* slots;                // host-mapped, per transmission slot: its code blocks' slots [kServeMaxCbs]
   ServeTxOut* outs;                // host-mapped, per transmission slot
   const unsigned long long* host_tail;  // host-mapped
   const unsigned* host_stop;       // host-mapped: 1 = exit once no item is left
