@@ -399,7 +399,12 @@ def serve_section(batch_gbps, dev, args):
                     "item_thread_occupancy": (st1["item_threads"] - st0["item_threads"]) / (384.0 * sat_items),
                     "wall_s": sat["wall_s"]}
     points = []
-    for frac in args.serve_loads:
+    tx_per_tb = sat["transmissions"] / max(sat["tbs"], 1)
+    # 85 % of the batch throughput (decoded information Gbit/s), offered
+    # at 87 % so that the achieved rate (arrivals are random, the run ends with a drain)
+    # reaches it
+    bar_lam = 0.87 * batch_gbps * 1e9 / (mean_bits * tx_per_tb)
+    for frac in list(args.serve_loads) + [bar_lam / capacity]:
         lam = frac * capacity
         rep = server.run_load(pool, offered_tb_per_s=lam, duration_s=args.serve_seconds, seed=int(frac * 1000))
         points.append({"offered_frac_of_capacity": frac, "offered_tb_per_s": lam, "tbs": rep["tbs"],
@@ -414,11 +419,19 @@ def serve_section(batch_gbps, dev, args):
     st = server.stats()
     server.close()
     sat_gbps = sat["info_bits_decoded"] / sat["wall_s"] / 1e9
+    b = points.pop()
+    bar = {"target_decoded_gbps": 0.85 * batch_gbps, "achieved_decoded_gbps": b["decoded_gbps"],
+           "achieved_vs_batch": b["decoded_gbps"] / batch_gbps, "offered_tb_per_s": b["offered_tb_per_s"],
+           "p50_tb_us": b["p50_us"], "p99_tb_us": b["p99_us"], "p50_tx_us": b["tx_p50_us"], "p99_tx_us": b["tx_p99_us"],
+           "met_per_transport_block": bool(b["p99_us"] <= 1000.0 and b["decoded_gbps"] >= 0.85 * batch_gbps),
+           "met_per_transmission": bool(b["tx_p99_us"] <= 1000.0 and b["decoded_gbps"] >= 0.85 * batch_gbps),
+           "note": "latency per transport block runs from its first transmission's arrival to its final result "
+                   "(up to four transmissions in sequence); per transmission from submission to result"}
     return {"workload": SERVE_WORKLOAD, "pool_tbs": len(pool), "mean_tb_bits": mean_bits,
             "step_code_blocks": args.serve_step_cbs, "steps_in_flight": args.serve_slots or 6,
             "latency_steps": args.serve_latency_steps or 3,
             "backlog_code_blocks": args.serve_backlog or 128, "decode_kernel": args.mixed_kernel,
-            "engine": args.serve_engine, "points": points,
+            "engine": args.serve_engine, "bar_85pct_of_batch": bar, "points": points,
             "capacity_tb_per_s": capacity, "saturated_decoded_gbps": sat_gbps,
             "saturated_goodput_gbps": sat["info_bits_ok"] / sat["wall_s"] / 1e9,
             "saturated_decoded_vs_batch": sat_gbps / batch_gbps, "saturation_diag": sat_diag,

@@ -270,9 +270,11 @@ int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const
  * working to a per-slot deadline must not call cudaMalloc (it can synchronise the
  * device and take milliseconds), and a plug-in inside an application that owns all
  * device allocations has no allocator to call.  Same arguments and results as
- * syndrome_ldpc_decode_batch_i8 without the workspace: the generic int8 kernel keeps
- * its messages in a static device array of SYNDROME_NOALLOC_SCRATCH_BYTES that every
- * GPU loading this library holds until exit.  A launch runs at most
+ * syndrome_ldpc_decode_batch_i8 without the workspace.  On 5G NR graphs it runs the
+ * kernel syndrome_ldpc_decoder_set_kernel chose (the NR kernels keep their state on
+ * chip and need no device memory) unless that is 1 or 4; otherwise the generic int8
+ * kernel keeps its messages in a static device array of SYNDROME_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading this library holds until exit.  A launch runs at most
  * SYNDROME_NOALLOC_SCRATCH_BYTES / (codewords per CTA * edges * Z) CTAs; a code whose
  * per-CTA messages exceed the array is rejected with SYNDROME_INVALID_PARAM.  The
  * first call on a device looks up the array's address (cudaGetSymbolAddress), so make
@@ -280,10 +282,9 @@ int32_t syndrome_ldpc_decode_batch_f32(const SyndromeLdpcDecoder* decoder, const
  * calls must not cross a cudaDeviceReset.  Nothing in the array must start at zero
  * and it keeps the last call's contents; calls that overlap on the GPU share the
  * array and race.  The current device must be the decoder's.  The array is used when
- * d_edge_r is NULL (with d_edge_r the messages go there instead).  The kernel choice
- * of syndrome_ldpc_decoder_set_kernel does not apply: this entry always runs the
- * generic layered kernel with its messages in global memory, the throughput of
- * kernel 4; every call also queries the kernel's occupancy on the host. */
+ * d_edge_r is NULL (with d_edge_r the messages go there instead).  The generic path
+ * runs at the throughput of kernel 4 (messages in global memory) and every call
+ * queries that kernel's occupancy on the host. */
 #define SYNDROME_NOALLOC_SCRATCH_BYTES (32u << 20)
 int32_t syndrome_ldpc_decode_batch_i8_noalloc(const SyndromeLdpcDecoder* decoder,
                                               const int8_t* d_llr, size_t llr_stride,

@@ -603,6 +603,7 @@ int32_t syndrome_ldpc_decode_batch_i8_noalloc(const SyndromeLdpcDecoder* decoder
     r.edge_r_stride = (long long)edge_r_stride;
     r.hard = d_hard;
     r.hard_stride = (long long)hard_stride;
+    r.kernel = decoder->kernel;
     std::string msg;
     cudaError_t e = decoder->dec.decode_i8_noalloc(r, static_cast<cudaStream_t>(stream), &msg);
     return from_cuda(e, msg);

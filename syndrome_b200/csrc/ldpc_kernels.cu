@@ -1303,6 +1303,10 @@ cudaError_t Decoder::decode_i8_noalloc(const BatchRequest& req, cudaStream_t str
   cudaError_t e = cudaGetDevice(&cur);
   if (e != cudaSuccess) return e;
   if (cur != device_) return bad("the current device is not the decoder's device");
+  // 5G NR graphs: the NR kernels keep their check-row state on chip and need no device
+  // memory beyond the caller's outputs, so the decoder's own choice runs unchanged
+  if (nr_bg_ >= 0 && !req.llr_i16 && req.app_clamp >= 255 && req.kernel != 1 && req.kernel != 4)
+    return decode(Precision::kInt8, req, stream, err);
   void* scratch = nullptr;
   e = noalloc_scratch(cur, &scratch);
   if (e != cudaSuccess) return e;

@@ -9,7 +9,10 @@ one running on the array the first one left behind) give exactly what the
 workspace-based entry point gives.  BG1 Z=384 with 600 codewords needs more CTAs
 than the array holds slots for (33,554,432 / 121,344 = 276), so the launch is capped
 and each CTA walks several groups through the same slot.  With a message output the
-kernel writes the messages there instead; that case is checked too.
+kernel writes the messages there instead; that case is checked too.  These shapes are
+5G NR graphs, on which the entry runs the decoder's own kernel choice (the NR kernels
+keep their state on chip and need no scratch): the static array is exercised with the
+generic kernel chosen, and the default choice is checked as well.
 Collected last so that a run stopping at the first failure has run everything else.
 """
 import ctypes
@@ -56,10 +59,11 @@ def noalloc_call(dec, llr, iters, quant, hard_bits, with_messages):
     return out
 
 
+@pytest.mark.parametrize("kernel", ["generic", "auto"])
 @pytest.mark.parametrize("with_messages", [False, True], ids=["scratch", "messages_out"])
 @pytest.mark.parametrize("bg,z,count", [(0, 384, 600), (1, 52, 150)])
-def test_noalloc_matches_workspace_entry_point_on_two_calls(bg, z, count, with_messages):
-    dec = S.QcLdpcDecoder.with_lifting_size(bg, z, 0.5)
+def test_noalloc_matches_workspace_entry_point_on_two_calls(bg, z, count, with_messages, kernel):
+    dec = S.QcLdpcDecoder.with_lifting_size(bg, z, 0.5).set_kernel(kernel)
     quant = S.QuantParams()
     hard_bits = dec.info_bit_count_5g()
     for call, (ebno, seed) in enumerate(((1.0, 11), (2.0, 12345))):
