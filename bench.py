@@ -73,6 +73,9 @@ def parse_args():
                    help="waiting code blocks that allow more steps in flight (0: the engine's default)")
     p.add_argument("--serve-loads", type=float, nargs="+", default=[0.1, 0.25, 0.5, 0.75],
                    help="offered loads as fractions of the measured serving capacity")
+    p.add_argument("--configs-only", action="store_true",
+                   help="print only the other workloads' section (profiling runs of their kernels)")
+    p.add_argument("--mixed-count", type=int, default=65536, help="code blocks of the mixed 5G NR workload")
     p.add_argument("--no-configs", action="store_true",
                    help="skip the other workloads (Wi-Fi single shape, mixed 5G NR, mixed Wi-Fi)")
     return p.parse_args()
@@ -456,7 +459,7 @@ def time_decodes(fn, reps, stream):
     return e0.elapsed_time(e1) / reps
 
 
-def configs_section(dev, mixed_kernel="auto"):
+def configs_section(dev, mixed_kernel="auto", mixed_count=65536):
     """The benchmark's other workloads, each device-resident, information Gbit/s:
     802.11 Z=27 R=1/2 (1024 codewords, f32, <= 10 iterations, 1.5 dB), mixed 5G NR code
     blocks (65536, rate-matched, int8, <= 8 iterations, one persistent launch from a CUDA
@@ -486,14 +489,14 @@ def configs_section(dev, mixed_kernel="auto"):
         "gbps": 1024 * k / (ms * 1e-3) / 1e9, "ms_per_launch": ms, "mean_iterations": float(r.iters.float().mean()),
         "frames_correct": int((got == info.cpu().numpy()).all(axis=1).sum()), "codewords": 1024}
     # mixed 5G NR, rate-matched
-    recs, llr8, words, bits = W.nr_rate_matched(65536, 33, device=dev)
+    recs, llr8, words, bits = W.nr_rate_matched(mixed_count, 33, device=dev)
     batch = S.MixedBatch(recs, 0.5, S.QuantParams(), ITERS)
     tmem = batch.set_kernel(mixed_kernel)
     o = torch.zeros(max(words, 1), dtype=torch.int32, device=dev)
     it = torch.zeros(len(recs), dtype=torch.int32, device=dev)
     ms = time_decodes(lambda: batch.decode(llr8, o, it, use_graph=True), 5, stream)
     out["nr_mixed_rate_matched"] = {
-        "workload": "65536 5G NR code blocks: BG1 with Z in {64,128,256,384} or BG2 with Z any lifting size <= 384 "
+        "workload": f"{mixed_count} 5G NR code blocks: BG1 with Z in {{64,128,256,384}} or BG2 with Z any lifting size <= 384 "
                     "(1/2 each), filler uniform in [0, K/5], target rate uniform in [1/5, 8/9] by RV0 bit selection "
                     "(puncturing or repetition), Eb/N0 uniform in [0, 3] dB, int8 at scale 8, <= 8 iterations; one "
                     "persistent launch replayed from a CUDA graph (MixedBatch)",
@@ -550,6 +553,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.configs_only:
+        print(json.dumps({"configs": configs_section(dev, args.mixed_kernel, args.mixed_count)}), flush=True)
+        return 0
     if world > 1:
         import datetime
 
@@ -708,7 +714,7 @@ def main():
                                  "compared": "iteration count and packed information bits of each codeword of the "
                                              "CPU sample, GPU output of the timed launches vs the CPU pipeline"}
     if rank == 0 and world == 1 and not args.no_configs:
-        line["configs"] = configs_section(dev, args.mixed_kernel)
+        line["configs"] = configs_section(dev, args.mixed_kernel, args.mixed_count)
     if rank == 0 and world == 1 and not args.no_serve:
         line["serve"] = serve_section(value, dev, args)
     if rank == 0:

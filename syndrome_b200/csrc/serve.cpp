@@ -181,16 +181,15 @@ bool ServeEngine::init(const ServeConfig& cfg, std::string* err) {
 
 long long RangeAlloc::alloc(long long n) {
   if (n <= 0) return -1;
-  for (auto it = free_.begin(); it != free_.end(); ++it) {
-    if (it->second < n) continue;
-    const long long off = it->first, rest = it->second - n;
-    free_.erase(it);
-    if (rest > 0) free_[off + n] = rest;
-    used_[off] = n;
-    used += n;
-    return off;
-  }
-  return -1;
+  auto b = by_len_.lower_bound(n);  // the shortest free range that holds n
+  if (b == by_len_.end()) return -1;
+  const long long off = b->second, len = b->first;
+  by_len_.erase(b);
+  free_.erase(off);
+  if (len > n) add(off + n, len - n);
+  used_[off] = n;
+  used += n;
+  return off;
 }
 
 void RangeAlloc::release(long long off) {
@@ -202,17 +201,20 @@ void RangeAlloc::release(long long off) {
   auto next = free_.lower_bound(off);
   if (next != free_.end() && off + size == next->first) {
     size += next->second;
-    free_.erase(next);
+    drop(next);
   }
   auto it = free_.lower_bound(off);
   if (it != free_.begin()) {
     auto prev = std::prev(it);
     if (prev->first + prev->second == off) {
-      prev->second += size;
+      const long long start = prev->first;
+      size += prev->second;
+      drop(prev);
+      add(start, size);
       return;
     }
   }
-  free_[off] = size;
+  add(off, size);
 }
 
 long long ServeEngine::harq_alloc(long long bytes) { return harq_.alloc(al256(bytes)); }

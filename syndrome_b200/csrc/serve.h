@@ -53,19 +53,37 @@ struct ServeConfig {
   long long idle_us = 2000;
 };
 
-// First-fit allocator of [0, size) in units (free list merged on release).
+// Best-fit allocator of [0, size) in units: free ranges by offset (merged on release)
+// and by length, so that both take O(log n).
 struct RangeAlloc {
   std::map<long long, long long> free_;  // offset -> length
+  std::multimap<long long, long long> by_len_;  // length -> offset
   std::unordered_map<long long, long long> used_;
   long long used = 0;
   void reset(long long size) {
     free_.clear();
+    by_len_.clear();
     used_.clear();
     used = 0;
-    if (size > 0) free_[0] = size;
+    if (size > 0) add(0, size);
   }
   long long alloc(long long n);  // offset, or -1
   void release(long long off);
+
+ private:
+  void add(long long off, long long len) {
+    free_[off] = len;
+    by_len_.emplace(len, off);
+  }
+  void drop(std::map<long long, long long>::iterator it) {
+    auto r = by_len_.equal_range(it->second);
+    for (auto j = r.first; j != r.second; ++j)
+      if (j->second == it->first) {
+        by_len_.erase(j);
+        break;
+      }
+    free_.erase(it);
+  }
 };
 
 struct ServeResult {
@@ -249,7 +267,10 @@ class ServeEngine {
   std::vector<int> c_free_cb_;  // free code-block slots
   int* h_slots_ = nullptr;       // host-mapped [c_txs_][kServeMaxCbs] code-block slots per transmission
   RangeAlloc c_bits_alloc_, c_stage_alloc_;
-  std::deque<Flight> c_flights_;     // admission order (worker thread only)
+  // flights by transmission slot (worker thread only): admitted and not yet published
+  // (admission order), published (any order, c_pub_pos_ = index in c_pub_ or -1)
+  std::vector<Flight> c_fl_;
+  std::vector<int> c_unpub_, c_pub_, c_pub_pos_, c_done_scratch_;
   std::vector<cudaEvent_t> c_events_;  // free staging events
   uint32_t c_seq_ = 0;
   unsigned c_epoch_ = 0;  // launches of the persistent kernel

@@ -133,6 +133,12 @@ bool ServeEngine::init_cont(std::string* err) {
   a.idle_ns = (unsigned long long)cfg_.idle_us * 1000ULL;
   c_free_tx_.clear();
   for (int i = c_txs_ - 1; i >= 0; --i) c_free_tx_.push_back(i);
+  c_fl_.assign(c_txs_, Flight());
+  c_pub_pos_.assign(c_txs_, -1);
+  c_unpub_.clear();
+  c_pub_.clear();
+  c_unpub_.reserve(c_txs_);
+  c_pub_.reserve(c_txs_);
   c_free_cb_.clear();
   for (long long i = c_cbs_ - 1; i >= 0; --i) c_free_cb_.push_back((int)i);
   c_bits_alloc_.reset(c_bits_words_);
@@ -146,9 +152,10 @@ void ServeEngine::release_cont() {
     if (c_stream_) cudaStreamSynchronize(c_stream_);  // CTAs exit once the ring is drained
   }
   if (c_copy_) cudaStreamSynchronize(c_copy_);
-  for (Flight& f : c_flights_)
-    if (f.staged) c_events_.push_back(f.staged);
-  c_flights_.clear();
+  for (int tx : c_unpub_)
+    if (c_fl_[tx].staged) c_events_.push_back(c_fl_[tx].staged);
+  c_unpub_.clear();
+  c_pub_.clear();
   for (cudaEvent_t e : c_events_) cudaEventDestroy(e);
   c_events_.clear();
   if (c_kernel_done_) cudaEventDestroy(c_kernel_done_);
@@ -189,8 +196,8 @@ void ServeEngine::release_cont() {
 // Moves queued transmissions into flights while every resource they need is free:
 // retransmissions first, then new transport blocks while their accumulators fit.
 bool ServeEngine::admit_cont() {
-  std::vector<size_t> stage;  // flights that copy host LLRs
-  const size_t before = c_flights_.size();
+  std::vector<int> stage;  // flights that copy host LLRs
+  const size_t before = c_unpub_.size();
   {
     std::lock_guard<std::mutex> lk(mu_);
     if (!fatal_.empty()) return false;
@@ -218,10 +225,12 @@ bool ServeEngine::admit_cont() {
           }
           t.tx_count = 0;
         }
-        Flight f;
-        f.pd = pd;
-        f.tx = c_free_tx_.back();
+        const int tx = c_free_tx_.back();
         c_free_tx_.pop_back();
+        Flight& f = c_fl_[tx];
+        f = Flight();
+        f.pd = pd;
+        f.tx = tx;
         int* slots = h_slots_ + (long long)f.tx * kServeMaxCbs;
         for (int i = 0; i < p.c; ++i) {
           slots[i] = c_free_cb_.back();
@@ -264,16 +273,16 @@ bool ServeEngine::admit_cont() {
         stats_.code_blocks += p.c;
         stats_.transmissions += 1;
         q.pop_front();
-        if (stage_n > 0) stage.push_back(c_flights_.size());
-        c_flights_.push_back(f);
+        if (stage_n > 0) stage.push_back(tx);
+        c_unpub_.push_back(tx);
       }
     };
     admit(pending_retx_, false);
     admit(pending_new_, true);
-    inflight_ = (int)c_flights_.size();
+    inflight_ = (int)(c_unpub_.size() + c_pub_.size());
   }
-  for (size_t i : stage) {  // host LLRs: copy, published once the copy has finished
-    Flight& f = c_flights_[i];
+  for (int tx : stage) {  // host LLRs: copy, published once the copy has finished
+    Flight& f = c_fl_[tx];
     if (c_events_.empty()) {
       cudaEvent_t e = nullptr;
       cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
@@ -290,7 +299,7 @@ bool ServeEngine::admit_cont() {
                     c_copy_);
     cudaEventRecord(f.staged, c_copy_);
   }
-  return c_flights_.size() > before;
+  return c_unpub_.size() > before;
 }
 
 // Writes the work items of admitted flights whose inputs are on the device into the
@@ -299,11 +308,15 @@ bool ServeEngine::publish_cont() {
   unsigned long long tail = c_tail_;
   long long items = 0, threads = 0;
   const auto now = std::chrono::steady_clock::now();
-  for (Flight& f : c_flights_) {
-    if (f.published) continue;
+  size_t kept = 0;  // flights still waiting for their staged LLRs stay, in order
+  for (size_t i = 0; i < c_unpub_.size(); ++i) {
+    Flight& f = c_fl_[c_unpub_[i]];
     if (f.staged) {
       const cudaError_t q = cudaEventQuery(f.staged);
-      if (q == cudaErrorNotReady) continue;
+      if (q == cudaErrorNotReady) {
+        c_unpub_[kept++] = f.tx;
+        continue;
+      }
       c_events_.push_back(f.staged);
       f.staged = nullptr;
     }
@@ -323,7 +336,10 @@ bool ServeEngine::publish_cont() {
     }
     f.published = true;
     f.t_pub = now;
+    c_pub_pos_[f.tx] = (int)c_pub_.size();
+    c_pub_.push_back(f.tx);
   }
+  c_unpub_.resize(kept);
   if (tail == c_tail_) return false;
   {
     std::lock_guard<std::mutex> lk(mu_);
@@ -338,18 +354,18 @@ bool ServeEngine::publish_cont() {
 
 // Takes the results of flights whose completion flag is set.
 bool ServeEngine::complete_cont() {
-  bool any = false;
+  std::vector<int>& done = c_done_scratch_;
+  done.clear();
+  for (int tx : c_pub_)
+    if (reinterpret_cast<std::atomic<uint32_t>*>(&h_outs_[tx].flag)->load(std::memory_order_acquire) == c_fl_[tx].seq)
+      done.push_back(tx);
+  if (done.empty()) return false;
   const auto now = std::chrono::steady_clock::now();
-  for (auto it = c_flights_.begin(); it != c_flights_.end();) {
-    Flight& f = *it;
-    if (!f.published ||
-        reinterpret_cast<std::atomic<uint32_t>*>(&h_outs_[f.tx].flag)->load(std::memory_order_acquire) != f.seq) {
-      ++it;
-      continue;
-    }
-    const int32_t* r = h_outs_[f.tx].result;
-    {
-      std::lock_guard<std::mutex> lk(mu_);
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    for (int tx : done) {
+      Flight& f = c_fl_[tx];
+      const int32_t* r = h_outs_[tx].result;
       Tb& t = tbs_[f.pd.id];
       t.tx_count += 1;
       ServeResult res;
@@ -372,34 +388,40 @@ bool ServeEngine::complete_cont() {
       t.busy = false;
       done_.push_back(res);
       stats_.step_ms += res.step_us * 1e-3;
-      const int* slots = h_slots_ + (long long)f.tx * kServeMaxCbs;
+      const int* slots = h_slots_ + (long long)tx * kServeMaxCbs;
       for (int i = 0; i < f.n_cb; ++i) c_free_cb_.push_back(slots[i]);
       c_bits_alloc_.release(f.bits_off);
       if (f.stage_off >= 0) c_stage_alloc_.release(f.stage_off);
-      c_free_tx_.push_back(f.tx);
+      c_free_tx_.push_back(tx);
+      // out of the published list: the last entry takes its place
+      const int pos = c_pub_pos_[tx], back = c_pub_.back();
+      c_pub_[pos] = back;
+      c_pub_pos_[back] = pos;
+      c_pub_.pop_back();
+      c_pub_pos_[tx] = -1;
     }
-    it = c_flights_.erase(it);
-    any = true;
+    inflight_ = (int)(c_unpub_.size() + c_pub_.size());
   }
-  if (any) {
-    std::lock_guard<std::mutex> lk(mu_);
-    inflight_ = (int)c_flights_.size();
-    cv_done_.notify_all();
-  }
-  return any;
+  cv_done_.notify_all();
+  return true;
 }
 
 // After a kernel failure: every flight and queued transmission ends with crc_ok = 0.
 void ServeEngine::fail_all_cont() {
   std::lock_guard<std::mutex> lk(mu_);
-  for (Flight& f : c_flights_) {
-    ServeResult res;
-    res.id = f.pd.id;
-    tbs_[res.id].busy = false;
-    done_.push_back(res);
-    if (f.staged) c_events_.push_back(f.staged);
-  }
-  c_flights_.clear();
+  for (const std::vector<int>* list : {&c_unpub_, &c_pub_})
+    for (int tx : *list) {
+      Flight& f = c_fl_[tx];
+      ServeResult res;
+      res.id = f.pd.id;
+      tbs_[res.id].busy = false;
+      done_.push_back(res);
+      if (f.staged) c_events_.push_back(f.staged);
+      f.staged = nullptr;
+      c_pub_pos_[tx] = -1;
+    }
+  c_unpub_.clear();
+  c_pub_.clear();
   for (std::deque<Pending>* q : {&pending_retx_, &pending_new_})
     while (!q->empty()) {
       ServeResult res;
@@ -431,8 +453,7 @@ void ServeEngine::worker_cont() {
     c_complete_ns_.fetch_add(ns(t0, t1), std::memory_order_relaxed);
     c_admit_ns_.fetch_add(ns(t1, t2), std::memory_order_relaxed);
     c_publish_ns_.fetch_add(ns(t2, t3), std::memory_order_relaxed);
-    bool waiting = false;  // published items whose results are outstanding
-    for (const Flight& f : c_flights_) waiting |= f.published;
+    const bool waiting = !c_pub_.empty();  // published items whose results are outstanding
     if (c_running_) {
       const cudaError_t q = cudaEventQuery(c_kernel_done_);
       if (q == cudaSuccess) {
@@ -464,7 +485,7 @@ void ServeEngine::worker_cont() {
         lk.lock();
         if (stop_) break;
       }
-      if (c_flights_.empty() && pending_retx_.empty() && pending_new_.empty()) {
+      if (c_unpub_.empty() && c_pub_.empty() && pending_retx_.empty() && pending_new_.empty()) {
         cv_work_.wait_for(lk, std::chrono::milliseconds(5));
         continue;
       }

@@ -240,3 +240,20 @@ def test_serve_continuous_kernel_exits_when_idle_and_relaunches():
 def test_serve_rejects_unknown_engine():
     with pytest.raises(ValueError):
         S.Server(engine="batch")
+
+
+@pytest.mark.parametrize("engine", ["continuous", "steps"])
+def test_serve_core_stats(engine):
+    """The continuous engine reports its kernel's work items and phase times (each
+    phase within the busy time); the step engine reports zeros."""
+    s = S.Server(engine=engine)
+    data, reports, payloads = run_sequences(s, CASES[:3], seed0=900)
+    c = s.core_stats()
+    s.close()
+    if engine == "steps":
+        assert all(v == 0 for v in c.values())
+        return
+    assert c["items"] >= sum(len(v) for v in reports.values())
+    parts = c["combine_us"] + c["decode_us"] + c["crc_us"] + c["finish_us"]
+    assert 0 < c["decode_us"] and parts <= c["busy_us"] * 1.001 + 1.0
+    assert c["loops"] > 0
