@@ -482,7 +482,7 @@ void ServeEngine::finish_step(Slot& s) {
       t.tx_count = 0;
     }
     t.busy = false;
-    done_.push_back(res);
+    push_done(res);
   }
   s.txs.clear();
   s.busy = false;
@@ -525,7 +525,7 @@ void ServeEngine::worker() {
             res.id = q->front().id;
             tbs_[res.id].busy = false;
             q->pop_front();
-            done_.push_back(res);
+            push_done(res);
           }
         pending_cbs_ = 0;
         cv_done_.notify_all();
@@ -561,7 +561,23 @@ void ServeEngine::worker() {
   }
 }
 
+void ServeEngine::push_done(const ServeResult& r) {  // under mu_
+  done_.push_back(r);
+  done_n_.store((long long)done_.size(), std::memory_order_release);
+}
+
 int ServeEngine::poll(ServeResult* out, int cap, long long timeout_us) {
+  if (timeout_us > 0 && done_n_.load(std::memory_order_acquire) == 0) {
+    // A result is usually a few hundred microseconds away: watch for it for up to
+    // kPollSpinUs before sleeping (a thread woken from a condition variable takes tens
+    // of microseconds, once per HARQ round trip).
+    const auto t0 = std::chrono::steady_clock::now();
+    const long long spin = std::min<long long>(timeout_us, kPollSpinUs);
+    while (done_n_.load(std::memory_order_acquire) == 0 &&
+           std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count() < spin)
+      std::this_thread::yield();
+    timeout_us -= (long long)std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+  }
   std::unique_lock<std::mutex> lk(mu_);
   if (done_.empty() && timeout_us > 0)
     cv_done_.wait_for(lk, std::chrono::microseconds(timeout_us), [&] { return !done_.empty(); });
@@ -570,6 +586,7 @@ int ServeEngine::poll(ServeResult* out, int cap, long long timeout_us) {
     out[n++] = done_.front();
     done_.pop_front();
   }
+  done_n_.store((long long)done_.size(), std::memory_order_release);
   return n;
 }
 

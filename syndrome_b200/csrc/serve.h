@@ -232,6 +232,9 @@ class ServeEngine {
   std::deque<Pending> pending_new_;   // first transmissions (need accumulators)
   long long pending_cbs_ = 0;         // code blocks of the two queues
   std::deque<ServeResult> done_;
+  std::atomic<long long> done_n_{0};  // done_.size(), readable without mu_
+  static constexpr long long kPollSpinUs = 200;
+  void push_done(const ServeResult& r);
   ServeStats stats_;
   bool stop_ = false;
   std::thread thread_;

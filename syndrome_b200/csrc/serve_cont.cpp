@@ -386,7 +386,7 @@ bool ServeEngine::complete_cont() {
         t.tx_count = 0;
       }
       t.busy = false;
-      done_.push_back(res);
+      push_done(res);
       stats_.step_ms += res.step_us * 1e-3;
       const int* slots = h_slots_ + (long long)tx * kServeMaxCbs;
       for (int i = 0; i < f.n_cb; ++i) c_free_cb_.push_back(slots[i]);
@@ -415,7 +415,7 @@ void ServeEngine::fail_all_cont() {
       ServeResult res;
       res.id = f.pd.id;
       tbs_[res.id].busy = false;
-      done_.push_back(res);
+      push_done(res);
       if (f.staged) c_events_.push_back(f.staged);
       f.staged = nullptr;
       c_pub_pos_[tx] = -1;
@@ -428,7 +428,7 @@ void ServeEngine::fail_all_cont() {
       res.id = q->front().id;
       tbs_[res.id].busy = false;
       q->pop_front();
-      done_.push_back(res);
+      push_done(res);
     }
   pending_cbs_ = 0;
   inflight_ = 0;
@@ -441,6 +441,7 @@ void ServeEngine::worker_cont() {
   auto ns = [](clk::time_point a, clk::time_point b) {
     return (long long)std::chrono::duration_cast<std::chrono::nanoseconds>(b - a).count();
   };
+  auto last_busy = clk::now();
   for (;;) {
     const auto t0 = clk::now();
     bool progressed = complete_cont();
@@ -486,9 +487,17 @@ void ServeEngine::worker_cont() {
         if (stop_) break;
       }
       if (c_unpub_.empty() && c_pub_.empty() && pending_retx_.empty() && pending_new_.empty()) {
+        // idle: watch the queues for a while before sleeping (a woken thread takes tens
+        // of microseconds; the next transmission, often a retransmission, is near)
+        if (clk::now() - last_busy < std::chrono::microseconds(kPollSpinUs)) {
+          lk.unlock();
+          std::this_thread::yield();
+          continue;
+        }
         cv_work_.wait_for(lk, std::chrono::milliseconds(5));
         continue;
       }
+      last_busy = clk::now();
     }
     if (!progressed) std::this_thread::yield();
   }
