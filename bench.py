@@ -422,6 +422,16 @@ def serve_section(batch_gbps, dev, args):
     st = server.stats()
     server.close()
     sat_gbps = sat["info_bits_decoded"] / sat["wall_s"] / 1e9
+    # the other engine's saturated capacity beside it (the step engine trades latency
+    # for throughput: the HARQ combine runs as a GPU-wide kernel per step)
+    other = "steps" if args.serve_engine == "continuous" else "continuous"
+    srv2 = S.Server(max_step_code_blocks=args.serve_step_cbs, steps_in_flight=args.serve_slots, iterations=ITERS,
+                    offset_beta=BETA, scale=SCALE, latency_steps=args.serve_latency_steps,
+                    backlog_code_blocks=args.serve_backlog, kernel=args.mixed_kernel, engine=other)
+    srv2.run_load(pool, offered_tb_per_s=200.0, duration_s=0.05, seed=1)
+    sat2 = srv2.run_load(pool, offered_tb_per_s=2.0 * batch_gbps * 1e9 / mean_bits, duration_s=0.5, seed=2)
+    srv2.close()
+    other_gbps = sat2["info_bits_decoded"] / sat2["wall_s"] / 1e9
     b = points.pop()
     bar = {"target_decoded_gbps": 0.85 * batch_gbps, "achieved_decoded_gbps": b["decoded_gbps"],
            "achieved_vs_batch": b["decoded_gbps"] / batch_gbps, "offered_tb_per_s": b["offered_tb_per_s"],
@@ -438,6 +448,8 @@ def serve_section(batch_gbps, dev, args):
             "capacity_tb_per_s": capacity, "saturated_decoded_gbps": sat_gbps,
             "saturated_goodput_gbps": sat["info_bits_ok"] / sat["wall_s"] / 1e9,
             "saturated_decoded_vs_batch": sat_gbps / batch_gbps, "saturation_diag": sat_diag,
+            "other_engine": {"engine": other, "capacity_tb_per_s": sat2["tbs"] / sat2["wall_s"],
+                             "saturated_decoded_gbps": other_gbps, "saturated_decoded_vs_batch": other_gbps / batch_gbps},
             "launches" if args.serve_engine == "continuous" else "steps": st["steps"],
             "code_blocks": st["code_blocks"]}
 
