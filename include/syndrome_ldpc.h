@@ -463,10 +463,13 @@ void syndrome_dlsch_decoder_flush_harq(SyndromeDlSchDecoder* decoder);
  * retransmissions of blocks that hold accumulators go ahead). */
 typedef struct SyndromeServer SyndromeServer;
 typedef struct {
-  uint32_t max_step_code_blocks; /* code blocks per GPU step, >= 160 (0 = 2048) */
+  uint32_t max_step_code_blocks; /* code blocks per GPU step, >= 160 (0 = 2048); the
+                                    continuous engine holds max_step_code_blocks *
+                                    steps_in_flight code blocks in flight */
   uint32_t steps_in_flight;      /* 1..16 (0 = 6): steps run concurrently on free SMs */
   uint64_t harq_bytes;           /* device memory for HARQ accumulators (0 = 8 GiB) */
-  uint64_t staging_bytes;        /* device staging for host-memory LLRs, per step (0 = 256 MiB) */
+  uint64_t staging_bytes;        /* device staging for host-memory LLRs, per step (the
+                                    continuous engine: in all) (0 = 256 MiB) */
   int32_t iterations;            /* maximum LOMS iterations (early stop on a zero syndrome) */
   float offset_beta;             /* beta_q = round(offset_beta * scale) clamped to [0, 127] */
   float scale;                   /* LLR quantizer scale (src/quantize.rs DEFAULT_SCALE = 8) */

@@ -48,7 +48,17 @@ class _LoadReport(ctypes.Structure):
 class Server:
     """A serving engine on the current CUDA device.  Zero-valued sizes take the
     library defaults (2048 code blocks per step, 6 steps in flight, 8 GiB of HARQ
-    accumulators, 256 MiB of staging for host-memory LLRs)."""
+    accumulators, 256 MiB of staging for host-memory LLRs).
+
+    engine="continuous" (default): one persistent kernel takes each transmission's
+    code blocks as soon as they are submitted (it holds max_step_code_blocks x
+    steps_in_flight code blocks in flight, exits after idle_us without work, 0 = 2000,
+    and is relaunched with the next transmission); it needs kernel="auto" and
+    app_clamp >= 7874, else the step engine runs.  engine="steps": batches of up to
+    max_step_code_blocks, up to steps_in_flight at once (latency_steps and
+    backlog_code_blocks set how many while few code blocks wait).  Results are
+    identical either way; the continuous engine has the shorter latency, the step
+    engine the higher saturated throughput."""
 
     def __init__(self, max_step_code_blocks=0, steps_in_flight=0, harq_bytes=0, staging_bytes=0, iterations=8,
                  offset_beta=0.5, scale=8.0, app_clamp=32767, latency_steps=0, backlog_code_blocks=0,
