@@ -374,7 +374,8 @@ typedef struct SyndromeWifiMixedPlan SyndromeWifiMixedPlan;
 
 /* Plans a batch of codewords of any mix of the twelve 802.11 matrices for one
  * persistent f32 launch: codewords grouped by matrix into chunks of `chunk` codewords
- * (0: four CTAs' worth of codeword slots) on a device queue, the costliest matrices
+ * (0: about four chunks per CTA over the batch, at least a CTA's codeword slots) on a
+ * device queue, the costliest matrices
  * first; every codeword slot of a CTA takes the next codeword as soon as its own
  * stops (zero syndrome or `iterations`), so skewed iteration counts keep the slots
  * busy.  f32 layered offset min-sum with offset_beta. */
