@@ -374,7 +374,7 @@ typedef struct SyndromeWifiMixedPlan SyndromeWifiMixedPlan;
 
 /* Plans a batch of codewords of any mix of the twelve 802.11 matrices for one
  * persistent f32 launch: codewords grouped by matrix into chunks of `chunk` codewords
- * (0: about four chunks per CTA over the batch, at least a CTA's codeword slots) on a
+ * (0: about four chunks per CTA over the batch, at least four codewords) on a
  * device queue, the costliest matrices
  * first; every codeword slot of a CTA takes the next codeword as soon as its own
  * stops (zero syndrome or `iterations`), so skewed iteration counts keep the slots

@@ -4,7 +4,7 @@
 // A plan is built once per batch layout: the codewords are grouped by matrix, the
 // matrices ordered by decreasing work per codeword (edges x Z) so that the long
 // codewords start first, and each matrix's codewords cut into chunks (by default about
-// four per CTA over the batch, at least a CTA's slots).  The matrices' edge and layer tables, the per-codeword records and
+// four per CTA over the batch, at least four codewords).  The matrices' edge and layer tables, the per-codeword records and
 // the chunk list go to the device once; decode() zeroes the device chunk counter and
 // launches the persistent kernel with as many CTAs as the SMs hold, optionally from a
 // captured CUDA graph.
@@ -85,10 +85,12 @@ bool WifiMixedPlan::init(const std::vector<WifiMixedCodeword>& cws, float beta, 
   std::stable_sort(order.begin(), order.end(), [&](const Key& x, const Key& y) {
     return (long long)graphs[x].edges() * graphs[x].z > (long long)graphs[y].edges() * graphs[y].z;
   });
-  // Default chunk: about four per CTA over the whole batch (two CTAs per SM), at least a
-  // CTA's slots: enough chunks that the CTAs finish together, few enough that a CTA
-  // rarely switches matrices (a sweep over 32,768 codewords: 16-32 codewords per chunk
-  // 3.95-4.00 Gbit/s, 8 3.77, 64 3.47, the earlier default of four CTAs' slots 3.65).
+  // Default chunk: about four per CTA over the whole batch (two CTAs per SM), at least
+  // four codewords (or a CTA's slots, if fewer): enough chunks that the CTAs finish
+  // together, few enough that a CTA rarely switches matrices (a sweep over 32,768
+  // codewords: 16-32 codewords per chunk 3.95-4.00 Gbit/s, 8 3.77, 64 3.47, the earlier
+  // default of four CTAs' slots 3.65; 1,024 codewords of one matrix, Z = 27: 4 per
+  // chunk 0.197 ms, 14 0.234 ms).
   int dev = 0, sms_now = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms_now, cudaDevAttrMultiProcessorCount, dev);
   const long long even = ((long long)cws.size() + 8LL * sms_now - 1) / (8LL * std::max(sms_now, 1));
@@ -116,7 +118,7 @@ bool WifiMixedPlan::init(const std::vector<WifiMixedCodeword>& cws, float beta, 
     smem = std::max(smem, wifi_mixed_smem_bytes(s));
     const int shape = (int)shapes.size();
     shapes.push_back(s);
-    const int per_chunk = chunk > 0 ? chunk : (int)std::max<long long>(s.cpb, even);
+    const int per_chunk = chunk > 0 ? chunk : (int)std::max<long long>(std::min(s.cpb, 4), even);
     const std::vector<int>& idx = groups[key];
     for (size_t f = 0; f < idx.size(); f += per_chunk) {
       WmChunk ch{};

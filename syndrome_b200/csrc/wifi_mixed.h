@@ -78,7 +78,7 @@ class WifiMixedPlan {
  public:
   ~WifiMixedPlan();
   // chunk: codewords per queue entry of a matrix (0: about four chunks per CTA over the
-  // whole batch, at least a CTA's slots).
+  // whole batch, at least four codewords or a CTA's slots if fewer).
   bool init(const std::vector<WifiMixedCodeword>& cws, float beta, int iterations, int chunk, std::string* err);
   cudaError_t decode(const float* d_llr, uint32_t* d_out, int32_t* d_iters, bool use_graph, cudaStream_t stream);
   long long llr_needed() const { return need_llr_; }
