@@ -403,7 +403,7 @@ def serve_section(batch_gbps, dev, args):
                     "wall_s": sat["wall_s"]}
     points = []
     tx_per_tb = sat["transmissions"] / max(sat["tbs"], 1)
-    # 85 % of the batch throughput (decoded information Gbit/s), offered
+    # the serving bar: 85 % of the batch throughput (decoded information Gbit/s), offered
     # at 87 % so that the achieved rate (arrivals are random, the run ends with a drain)
     # reaches it
     bar_lam = 0.87 * batch_gbps * 1e9 / (mean_bits * tx_per_tb)
